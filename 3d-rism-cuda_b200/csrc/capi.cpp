@@ -1,0 +1,511 @@
+// C ABI of the solver (include/rism3d_b200.h).  Host code: validation,
+// device buffers, cuFFT plans, and the file-driven RISM3D-style entry
+// points.  No compute happens on the host: every grid operation is a CUDA
+// kernel or cuFFT, and a missing or failing device is an error, never a
+// fallback.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <new>
+#include <string>
+
+#include "rism3d_impl.h"
+#include "rism3d_io.h"
+
+using namespace rism3d;
+
+struct rism3d_ctx {
+  Context c;
+};
+
+static std::string g_create_err;
+
+namespace rism3d {
+
+bool cuda_ok(Context &c, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return true;
+  c.err = std::string(what) + ": " + cudaGetErrorString(e);
+  return false;
+}
+
+bool cufft_ok(Context &c, cufftResult r, const char *what) {
+  if (r == CUFFT_SUCCESS) return true;
+  c.err = std::string(what) + ": cuFFT error " + std::to_string((int)r);
+  return false;
+}
+
+void free_device(Context &c) {
+  void *ptrs[] = {c.d_u, c.d_e, c.d_fr, c.d_fkh, c.d_atoms, c.d_tw, c.d_twf,
+                  c.d_U, c.d_t, c.d_Y, c.d_RP, c.d_buf, c.d_h, c.d_g,
+                  c.f_U, c.f_t, c.f_Y, c.f_RP, c.f_buf, c.d_part, c.d_state,
+                  c.d_stage, c.d_obs, c.d_atom_part, c.chi.d_coef};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  c.d_u = c.d_e = c.d_fr = nullptr; c.d_fkh = nullptr; c.d_atoms = nullptr;
+  c.d_tw = nullptr; c.d_twf = nullptr; c.d_U = c.d_t = c.d_Y = c.d_RP = nullptr;
+  c.d_buf = nullptr; c.d_h = c.d_g = nullptr;
+  c.f_U = c.f_t = c.f_Y = c.f_RP = nullptr; c.f_buf = nullptr;
+  c.d_part = nullptr; c.d_state = nullptr; c.d_stage = nullptr; c.d_obs = nullptr;
+  c.d_atom_part = nullptr; c.chi.d_coef = nullptr; c.natom_part_cap = 0;
+  if (c.h_state) cudaFreeHost(c.h_state);
+  c.h_state = nullptr;
+  if (c.plan64) cufftDestroy(c.plan64);
+  if (c.plan32) cufftDestroy(c.plan32);
+  c.plan64 = c.plan32 = 0;
+  c.plans_ok = false;
+}
+
+int fetch_grid(Context &c, int which, double *host) {
+  const size_t n = (size_t)c.n, V = (size_t)c.natv;
+  auto get = [&](const double *d, double *h, size_t cnt) {
+    return cuda_ok(c, cudaMemcpy(h, d, sizeof(double) * cnt, cudaMemcpyDeviceToHost), "get_grid");
+  };
+  switch (which) {
+    case RISM3D_GRID_U: return get(c.d_u, host, V * n) ? RISM3D_OK : RISM3D_CUDA_ERROR;
+    case RISM3D_GRID_FR: return get(c.d_fr, host, n) ? RISM3D_OK : RISM3D_CUDA_ERROR;
+    case RISM3D_GRID_E: {
+      std::vector<double> fr(n);
+      if (!get(c.d_e, host, n) || !get(c.d_fr, fr.data(), n)) return RISM3D_CUDA_ERROR;
+      for (size_t j = 0; j < n; ++j) host[j] += fr[j];   // e = esr + fr
+      return RISM3D_OK;
+    }
+    default: break;
+  }
+  if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
+  switch (which) {
+    case RISM3D_GRID_G: return get(c.d_g, host, V * n) ? RISM3D_OK : RISM3D_CUDA_ERROR;
+    case RISM3D_GRID_H: return get(c.d_h, host, V * n) ? RISM3D_OK : RISM3D_CUDA_ERROR;
+    case RISM3D_GRID_T:
+    case RISM3D_GRID_C: {
+      std::vector<double> fr(n), h;
+      if (!get(c.d_t, host, V * n) || !get(c.d_fr, fr.data(), n)) return RISM3D_CUDA_ERROR;
+      for (size_t v = 0; v < V; ++v)
+        for (size_t j = 0; j < n; ++j) host[v * n + j] += c.qv[v] * c.cf_final * fr[j];
+      if (which == RISM3D_GRID_C) {
+        h.resize(V * n);
+        if (!get(c.d_h, h.data(), V * n)) return RISM3D_CUDA_ERROR;
+        for (size_t i = 0; i < V * n; ++i) host[i] = h[i] - host[i];
+      }
+      return RISM3D_OK;
+    }
+    case RISM3D_GRID_QV: {                                  // cal_qv.cu:20-27
+      std::vector<double> g(V * n);
+      if (!get(c.d_g, g.data(), V * n)) return RISM3D_CUDA_ERROR;
+      for (size_t j = 0; j < n; ++j) host[j] = 0.0;
+      for (size_t v = 0; v < V; ++v)
+        for (size_t j = 0; j < n; ++j) host[j] += g[v * n + j] * (c.rho[v] * c.qv[v]);
+      return RISM3D_OK;
+    }
+  }
+  c.err = "unknown grid id";
+  return RISM3D_BAD_INPUT;
+}
+
+}  // namespace rism3d
+
+static int alloc_state(Context &c) {
+  const size_t n = (size_t)c.n, V = (size_t)c.natv, P = (V + 1) / 2;
+  const bool mixed = c.prm.precision == RISM3D_MIXED;
+  auto A = [&](void **p, size_t bytes, const char *w) {
+    return cuda_ok(c, cudaMalloc(p, bytes), w);
+  };
+  bool ok = A((void **)&c.d_u, sizeof(double) * V * n, "alloc u") &&
+            A((void **)&c.d_U, sizeof(double) * V * n, "alloc U") &&
+            A((void **)&c.d_t, sizeof(double) * V * n, "alloc t") &&
+            A((void **)&c.d_Y, sizeof(double) * 2 * V * n, "alloc Y") &&
+            A((void **)&c.d_RP, sizeof(double) * 2 * V * n, "alloc RP") &&
+            A((void **)&c.d_buf, sizeof(double2) * P * n, "alloc buf") &&
+            A((void **)&c.d_h, sizeof(double) * V * n, "alloc h") &&
+            A((void **)&c.d_g, sizeof(double) * V * n, "alloc g") &&
+            A((void **)&c.d_obs, sizeof(double) * 64, "alloc obs");
+  if (ok && mixed)
+    ok = A((void **)&c.f_U, sizeof(float) * V * n, "alloc U32") &&
+         A((void **)&c.f_t, sizeof(float) * V * n, "alloc t32") &&
+         A((void **)&c.f_Y, sizeof(float) * 2 * V * n, "alloc Y32") &&
+         A((void **)&c.f_RP, sizeof(float) * 2 * V * n, "alloc RP32") &&
+         A((void **)&c.f_buf, sizeof(float2) * P * n, "alloc buf32");
+  if (!ok) return RISM3D_CUDA_ERROR;
+  // batched 3D plans over the site pairs; x is the fastest axis
+  int dims[3] = {c.nz, c.ny, c.nx};
+  if (!cufft_ok(c, cufftPlanMany(&c.plan64, 3, dims, nullptr, 1, (int)n, nullptr, 1, (int)n,
+                                 CUFFT_Z2Z, (int)P), "cufftPlanMany Z2Z"))
+    return RISM3D_CUFFT_ERROR;
+  if (mixed && !cufft_ok(c, cufftPlanMany(&c.plan32, 3, dims, nullptr, 1, (int)n, nullptr, 1,
+                                          (int)n, CUFFT_C2C, (int)P), "cufftPlanMany C2C"))
+    return RISM3D_CUFFT_ERROR;
+  c.plans_ok = true;
+  return RISM3D_OK;
+}
+
+extern "C" {
+
+int rism3d_create(const rism3d_params *p, rism3d_ctx **out) {
+  if (!p || !out) { g_create_err = "null argument"; return RISM3D_BAD_INPUT; }
+  *out = nullptr;
+  for (int d = 0; d < 3; ++d) {
+    if (p->grid[d] < 4 || p->grid[d] % 4 != 0 || p->grid[d] > 2048) {
+      g_create_err = "grid sizes must be multiples of 4 in [4, 2048] (half-shifted transform, fft3d.cu)";
+      return RISM3D_UNSUPPORTED_SHAPE;
+    }
+    if (!(p->box[d] > 0)) { g_create_err = "box must be positive"; return RISM3D_BAD_INPUT; }
+  }
+  if (p->closure != RISM3D_KH && p->closure != RISM3D_HNC) {
+    g_create_err = "Unexpected closure switch";
+    return RISM3D_BAD_INPUT;
+  }
+  if (p->maxstep < 1 || !(p->convergence > 0) || p->an2_count < 0) {
+    g_create_err = "bad iteration control";
+    return RISM3D_BAD_INPUT;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    g_create_err = "no CUDA device";
+    return RISM3D_NO_DEVICE;
+  }
+  if (p->device < 0 || p->device >= ndev) { g_create_err = "bad device ordinal"; return RISM3D_NO_DEVICE; }
+  rism3d_ctx *x = new (std::nothrow) rism3d_ctx;
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  c.prm = *p;
+  c.dev = p->device;
+  if (cudaSetDevice(c.dev) != cudaSuccess || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    g_create_err = "cannot initialise the CUDA device";
+    delete x;
+    return RISM3D_CUDA_ERROR;
+  }
+  c.nx = p->grid[0]; c.ny = p->grid[1]; c.nz = p->grid[2];
+  c.n = (long long)c.nx * c.ny * c.nz;
+  c.vol = p->box[0] * p->box[1] * p->box[2];             // cell.cc:9-14
+  c.dv = c.vol / (double)c.n;
+  for (int d = 0; d < 3; ++d) c.dr[d] = p->box[d] / p->grid[d];
+  bool ok = cuda_ok(c, cudaMalloc(&c.d_e, sizeof(double) * c.n), "alloc esr") &&
+            cuda_ok(c, cudaMalloc(&c.d_fr, sizeof(double) * c.n), "alloc fr") &&
+            cuda_ok(c, cudaMalloc(&c.d_fkh, sizeof(double2) * (c.n / 2)), "alloc fk") &&
+            cuda_ok(c, cudaMalloc(&c.d_tw, sizeof(double2) * (c.nx + c.ny + c.nz)), "alloc tw") &&
+            cuda_ok(c, cudaMalloc(&c.d_twf, sizeof(float2) * (c.nx + c.ny + c.nz)), "alloc tw") &&
+            cuda_ok(c, cudaMalloc(&c.d_state, sizeof(DevState)), "alloc state") &&
+            cuda_ok(c, cudaMalloc(&c.d_stage, sizeof(StageParams)), "alloc stage") &&
+            cuda_ok(c, cudaHostAlloc(&c.h_state, sizeof(DevState) * 4, cudaHostAllocDefault), "alloc pinned");
+  long long nb = (c.n + 255) / 256;
+  c.nred_blocks = (int)(nb < 148 * 8 ? nb : 148 * 8);
+  ok = ok && cuda_ok(c, cudaMalloc(&c.d_part, sizeof(double) * 64 * c.nred_blocks), "alloc partials");
+  for (Timer *t : {&c.tm_setup, &c.tm_iter, &c.tm_obs}) {
+    cudaEventCreate(&t->a);
+    cudaEventCreate(&t->b);
+  }
+  if (!ok || build_twiddles(c) != RISM3D_OK) {
+    g_create_err = c.err;
+    free_device(c);
+    cudaStreamDestroy(c.stream);
+    delete x;
+    return RISM3D_CUDA_ERROR;
+  }
+  *out = x;
+  return RISM3D_OK;
+}
+
+int rism3d_set_solvent(rism3d_ctx *x, int natv, const double *rho, const double *q,
+                       const double *sig, const double *eps, double temperature, double xt,
+                       int ntab, double dr, const double *xvv) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (natv < 1 || natv > kMaxSites) { c.err = "natv must be 1..8"; return RISM3D_UNSUPPORTED_SHAPE; }
+  if (!rho || !q || !sig || !eps || !xvv || ntab < 4 || !(dr > 0) || !(temperature > 0) || !(xt > 0)) {
+    c.err = "bad solvent arguments";
+    return RISM3D_BAD_INPUT;
+  }
+  for (int v = 0; v < natv; ++v)
+    if (!(rho[v] > 0)) { c.err = "solvent densities must be positive"; return RISM3D_BAD_INPUT; }
+  if (c.have_solvent && natv != c.natv) {
+    c.err = "solvent site count cannot change on a context";
+    return RISM3D_BAD_STATE;
+  }
+  c.natv = natv;
+  for (int v = 0; v < natv; ++v) { c.rho[v] = rho[v]; c.qv[v] = q[v]; c.sigv[v] = sig[v]; c.epsv[v] = eps[v]; }
+  c.temper = temperature; c.xt = xt; c.ntab = ntab; c.xdr = dr;
+  c.xvv_host.assign(xvv, xvv + (size_t)natv * natv * ntab);
+  if (!c.have_solvent) {
+    int rc = alloc_state(c);
+    if (rc != RISM3D_OK) return rc;
+  }
+  int rc = upload_chi(c);
+  if (rc != RISM3D_OK) return rc;
+  c.have_solvent = true;
+  c.have_solute = false;
+  c.solved = false;
+  return RISM3D_OK;
+}
+
+int rism3d_set_solute(rism3d_ctx *x, int natom, const double *sig, const double *eps,
+                      const double *q, const double *xyz) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (!c.have_solvent) { c.err = "set the solvent first"; return RISM3D_BAD_STATE; }
+  if (natom < 1 || !sig || !eps || !q || !xyz) { c.err = "bad solute arguments"; return RISM3D_BAD_INPUT; }
+  c.natom = natom;
+  c.sig.assign(sig, sig + natom);
+  c.eps.assign(eps, eps + natom);
+  c.q.assign(q, q + natom);
+  c.xyz.assign(xyz, xyz + 3 * (size_t)natom);
+  std::vector<double> pack((size_t)natom * 8, 0.0);
+  for (int i = 0; i < natom; ++i) {
+    double *a = &pack[(size_t)i * 8];
+    a[0] = xyz[3 * i]; a[1] = xyz[3 * i + 1]; a[2] = xyz[3 * i + 2];
+    a[3] = q[i]; a[4] = sig[i]; a[5] = eps[i];
+    if (!std::isfinite(a[0] + a[1] + a[2] + a[3] + a[4] + a[5]) || eps[i] < 0) {
+      c.err = "non-finite or negative solute parameter";
+      return RISM3D_BAD_INPUT;
+    }
+  }
+  if (c.d_atoms) cudaFree(c.d_atoms);
+  c.d_atoms = nullptr;
+  if (!cuda_ok(c, cudaMalloc(&c.d_atoms, sizeof(double) * pack.size()), "alloc atoms") ||
+      !cuda_ok(c, cudaMemcpyAsync(c.d_atoms, pack.data(), sizeof(double) * pack.size(),
+                                  cudaMemcpyHostToDevice, c.stream), "copy atoms"))
+    return RISM3D_CUDA_ERROR;
+  cudaEventRecord(c.tm_setup.a, c.stream);
+  int rc = compute_potentials(c);
+  cudaEventRecord(c.tm_setup.b, c.stream);
+  if (rc != RISM3D_OK) return rc;
+  if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "potentials")) return RISM3D_CUDA_ERROR;
+  c.have_solute = true;
+  c.solved = false;
+  c.have_forces = false;
+  return RISM3D_OK;
+}
+
+int rism3d_set_tuv(rism3d_ctx *x, const double *t) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  if (!c.have_solvent) { c.err = "set the solvent first"; return RISM3D_BAD_STATE; }
+  if (!t) c.t_init.clear();
+  else c.t_init.assign(t, t + (size_t)c.natv * c.n);
+  return RISM3D_OK;
+}
+
+int rism3d_solve(rism3d_ctx *x, int chargeup, rism3d_result *res) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (!c.have_solvent || !c.have_solute) { c.err = "solvent and solute must be set"; return RISM3D_BAD_STATE; }
+  if (chargeup < 0) { c.err = "chargeup must be >= 0"; return RISM3D_BAD_INPUT; }
+  c.res = rism3d_result{};
+  c.have_forces = false;
+  cudaEventRecord(c.tm_iter.a, c.stream);
+  int rc = run_solve(c, chargeup);
+  cudaEventRecord(c.tm_iter.b, c.stream);
+  if (rc != RISM3D_OK) return rc;
+  cudaEventRecord(c.tm_obs.a, c.stream);
+  rc = compute_observables(c);
+  if (rc == RISM3D_OK) rc = compute_atom_integrals(c, false);
+  cudaEventRecord(c.tm_obs.b, c.stream);
+  if (rc != RISM3D_OK) return rc;
+  if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "solve")) return RISM3D_CUDA_ERROR;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c.tm_setup.a, c.tm_setup.b); c.res.ms_setup = ms;
+  cudaEventElapsedTime(&ms, c.tm_iter.a, c.tm_iter.b); c.res.ms_iterate = ms;
+  cudaEventElapsedTime(&ms, c.tm_obs.a, c.tm_obs.b); c.res.ms_observe = ms;
+  c.solved = true;
+  if (res) *res = c.res;
+  if (c.res.status != RISM3D_OK) return c.res.status;
+  return RISM3D_OK;
+}
+
+int rism3d_euv(rism3d_ctx *x, double *euv) {
+  if (!x || !euv) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
+  std::copy(c.euv.begin(), c.euv.end(), euv);
+  return RISM3D_OK;
+}
+
+int rism3d_forces(rism3d_ctx *x, double *dulj, double *due) {
+  if (!x || !dulj || !due) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
+  if (!c.have_forces) {
+    int rc = compute_atom_integrals(c, true);
+    if (rc != RISM3D_OK) return rc;
+  }
+  std::copy(c.dulj.begin(), c.dulj.end(), dulj);
+  std::copy(c.due.begin(), c.due.end(), due);
+  return RISM3D_OK;
+}
+
+int rism3d_grad(rism3d_ctx *x, double *dq, double *dsig, double *deps, double *dR) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
+  return compute_adjoint(c, dq, dsig, deps, dR);
+}
+
+int rism3d_get_grid(rism3d_ctx *x, int which, double *host) {
+  if (!x || !host) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (!c.have_solute) { c.err = "no solute"; return RISM3D_BAD_STATE; }
+  return fetch_grid(c, which, host);
+}
+
+void rism3d_destroy(rism3d_ctx *x) {
+  if (!x) return;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  free_device(c);
+  for (Timer *t : {&c.tm_setup, &c.tm_iter, &c.tm_obs}) {
+    if (t->a) cudaEventDestroy(t->a);
+    if (t->b) cudaEventDestroy(t->b);
+  }
+  if (c.stream) cudaStreamDestroy(c.stream);
+  delete x;
+}
+
+const char *rism3d_last_error(const rism3d_ctx *x) {
+  if (!x) return g_create_err.c_str();
+  return x->c.err.c_str();
+}
+
+// ------------------------------------------------------------ file driven
+static std::string dir_of(const std::string &p) {
+  size_t s = p.rfind('/');
+  return s == std::string::npos ? std::string() : p.substr(0, s + 1);
+}
+
+int rism3d_initialize(rism3d_ctx **out, const char *control, const char *structure,
+                      const char *esp, const char *hs, int centering, int q0, int device,
+                      int precision) {
+  if (!out || !control) { g_create_err = "null argument"; return RISM3D_BAD_INPUT; }
+  *out = nullptr;
+  if ((esp && *esp) || (hs && *hs)) {
+    g_create_err = "ESP cube and RMDFT inputs are not supported by this build";
+    return RISM3D_BAD_INPUT;
+  }
+  io::ControlFile cf;
+  std::string err;
+  std::string st = structure ? structure : "";
+  if (!io::read_control(control, st, cf, err)) { g_create_err = err; return RISM3D_BAD_INPUT; }
+  std::string ctl = control;
+  std::string svpath = cf.fsolvent;
+  if (!svpath.empty() && svpath[0] != '/') {
+    // the reference opens the solvent path relative to the working directory
+    std::ifstream probe(svpath.c_str());
+    if (!probe) svpath = dir_of(ctl) + cf.fsolvent;
+  }
+  io::SolventFile sf;
+  if (!io::read_xvk(svpath, sf, err)) { g_create_err = err; return RISM3D_BAD_INPUT; }
+  rism3d_params p{};
+  for (int d = 0; d < 3; ++d) { p.grid[d] = cf.grid[d]; p.box[d] = cf.box[d]; }
+  p.closure = cf.closure; p.convergence = cf.conv; p.maxstep = cf.maxstep;
+  p.an2_count = cf.count; p.an2_m = cf.m; p.an2_mp = cf.mp;
+  p.precision = precision; p.device = device; p.verbose = 1;
+  rism3d_ctx *x = nullptr;
+  int rc = rism3d_create(&p, &x);
+  if (rc != RISM3D_OK) return rc;
+  Context &c = x->c;
+  c.outlist = cf.outlist; c.ksave = cf.ksave; c.zero = q0 != 0;
+  c.sig_in = cf.sig; c.eps_in = cf.eps; c.q_in = cf.q; c.xyz_in = cf.xyz;
+  std::string base = st.empty() ? ctl : st;                    // set_fname.cu:5-12
+  size_t dot = base.rfind('.');
+  c.fname = dot == std::string::npos ? base : base.substr(0, dot);
+  std::vector<double> xyz = cf.xyz, q = cf.q;
+  if (centering) io::centre(xyz, c.shift);                    // read_input.cu:80-82
+  if (q0) for (double &v : q) v = 0.0;                        // solute.cu:45-49
+  rc = rism3d_set_solvent(x, sf.natv, sf.rho.data(), sf.q.data(), sf.sig.data(), sf.eps.data(),
+                          sf.temper, sf.xt, sf.ntab, sf.dr, sf.xvv.data());
+  if (rc == RISM3D_OK)
+    rc = rism3d_set_solute(x, (int)q.size(), cf.sig.data(), cf.eps.data(), q.data(), xyz.data());
+  if (rc != RISM3D_OK) {
+    g_create_err = c.err;
+    rism3d_destroy(x);
+    return rc;
+  }
+  *out = x;
+  return RISM3D_OK;
+}
+
+int rism3d_iterate(rism3d_ctx *x, int chargeup) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  std::string tuv = c.fname + ".tuv";                          // iterate.cu:25-33
+  std::vector<double> t;
+  std::string warn;
+  if (io::read_tuv(tuv, c.prm.grid, c.natv, t, warn)) {
+    if (!warn.empty()) fprintf(stderr, "%s\n", warn.c_str());
+    if (t.size() == (size_t)c.natv * c.n) c.t_init = t;
+    chargeup = 0;
+  }
+  if (chargeup > 0) printf("Charge up %d\n", chargeup);
+  int rc = rism3d_solve(x, chargeup, nullptr);
+  c.t_init.clear();
+  if (rc == RISM3D_CUDA_ERROR || rc == RISM3D_CUFFT_ERROR || rc == RISM3D_BAD_STATE) return rc;
+  if (c.ksave != 0 && c.res.status == RISM3D_OK) {             // iterate.cu:64-71
+    std::vector<double> tt((size_t)c.natv * c.n);
+    if (fetch_grid(c, RISM3D_GRID_T, tt.data()) == RISM3D_OK)
+      io::write_tuv(tuv, c.prm.grid, c.natv, tt.data(), c.n);
+  }
+  return rc;
+}
+
+int rism3d_output(rism3d_ctx *x) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
+  std::string ol = c.outlist;
+  for (char &ch : ol) ch = (char)tolower(ch);                   // output.cu:8
+  auto has = [&](char k) { return ol.find(k) != std::string::npos; };
+  const size_t n = (size_t)c.n, V = (size_t)c.natv;
+  if (has('m')) {
+    io::XmuValues xv{};
+    xv.natv = c.natv; xv.closure = c.prm.closure;
+    for (int v = 0; v < c.natv; ++v) {
+      xv.sfec_sc[v] = c.res.sfec_sc[v];
+      xv.sfec_sc_hnc[v] = c.res.sfec_sc_hnc[v];
+      xv.sfec_gf[v] = c.res.sfec_gf[v];
+    }
+    xv.se = c.res.se; xv.se_lj = c.res.se_lj; xv.se_es = c.res.se_es;
+    xv.pmv_l = c.res.pmv; xv.pressure = c.res.pressure; xv.correction = c.res.correction;
+    if (!io::write_xmu(c.fname + (c.zero ? ".xmu0" : ".xmu"), xv)) { c.err = "cannot write .xmu"; return RISM3D_BAD_INPUT; }
+  }
+  if (has('d')) {
+    std::vector<double> a((size_t)c.natom * 3), b((size_t)c.natom * 3);
+    int rc = rism3d_forces(x, a.data(), b.data());
+    if (rc != RISM3D_OK) return rc;
+    io::write_gra(c.fname + ".gra", c.natom, a.data(), b.data());
+  }
+  std::vector<double> buf;
+  if (has('c')) {
+    buf.resize(V * n);
+    fetch_grid(c, RISM3D_GRID_C, buf.data());
+    io::write_grid_text(c.fname + ".cuv", c.prm.box, c.prm.grid, c.natom, c.q.data(), c.sig.data(),
+                        c.eps.data(), c.xyz.data(), c.natv, buf.data(), c.n);
+  }
+  if (has('g')) {
+    buf.resize(V * n);
+    fetch_grid(c, RISM3D_GRID_G, buf.data());
+    io::write_guv(c.fname + ".guv", c.natv, c.prm.grid, c.prm.box, c.shift, buf.data(), c.n);
+  }
+  if (has('h')) {
+    buf.resize(V * n);
+    fetch_grid(c, RISM3D_GRID_H, buf.data());
+    io::write_grid_text(c.fname + ".huv", c.prm.box, c.prm.grid, c.natom, c.q.data(), c.sig.data(),
+                        c.eps.data(), c.xyz.data(), c.natv, buf.data(), c.n);
+  }
+  if (has('e')) io::write_euv(c.fname + ".euv", c.natom, c.natv, c.euv.data());
+  if (has('q')) {
+    buf.resize(n);
+    fetch_grid(c, RISM3D_GRID_QV, buf.data());
+    for (double &v : buf) v *= c.dv;
+    io::write_qv(c.fname + ".qv", c.prm.grid, c.dr, buf.data(), c.n);
+  }
+  return RISM3D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,316 @@
+// Observables at convergence (reference: output.cu:6-62).
+//
+// k_observe: one FP64 pass over the grid gives, per site v, the KH, HNC and
+// GF excess-chemical-potential integrands and the PMV integral
+// (cal_exchem.cu:55-154, cal_pmv.cu:25-55) with h = Re h_OZ and
+// t = t_SR + q_v cf fr, c = h - t.  Block partials are reduced in a fixed
+// order, so the sums do not depend on scheduling.
+//
+// k_atom_integrals: SE per (site, atom) (cal_euv.cu:35-76) and the
+// cal_grad gradients (cal_grad.cu:51-145) for ALL atoms in one launch: one
+// atom per thread, grid points streamed through shared memory (the
+// reference launches one full-grid kernel + Thrust reductions per pair).
+#include <cmath>
+#include <vector>
+
+#include "rism3d_impl.h"
+
+namespace rism3d {
+namespace {
+
+constexpr int kThreads = 256;
+
+template <int V, int CLOS>
+__global__ void __launch_bounds__(kThreads)
+k_observe(long long n, const double *__restrict__ h, const double *__restrict__ t,
+          const double *__restrict__ fr, const StageParams *sp, double *part,
+          int nblocks) {
+  constexpr int NS = 4 * V;
+  __shared__ double red[kThreads / 32][NS];
+  double acc[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) acc[k] = 0.0;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const double f = fr[j];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const double hh = h[(size_t)v * n + j];
+      const double tt = t[(size_t)v * n + j] + sp->qcf[v] * f;
+      const double c = hh - tt;
+      const double hnc = hh * 0.5 * tt - c;                     // ehnc
+      const double gf = -(hh * 0.5 + 1.0) * c;                  // egf
+      const double kh = hh > 0.0 ? gf : hnc;                    // ekh
+      acc[4 * v + 0] += CLOS == 0 ? kh : hnc;
+      acc[4 * v + 1] += hnc;
+      acc[4 * v + 2] += gf;
+      acc[4 * v + 3] += c;                                      // pmv_cuv
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[k] = v;
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int k = 0; k < NS; ++k) red[wid][k] = acc[k];
+  __syncthreads();
+  for (int k = threadIdx.x; k < NS; k += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) s += red[w][k];
+    part[(size_t)k * nblocks + blockIdx.x] = s;
+  }
+}
+
+// out[k] = sum_b part[k][b], fixed order, one block per k.
+__global__ void k_reduce_rows(const double *part, int ncols, double *out) {
+  __shared__ double red[256];
+  const int k = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < ncols; b += blockDim.x) s += part[(size_t)k * ncols + b];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[k] = red[0];
+}
+
+struct SiteAll {
+  double sig[kMaxSites], eps[kMaxSites], q[kMaxSites], rho[kMaxSites];
+};
+
+constexpr int kAtomsPerBlock = 128;
+constexpr int kPtsTile = 128;
+
+// part layout: [chunk][atom][2V + 6]: SE_LJ[v], SE_ES[v] (rho_v applied),
+// grad LJ xyz, grad ES xyz (sum over v of rho_v * ...).
+template <int V>
+__global__ void __launch_bounds__(kAtomsPerBlock)
+k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
+                 const double *__restrict__ g, const double *__restrict__ atoms,
+                 int natom, SiteAll sv, double cc, long long chunk,
+                 double *part, int want_grad) {
+  constexpr int NA = 2 * V + 6;
+  __shared__ double px[kPtsTile], py[kPtsTile], pz[kPtsTile], pg[V][kPtsTile];
+  const long long n = (long long)nx * ny * nz;
+  const int ia = blockIdx.x * kAtomsPerBlock + threadIdx.x;
+  const bool live = ia < natom;
+  double X = 0, Y = 0, Z = 0, qu = 0, su = 0, eu = 0;
+  if (live) {
+    const double *a = atoms + 8 * (size_t)ia;
+    X = a[0]; Y = a[1]; Z = a[2]; qu = a[3]; su = a[4]; eu = a[5];
+  }
+  double sg[V], ep[V], qq[V], hs[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    sg[v] = (su + sv.sig[v]) * 0.5;          // cal_LJ.cu:28
+    ep[v] = sqrt(eu * sv.eps[v]);            // cal_LJ.cu:29
+    qq[v] = qu * sv.q[v] * cc;
+    hs[v] = sg[v] * 0.5;
+  }
+  double acc[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) acc[k] = 0.0;
+  const long long j0 = (long long)blockIdx.y * chunk;
+  const long long j1 = min(n, j0 + chunk);
+  for (long long base = j0; base < j1; base += kPtsTile) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < kPtsTile; i += blockDim.x) {
+      long long j = base + i;
+      if (j < j1) {
+        long long r = j / nx;
+        int ix = (int)(j - r * nx), iy = (int)(r % ny), iz = (int)(r / ny);
+        px[i] = (ix - nx / 2) * drx;       // cal_euv.cu:45-47
+        py[i] = (iy - ny / 2) * dry;
+        pz[i] = (iz - nz / 2) * drz;
+#pragma unroll
+        for (int v = 0; v < V; ++v) pg[v][i] = g[(size_t)v * n + j];
+      } else {
+        px[i] = py[i] = pz[i] = 1.0e30;
+#pragma unroll
+        for (int v = 0; v < V; ++v) pg[v][i] = 0.0;
+      }
+    }
+    __syncthreads();
+    if (!live) continue;
+    const int m = (int)min((long long)kPtsTile, j1 - base);
+    for (int i = 0; i < m; ++i) {
+      const double dx = px[i] - X, dy = py[i] - Y, dz = pz[i] - Z;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double r1 = sqrt(r2);
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        if (r1 < hs[v]) continue;            // cutoff r < sigma/2
+        const double gv = pg[v][i];
+        const double rs2i = sg[v] * sg[v] / r2;
+        const double rs6i = rs2i * rs2i * rs2i;
+        acc[v] += ep[v] * 4.0 * rs6i * (rs6i - 1.0) * gv;
+        acc[V + v] += qq[v] / r1 * gv;
+        if (want_grad) {
+          const double ulj = ep[v] * 24.0 * rs6i / r2 * (2.0 * rs6i - 1.0) * gv * sv.rho[v];
+          const double uco = qq[v] / (r2 * r1) * gv * sv.rho[v];
+          acc[2 * V + 0] += ulj * dx; acc[2 * V + 1] += ulj * dy; acc[2 * V + 2] += ulj * dz;
+          acc[2 * V + 3] += uco * dx; acc[2 * V + 4] += uco * dy; acc[2 * V + 5] += uco * dz;
+        }
+      }
+    }
+  }
+  if (live) {
+    double *o = part + ((size_t)blockIdx.y * natom + ia) * NA;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      o[v] = acc[v] * sv.rho[v];
+      o[V + v] = acc[V + v] * sv.rho[v];
+    }
+#pragma unroll
+    for (int k = 2 * V; k < NA; ++k) o[k] = acc[k];
+  }
+}
+
+// sum over chunks, fixed order: out[atom][k]
+__global__ void k_sum_chunks(const double *part, int nchunk, int natom, int na,
+                             double *out) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= natom * na) return;
+  double s = 0.0;
+  for (int c = 0; c < nchunk; ++c) s += part[(size_t)c * natom * na + idx];
+  out[idx] = s;
+}
+
+template <int V>
+int observe_v(Context &c) {
+  const int nb = c.nred_blocks;
+  StageParams sp{};
+  for (int v = 0; v < V; ++v) sp.qcf[v] = c.qv[v] * c.cf_final;
+  cudaMemcpyAsync(c.d_stage, &sp, sizeof(sp), cudaMemcpyHostToDevice, c.stream);
+  if (c.prm.closure == RISM3D_KH)
+    k_observe<V, 0><<<nb, kThreads, 0, c.stream>>>(c.n, c.d_h, c.d_t, c.d_fr, c.d_stage, c.d_part, nb);
+  else
+    k_observe<V, 1><<<nb, kThreads, 0, c.stream>>>(c.n, c.d_h, c.d_t, c.d_fr, c.d_stage, c.d_part, nb);
+  k_reduce_rows<<<4 * V, 256, 0, c.stream>>>(c.d_part, nb, c.d_obs);
+  std::vector<double> s(4 * V);
+  if (!cuda_ok(c, cudaMemcpyAsync(s.data(), c.d_obs, sizeof(double) * 4 * V, cudaMemcpyDeviceToHost, c.stream), "observe") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "observe"))
+    return RISM3D_CUDA_ERROR;
+  const double ibeta = kAvogadro * kBoltzmann * c.temper;   // output_xmu.cu:19
+  rism3d_result &r = c.res;
+  r.natv = V;
+  r.natom = c.natom;
+  r.sfe_sc = r.sfe_sc_hnc = r.sfe_gf = 0.0;
+  double cuv = 0.0;
+  for (int v = 0; v < V; ++v) {
+    r.sfec_sc[v] = ibeta * s[4 * v + 0] * c.rho[v] * c.dv;
+    r.sfec_sc_hnc[v] = ibeta * s[4 * v + 1] * c.rho[v] * c.dv;
+    r.sfec_gf[v] = ibeta * s[4 * v + 2] * c.rho[v] * c.dv;
+    r.sfe_sc += r.sfec_sc[v];
+    r.sfe_sc_hnc += r.sfec_sc_hnc[v];
+    r.sfe_gf += r.sfec_gf[v];
+    cuv += s[4 * v + 3] * c.rho[v];
+  }
+  cuv *= c.dv;
+  const double pmv = c.xt * (1.0 - cuv) * ibeta;             // cal_pmv.cu:18-19
+  double pres = 0.0;                                         // cal_pressure.cu
+  for (int v = 0; v < V; ++v) pres += c.rho[v];
+  pres *= 1.0e30 / kAvogadro;
+  pres = 0.5 * (pres + 1.0 / (c.xt * ibeta));
+  r.pmv = pmv * 1000.0;
+  r.pressure = ibeta * pres;
+  r.correction = -pres * pmv * ibeta;                        // output_xmu.cu:21
+  return RISM3D_OK;
+}
+
+template <int V>
+int atoms_v(Context &c, bool forces) {
+  constexpr int NA = 2 * V + 6;
+  const int A = c.natom;
+  const int tiles = (A + kAtomsPerBlock - 1) / kAtomsPerBlock;
+  // enough chunks to fill the GPU a few times over
+  int nchunk = (148 * 8 + tiles - 1) / tiles;
+  if (nchunk < 1) nchunk = 1;
+  long long chunk = (c.n + nchunk - 1) / nchunk;
+  chunk = ((chunk + kPtsTile - 1) / kPtsTile) * kPtsTile;
+  nchunk = (int)((c.n + chunk - 1) / chunk);
+  size_t need = (size_t)nchunk * A * NA + (size_t)A * NA;
+  if ((int)need > c.natom_part_cap) {
+    if (c.d_atom_part) cudaFree(c.d_atom_part);
+    if (!cuda_ok(c, cudaMalloc(&c.d_atom_part, sizeof(double) * need), "atom partials"))
+      return RISM3D_CUDA_ERROR;
+    c.natom_part_cap = (int)need;
+  }
+  SiteAll sv{};
+  for (int v = 0; v < V; ++v) {
+    sv.sig[v] = c.sigv[v]; sv.eps[v] = c.epsv[v]; sv.q[v] = c.qv[v]; sv.rho[v] = c.rho[v];
+  }
+  const double cc = kHartree * kBohr * kAvogadro;            // cal_euv.cu:39
+  dim3 grid(tiles, nchunk);
+  k_atom_integrals<V><<<grid, kAtomsPerBlock, 0, c.stream>>>(
+      c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, A, sv, cc,
+      chunk, c.d_atom_part, forces ? 1 : 0);
+  double *sum = c.d_atom_part + (size_t)nchunk * A * NA;
+  k_sum_chunks<<<(A * NA + 255) / 256, 256, 0, c.stream>>>(c.d_atom_part, nchunk, A, NA, sum);
+  std::vector<double> h((size_t)A * NA);
+  if (!cuda_ok(c, cudaGetLastError(), "atom integrals") ||
+      !cuda_ok(c, cudaMemcpyAsync(h.data(), sum, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream), "atom integrals") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "atom integrals"))
+    return RISM3D_CUDA_ERROR;
+  c.euv.assign((size_t)2 * V * A, 0.0);
+  double slj = 0.0, ses = 0.0;
+  for (int u = 0; u < A; ++u)
+    for (int v = 0; v < V; ++v) {
+      double lj = h[(size_t)u * NA + v] * c.dv, es = h[(size_t)u * NA + V + v] * c.dv;
+      c.euv[(size_t)A * v + u] = lj;                         // cal_euv.cu:28-29
+      c.euv[(size_t)V * A + (size_t)A * v + u] = es;
+    }
+  for (size_t i = 0; i < (size_t)V * A; ++i) slj += c.euv[i];
+  for (size_t i = (size_t)V * A; i < (size_t)2 * V * A; ++i) ses += c.euv[i];
+  c.res.se_lj = slj;
+  c.res.se_es = ses;
+  c.res.se = slj + ses;
+  if (forces) {
+    c.dulj.assign((size_t)A * 3, 0.0);
+    c.due.assign((size_t)A * 3, 0.0);
+    for (int u = 0; u < A; ++u)
+      for (int k = 0; k < 3; ++k) {
+        c.dulj[(size_t)u * 3 + k] = h[(size_t)u * NA + 2 * V + k] * c.dv;
+        c.due[(size_t)u * 3 + k] = h[(size_t)u * NA + 2 * V + 3 + k] * c.dv;
+      }
+    c.have_forces = true;
+  }
+  return RISM3D_OK;
+}
+
+}  // namespace
+
+int compute_observables(Context &c) {
+  switch (c.natv) {
+    case 1: return observe_v<1>(c);
+    case 2: return observe_v<2>(c);
+    case 3: return observe_v<3>(c);
+    case 4: return observe_v<4>(c);
+    case 5: return observe_v<5>(c);
+    case 6: return observe_v<6>(c);
+    case 7: return observe_v<7>(c);
+    case 8: return observe_v<8>(c);
+  }
+  return RISM3D_UNSUPPORTED_SHAPE;
+}
+
+int compute_atom_integrals(Context &c, bool forces) {
+  switch (c.natv) {
+    case 1: return atoms_v<1>(c, forces);
+    case 2: return atoms_v<2>(c, forces);
+    case 3: return atoms_v<3>(c, forces);
+    case 4: return atoms_v<4>(c, forces);
+    case 5: return atoms_v<5>(c, forces);
+    case 6: return atoms_v<6>(c, forces);
+    case 7: return atoms_v<7>(c, forces);
+    case 8: return atoms_v<8>(c, forces);
+  }
+  return RISM3D_UNSUPPORTED_SHAPE;
+}
+
+}  // namespace rism3d

@@ -1,0 +1,158 @@
+// Internal declarations of the B200 3D-RISM solver (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <string>
+#include <vector>
+
+#include "rism3d_b200.h"
+
+namespace rism3d {
+
+constexpr int kMaxSites = RISM3D_MAX_SITES;
+
+// Physical constants, the same values as the reference (physical.h:4-17).
+constexpr double kAvogadro = 6.02214076e23;
+constexpr double kBohr = 0.5291771500001;         // Angstrom
+constexpr double kBoltzmann = 1.380649e-23;       // J/K
+constexpr double kHartree = 4.359744722207185e-18;
+constexpr double kPi = 3.14159265358979323846;
+
+// Device-resident iteration control.  Written only by k_finalize (one
+// thread); read by every pass of the next iteration, so the loop runs with
+// no host round trip.  Mirrors the host-side state of AN2
+// (anderson.h:16-37) and RISM3D::iterate (iterate.cu:49-73).
+struct DevState {
+  int done;        // 0 running, 1 converged, 2 diverged, 3 maxstep reached
+  int after_done;  // finalize calls since `done` was set
+  int iter;        // iterations completed in this run
+  int mode;        // update the next pass A applies: 0 none, 1 Picard, 2 AN2
+  int upd_slot;    // history slot written by that update
+  int binary;      // AN2 ping-pong bit for the following update
+  int count;       // Picard warm-up steps left
+  int maxstep;
+  double conv;
+  double m, mp;    // AN2 mixing factor and bias
+  double s1, s2;   // AN2 coefficients for the next update
+  double rms;
+  double sums[6];  // sum R^2, c0, c1, a00, a01, a11 of the last pass R
+};
+
+// Per charge-up stage constants, read by the kernels through a pointer so
+// that one captured iteration graph serves every stage.
+struct StageParams {
+  double qcf[kMaxSites];   // q_v * cf
+  double irho[kMaxSites];  // 1 / rho_v (AN2 weights, anderson.cu:28-31)
+};
+
+// Natural-spline coefficients of chi_ab(k) on the uniform knots
+// k_i = dk (i+1): for knot i and pair ab, {y, c0, c1, c2}
+// (spline.cc:36-42, splint.cc:18-19).
+struct ChiTable {
+  int ntab = 0;
+  double dk = 0.0;
+  double *d_coef = nullptr;  // [ntab][natv*natv][4]
+};
+
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr;
+};
+
+struct Context {
+  rism3d_params prm{};
+  std::string err;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+
+  // cell (cell.cc:8-22)
+  int nx = 0, ny = 0, nz = 0;
+  long long n = 0;
+  double vol = 0, dv = 0, dr[3] = {0, 0, 0};
+
+  // solvent
+  int natv = 0;
+  double rho[kMaxSites], qv[kMaxSites], sigv[kMaxSites], epsv[kMaxSites];
+  double temper = 0, xt = 0;
+  bool have_solvent = false;
+  ChiTable chi;
+  std::vector<double> xvv_host;
+  int ntab = 0;
+  double xdr = 0;
+
+  // solute
+  int natom = 0;
+  std::vector<double> sig, eps, q, xyz;
+  bool have_solute = false;
+
+  // device grids
+  double *d_u = nullptr;     // [V][N] beta u_LJ
+  double *d_e = nullptr;     // [N]   beta sum q/r
+  double *d_fr = nullptr;    // [N]   beta long-range part
+  double2 *d_fkh = nullptr;  // [N/2] beta fk on the owner half of k space
+  double *d_atoms = nullptr; // [A][8] x y z q sig eps pad
+  double2 *d_tw = nullptr;   // twiddle rows: [nx] [ny] [nz] exp(-i pi x/n)
+  float2 *d_twf = nullptr;
+
+  // FP64 iteration state
+  double *d_U = nullptr;     // [V][N] short-range potential of the stage
+  double *d_t = nullptr;     // [V][N] t_SR = t - q cf fr
+  double *d_Y = nullptr;     // [2][V][N] history t + m R
+  double *d_RP = nullptr;    // [2][V][N] history R
+  double2 *d_buf = nullptr;  // [P][N] packed site pairs (FFT in place)
+  double *d_h = nullptr;     // [V][N] final h (snapshot)
+  double *d_g = nullptr;     // [V][N] final g
+  // FP32 iteration state (MIXED)
+  float *f_U = nullptr, *f_t = nullptr, *f_Y = nullptr, *f_RP = nullptr;
+  float2 *f_buf = nullptr;
+
+  double *d_part = nullptr;  // reduction partials
+  int nred_blocks = 0;
+  DevState *d_state = nullptr;
+  DevState *h_state = nullptr;  // pinned mirror
+  StageParams *d_stage = nullptr;
+  double *d_obs = nullptr;      // observables scratch
+  double *d_atom_part = nullptr;
+  int natom_part_cap = 0;
+
+  cufftHandle plan64 = 0, plan32 = 0;
+  bool plans_ok = false;
+
+  // restart guess
+  std::vector<double> t_init;
+
+  // results
+  bool solved = false;
+  double cf_final = 1.0;
+  rism3d_result res{};
+  std::vector<double> euv;       // [2][V][A] (x dv)
+  std::vector<double> dulj, due; // [A][3] (x dv)
+  bool have_forces = false;
+
+  // file-driven mode (rism3d_initialize)
+  std::string outlist, fname, fsolvent, control_dir;
+  int ksave = 0;
+  bool zero = false;
+  double shift[3] = {0, 0, 0};
+  std::vector<double> sig_in, eps_in, q_in, xyz_in;  // as read (pre-shift)
+
+  Timer tm_setup, tm_iter, tm_obs;
+};
+
+// ---- kernels/launchers (implemented in the .cu files) ----
+int build_twiddles(Context &c);
+int compute_potentials(Context &c);               // potential.cu
+int upload_chi(Context &c);                       // solver.cu
+int run_solve(Context &c, int chargeup);          // solver.cu
+int compute_observables(Context &c);              // observe.cu
+int compute_atom_integrals(Context &c, bool forces);  // observe.cu
+int compute_adjoint(Context &c, double *dq, double *dsig, double *deps,
+                    double *dR);                  // adjoint.cu
+int fetch_grid(Context &c, int which, double *host);
+void free_device(Context &c);
+
+bool cuda_ok(Context &c, cudaError_t e, const char *what);
+bool cufft_ok(Context &c, cufftResult r, const char *what);
+
+}  // namespace rism3d

@@ -1,0 +1,753 @@
+// The 3D-RISM fixed-point iteration (reference: iterate.cu:6-90,
+// calculate.cu:4-58, calculate_cuda.cu:1-66, fft3d.cu:4-94, cal_rms.cu,
+// anderson.cu:13-112, anderson_cuda.cu:1-66), re-designed around three
+// streaming passes and two cuFFT transforms per iteration:
+//
+//   pass A  (k_pass_a)   residual of the previous cycle + AN2/Picard update
+//                        + closure + c_SR + forward pre-twiddle; two real
+//                        sites are packed into one complex grid
+//   FFT forward          cuFFT C2C/Z2Z, in place, one transform per site pair
+//   pass K  (k_kspace)   unpack the pair (F(-k) = conj F(k)), post-twiddle,
+//                        minus the long-range fk, OZ site product with chi
+//                        spline-evaluated at |k|, repack for the inverse
+//   FFT inverse
+//   pass R  (k_pass_r)   post-twiddle, closure, residual R = h + 1 - g,
+//                        FP64 block sums of R^2 and the five AN2 Gram terms
+//   finalize (k_finalize) fixed-order reduction of the block sums, rms,
+//                        convergence / divergence / maxstep decision, 2x2
+//                        AN2 solve -- all on the device, no host sync.
+//
+// The state variable is the short-range indirect correlation
+// t_SR = t - q_v cf fr.  The closure exponent -u - q cf e + t equals
+// -U_SR + t_SR with U_SR = u + q cf (e - fr), and c_SR = g - 1 - t + q cf fr
+// = g - 1 - t_SR, so the long-range Coulomb terms never enter the passes.
+// The AN2 history stores Y_i = tp_i + m rp_i and RP_i = rp_i: the reference
+// update u + m(v - u) (anderson_cuda.cu:16-22) is algebraically
+// y + s1 (Y_0 - y) + s2 (Y_1 - y) with y = t + m R.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "rism3d_impl.h"
+
+namespace rism3d {
+
+template <typename T> struct Cx;
+template <> struct Cx<double> { typedef double2 t; };
+template <> struct Cx<float> { typedef float2 t; };
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <typename T>
+struct IterArgs {
+  long long n;
+  int nx, ny, nz;
+  typename Cx<T>::t *buf;   // [P][N]
+  T *t, *U, *Y, *RP;        // t, U: [V][N]; Y, RP: [2][V][N]
+  double *hout, *gout;      // final snapshot, [V][N] (may be null)
+  const typename Cx<T>::t *tw;  // px[nx] py[ny] pz[nz]
+  double invvol, dv;
+  const double2 *fkh;       // [N/2]
+  const double *chi;        // [ntab][V*V][4]
+  int ntab;
+  double dk;
+  double bx, by, bz;
+  DevState *st;
+  const StageParams *sp;
+  double *part;
+  int nblocks;
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C> __device__ __forceinline__ C mk(double x, double y);
+template <> __device__ __forceinline__ double2 mk<double2>(double x, double y) {
+  return make_double2(x, y);
+}
+template <> __device__ __forceinline__ float2 mk<float2>(double x, double y) {
+  return make_float2((float)x, (float)y);
+}
+
+__device__ __forceinline__ double fexp(double x) { return exp(x); }
+__device__ __forceinline__ float fexp(float x) { return expf(x); }
+
+// calculate_cuda.cu:1-20: KH g = 1 + x (x >= 0) or e^x; HNC g = e^x.
+template <int CLOS, typename T>
+__device__ __forceinline__ T closure(T x) {
+  if (CLOS == 0) return x >= T(0) ? T(1) + x : fexp(x);
+  return fexp(x);
+}
+
+// Point index -> (ix, iy, iz), +-1 checkerboard dir = (-1)^(ix+iy+iz)
+// (set_ir, fft3d.cu:86-94) and dkf = exp(-i pi sum x_d/n_d)
+// (set_kf, fft3d.cu:71-83) as a product of three per-axis phases.
+template <typename C>
+__device__ __forceinline__ void point_phase(long long j, int nx, int ny,
+                                            const C *tw, int &ix, int &iy,
+                                            int &iz, int &dir, C &dkf) {
+  long long r = j / nx;
+  ix = (int)(j - r * nx);
+  iy = (int)(r % ny);
+  iz = (int)(r / ny);
+  dir = ((ix + iy + iz) & 1) ? -1 : 1;
+  dkf = cmul(cmul(tw[ix], tw[nx + iy]), tw[nx + ny + iz]);
+}
+
+// ---------------------------------------------------------------- pass A
+template <typename T, int V, int CLOS>
+__global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a) {
+  typedef typename Cx<T>::t C;
+  constexpr int P = (V + 1) / 2;
+  const DevState *st = a.st;
+  const int done = st->done;
+  if (done && st->after_done > 0) return;     // past the snapshot: idle
+  const int mode = st->mode;
+  const int slot = st->upd_slot;
+  const T s1 = (T)st->s1, s2 = (T)st->s2, m = (T)st->m;
+  const long long n = a.n;
+  const bool need_h = (mode != 0) || done;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    int ix, iy, iz, dir;
+    C dkf;
+    point_phase(j, a.nx, a.ny, a.tw, ix, iy, iz, dir, dkf);
+    T h[V];
+    if (need_h) {
+      // inverse post-twiddle (timekb, fft3d.cu:52-60): (1/V) dir conj(dkf)
+      const T sc = (T)a.invvol * (T)dir;
+      C w = mk<C>(dkf.x * sc, -dkf.y * sc);
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        C z = cmul(a.buf[(size_t)p * n + j], w);
+        h[2 * p] = z.x;
+        if (2 * p + 1 < V) h[2 * p + 1] = z.y;
+      }
+    }
+    T cc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const size_t iv = (size_t)v * n + j;
+      const T t = a.t[iv];
+      const T U = a.U[iv];
+      T tn = t;
+      if (need_h) {
+        const T gold = closure<CLOS>(t - U);
+        const T R = h[v] + T(1) - gold;          // tr, calculate_cuda.cu:64
+        if (done) {
+          if (a.hout) { a.hout[iv] = (double)h[v]; a.gout[iv] = (double)gold; }
+        }
+        if (mode == 1) {                         // newdt0 (Picard)
+          a.Y[(size_t)slot * V * n + iv] = t + m * R;
+          a.RP[(size_t)slot * V * n + iv] = R;
+          tn = t + R;
+        } else if (mode == 2) {                  // newdt (AN2)
+          const T y = t + m * R;
+          const T y0 = a.Y[iv];
+          const T y1 = a.Y[(size_t)V * n + iv];
+          tn = y + s1 * (y0 - y) + s2 * (y1 - y);
+          a.Y[(size_t)slot * V * n + iv] = y;
+          a.RP[(size_t)slot * V * n + iv] = R;
+        }
+        if (mode != 0 && (!done || done == 3)) a.t[iv] = tn;
+      }
+      // closure + c_SR (kh/hnc + trm1mt, calculate_cuda.cu:1-29)
+      const T g = closure<CLOS>(tn - U);
+      cc[v] = g - T(1) - tn;
+    }
+    if (done) continue;
+    // forward pre-twiddle (timekf, fft3d.cu:41-49): dir * dkf * (c_a + i c_b)
+    const C wf = mk<C>(dkf.x * dir, dkf.y * dir);
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      C z;
+      z.x = cc[2 * p];
+      z.y = (2 * p + 1 < V) ? cc[2 * p + 1] : T(0);
+      a.buf[(size_t)p * n + j] = cmul(z, wf);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- pass K
+template <typename T, int V>
+__global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a) {
+  typedef typename Cx<T>::t C;
+  constexpr int P = (V + 1) / 2;
+  if (a.st->done) return;
+  const long long n = a.n, nh = n / 2;
+  const StageParams *sp = a.sp;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nh;
+       j += (long long)gridDim.x * blockDim.x) {
+    const long long jm = n - 1 - j;             // k(jm) = -k(j)
+    long long r = j / a.nx;
+    const int ix = (int)(j - r * a.nx);
+    const int iy = (int)(r % a.ny), iz = (int)(r / a.ny);
+    const int dir = ((ix + iy + iz) & 1) ? -1 : 1;
+    // set_g (initialize_g.cu:58-62)
+    const double kx = 2.0 * kPi * (ix - a.nx / 2.0 + 0.5) / a.bx;
+    const double ky = 2.0 * kPi * (iy - a.ny / 2.0 + 0.5) / a.by;
+    const double kz = 2.0 * kPi * (iz - a.nz / 2.0 + 0.5) / a.bz;
+    const double kk = sqrt(kx * kx + ky * ky + kz * kz);
+    const double2 fk = a.fkh[j];
+    // unpack the site pairs and finish the forward transform
+    // (timeirvol * dv, fft3d.cu:32) and subtract q cf fk (mqvfk)
+    C F[V];
+    const T sc = (T)(a.dv * 0.5 * dir);
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const C y = a.buf[(size_t)p * n + j];
+      const C ym = a.buf[(size_t)p * n + jm];
+      const double qa = sp->qcf[2 * p];
+      F[2 * p] = mk<C>(sc * (y.x - ym.x) - qa * fk.x, sc * (y.y + ym.y) - qa * fk.y);
+      if (2 * p + 1 < V) {
+        const double qb = sp->qcf[2 * p + 1];
+        F[2 * p + 1] = mk<C>(sc * (y.y - ym.y) - qb * fk.x, -sc * (y.x + ym.x) - qb * fk.y);
+      }
+    }
+    // chi_ab(|k|): natural spline on knots k_i = dk (i+1), bisection
+    // semantics of splint.cc:9-16 reproduced on the uniform knots
+    int k0 = (int)(kk / a.dk) - 1;
+    k0 = k0 < 0 ? 0 : (k0 > a.ntab - 2 ? a.ntab - 2 : k0);
+    while (k0 < a.ntab - 2 && a.dk * (k0 + 2) <= kk) ++k0;
+    while (k0 > 0 && a.dk * (k0 + 1) > kk) --k0;
+    const double tt = kk - a.dk * (k0 + 1);
+    const double *cf = a.chi + (size_t)k0 * V * V * 4;
+    C H[V];
+#pragma unroll
+    for (int va = 0; va < V; ++va) {
+      T hr = 0, hi = 0;
+#pragma unroll
+      for (int vb = 0; vb < V; ++vb) {
+        const double *q = cf + (va * V + vb) * 4;
+        const T x = (T)(((q[3] * tt + q[2]) * tt + q[1]) * tt + q[0]);
+        hr += F[vb].x * x;                       // oz, calculate_cuda.cu:44-58
+        hi += F[vb].y * x;
+      }
+      H[va] = mk<C>(hr, hi);
+    }
+    // repack for the inverse: dir (h_a + i h_b) at k and its mirror
+    // (timeirvol before the inverse, fft3d.cu:34)
+    const T d = (T)dir;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const C ha = H[2 * p];
+      const C hb = (2 * p + 1 < V) ? H[2 * p + 1] : mk<C>(0.0, 0.0);
+      a.buf[(size_t)p * n + j] = mk<C>(d * (ha.x - hb.y), d * (ha.y + hb.x));
+      a.buf[(size_t)p * n + jm] = mk<C>(-d * (ha.x + hb.y), -d * (hb.x - ha.y));
+    }
+  }
+}
+
+// ---------------------------------------------------------------- pass R
+template <typename T, int V, int CLOS>
+__global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a) {
+  typedef typename Cx<T>::t C;
+  constexpr int P = (V + 1) / 2;
+  __shared__ double red[kThreads / 32][6];
+  const DevState *st = a.st;
+  if (st->done) return;
+  const bool gram = st->count <= 0;
+  const long long n = a.n;
+  const StageParams *sp = a.sp;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    int ix, iy, iz, dir;
+    C dkf;
+    point_phase(j, a.nx, a.ny, a.tw, ix, iy, iz, dir, dkf);
+    const T sc = (T)a.invvol * (T)dir;
+    const C w = mk<C>(dkf.x * sc, -dkf.y * sc);
+    T h[V];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      C z = cmul(a.buf[(size_t)p * n + j], w);
+      h[2 * p] = z.x;
+      if (2 * p + 1 < V) h[2 * p + 1] = z.y;
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const size_t iv = (size_t)v * n + j;
+      const T g = closure<CLOS>(a.t[iv] - a.U[iv]);
+      const double R = (double)(h[v] + T(1) - g);
+      acc[0] += R * R;                          // cal_rms.cu:18
+      if (gram) {                               // theta30, anderson_cuda.cu:33-39
+        const double w8 = sp->irho[v];
+        const double d0 = R - (double)a.RP[iv];
+        const double d1 = R - (double)a.RP[(size_t)V * n + iv];
+        acc[1] += w8 * R * d0;
+        acc[2] += w8 * R * d1;
+        acc[3] += w8 * d0 * d0;
+        acc[4] += w8 * d0 * d1;
+        acc[5] += w8 * d1 * d1;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[k] = v;
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k) red[wid][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) s += red[w][threadIdx.x];
+    a.part[(size_t)threadIdx.x * a.nblocks + blockIdx.x] = s;
+  }
+}
+
+// ------------------------------------------------------------- finalize
+// Fixed-order reduction of the pass-R block sums, then the host logic of
+// iterate.cu:52-62 and AN2::calculate (anderson.cu:35-63) on one thread.
+__global__ void k_finalize(DevState *st, const double *part, int nblocks,
+                           double nv_points) {
+  __shared__ double red[6][256];
+  if (st->done) {
+    if (threadIdx.x == 0) st->after_done += 1;
+    return;
+  }
+  for (int k = 0; k < 6; ++k) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += part[(size_t)k * nblocks + b];
+    red[k][threadIdx.x] = s;
+  }
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int k = 0; k < 6; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  for (int k = 0; k < 6; ++k) st->sums[k] = red[k][0];
+  st->iter += 1;
+  const double rms = sqrt(red[0][0] / nv_points);
+  st->rms = rms;
+  if (!isfinite(rms)) { st->done = 2; st->mode = 0; return; }  // iterate.cu:54-57
+  if (rms <= st->conv) { st->done = 1; st->mode = 0; return; } // :58-59
+  if (st->count > 0) {                                         // anderson.cu:43-49
+    st->count -= 1;
+    st->mode = 1;
+  } else {                                                     // anderson.cu:50-61
+    // [[a00 a01][a01 a11]] x = [c0 c1], eliminated as leg() does (:87-112)
+    double a00 = red[3][0], a01 = red[4][0], a11 = red[5][0];
+    double c0 = red[1][0], c1 = red[2][0];
+    double p = a00;
+    double a01n = a01 / p;
+    double r = c0 / p;
+    double a11n = a11 - a01 * a01n;
+    double c1n = c1 - a01 * r;
+    double x1 = c1n / a11n;
+    double x0 = r - a01n * x1;
+    st->s1 = x0 + st->mp * ((st->binary == 0) ? 0.0 : 1.0);
+    st->s2 = x1 + st->mp * ((st->binary == 0) ? 1.0 : 0.0);
+    st->mode = 2;
+  }
+  st->upd_slot = st->binary;
+  st->binary = (st->binary == 0) ? 1 : 0;
+  if (st->iter >= st->maxstep) st->done = 3;   // iterate.cu:51 loop bound
+}
+
+// U_SR = u_v + q_v cf esr for a charge-up stage (FP64 and FP32 copies).
+__global__ void k_stage_u(long long n, int nv, const double *u,
+                          const double *esr, const StageParams *sp, double *U,
+                          float *Uf) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const double e = esr[j];
+    for (int v = 0; v < nv; ++v) {
+      double x = u[(size_t)v * n + j] + sp->qcf[v] * e;
+      U[(size_t)v * n + j] = x;
+      if (Uf) Uf[(size_t)v * n + j] = (float)x;
+    }
+  }
+}
+
+// t_SR from an absolute restart t (read_tuv.cu) or zero (initialize_tuv.cu:
+// t = q fr  <=>  t_SR = 0; charge-up start t = 0 with cf = 0 <=> t_SR = 0).
+__global__ void k_init_t(long long n, int nv, const double *tabs,
+                         const double *fr, const StageParams *sp, double *t) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x)
+    for (int v = 0; v < nv; ++v)
+      t[(size_t)v * n + j] = tabs ? tabs[(size_t)v * n + j] - sp->qcf[v] * fr[j] : 0.0;
+}
+
+// Charge-up step (add_tuv.cu): the absolute t gains q cuf fr, so t_SR is
+// unchanged while the stored history tp_i (absolute in the reference) must
+// be re-expressed in the new stage's short-range frame: Y_i -= q cuf fr.
+template <typename T>
+__global__ void k_shift_history(long long n, int nv, const double *fr,
+                                const StageParams *sp_step, T *Y) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x)
+    for (int s = 0; s < 2; ++s)
+      for (int v = 0; v < nv; ++v) {
+        size_t i = ((size_t)s * nv + v) * n + j;
+        Y[i] = (T)((double)Y[i] - sp_step->qcf[v] * fr[j]);
+      }
+}
+
+template <typename A, typename B>
+__global__ void k_convert(long long n, const A *src, B *dst) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x)
+    dst[j] = (B)src[j];
+}
+
+int grid_blocks(long long work) {
+  long long b = (work + kThreads - 1) / kThreads;
+  const long long cap = 148LL * 16;   // 148 SMs x 16 resident 256-thread blocks
+  return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+template <typename T, int V, int CLOS>
+void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
+  int ba = grid_blocks(a.n), bk = grid_blocks(a.n / 2);
+  k_pass_a<T, V, CLOS><<<ba, kThreads, 0, c.stream>>>(a);
+  typedef typename Cx<T>::t C;
+  if (sizeof(T) == 8) {
+    cufftExecZ2Z(plan, (cufftDoubleComplex *)a.buf, (cufftDoubleComplex *)a.buf, CUFFT_FORWARD);
+  } else {
+    cufftExecC2C(plan, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_FORWARD);
+  }
+  k_kspace<T, V><<<bk, kThreads, 0, c.stream>>>(a);
+  if (sizeof(T) == 8) {
+    cufftExecZ2Z(plan, (cufftDoubleComplex *)a.buf, (cufftDoubleComplex *)a.buf, CUFFT_INVERSE);
+  } else {
+    cufftExecC2C(plan, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
+  }
+  k_pass_r<T, V, CLOS><<<a.nblocks, kThreads, 0, c.stream>>>(a);
+  k_finalize<<<1, 256, 0, c.stream>>>(a.st, a.part, a.nblocks, (double)a.n * V);
+  (void)sizeof(C);
+}
+
+template <typename T>
+IterArgs<T> make_args(Context &c, bool fp64) {
+  IterArgs<T> a{};
+  a.n = c.n; a.nx = c.nx; a.ny = c.ny; a.nz = c.nz;
+  a.invvol = 1.0 / c.vol; a.dv = c.dv;
+  a.fkh = c.d_fkh; a.chi = c.chi.d_coef; a.ntab = c.chi.ntab; a.dk = c.chi.dk;
+  a.bx = c.prm.box[0]; a.by = c.prm.box[1]; a.bz = c.prm.box[2];
+  a.st = c.d_state; a.sp = c.d_stage; a.part = c.d_part; a.nblocks = c.nred_blocks;
+  (void)fp64;
+  return a;
+}
+
+struct Loop {
+  cudaGraphExec_t exec = nullptr;
+  bool graph = false;
+};
+
+// One captured iteration per precision; falls back to direct launches if
+// capture of the cuFFT calls is refused.
+template <typename T, int V, int CLOS>
+int capture(Context &c, const IterArgs<T> &a, cufftHandle plan, Loop &L) {
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    L.graph = false;
+    return RISM3D_OK;
+  }
+  launch_iteration<T, V, CLOS>(c, a, plan);
+  cudaError_t e = cudaStreamEndCapture(c.stream, &g);
+  if (e != cudaSuccess || !g) {
+    cudaGetLastError();
+    L.graph = false;
+    return RISM3D_OK;
+  }
+  e = cudaGraphInstantiate(&L.exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    L.exec = nullptr;
+    L.graph = false;
+    return RISM3D_OK;
+  }
+  L.graph = true;
+  return RISM3D_OK;
+}
+
+template <typename T, int V, int CLOS>
+int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
+                  typename Cx<T>::t *buf, bool snapshot, double conv,
+                  int max_iter, bool watch_stagnation, int &iters_out) {
+  IterArgs<T> a = make_args<T>(c, sizeof(T) == 8);
+  a.buf = buf; a.t = t; a.U = U; a.Y = Y; a.RP = RP;
+  a.hout = snapshot ? c.d_h : nullptr;
+  a.gout = snapshot ? c.d_g : nullptr;
+  a.tw = (const typename Cx<T>::t *)(sizeof(T) == 8 ? (void *)c.d_tw : (void *)c.d_twf);
+  // reset the per-run control words; AN2 count/binary persist
+  DevState hs;
+  if (!cuda_ok(c, cudaMemcpyAsync(&hs, c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream), "state read") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "sync"))
+    return RISM3D_CUDA_ERROR;
+  hs.done = 0; hs.after_done = 0; hs.iter = 0; hs.mode = 0;
+  hs.conv = conv; hs.maxstep = max_iter;
+  if (!cuda_ok(c, cudaMemcpyAsync(c.d_state, &hs, sizeof(DevState), cudaMemcpyHostToDevice, c.stream), "state write"))
+    return RISM3D_CUDA_ERROR;
+  if (!cufft_ok(c, cufftSetStream(plan, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
+  Loop L;
+  capture<T, V, CLOS>(c, a, plan, L);
+  const int kRing = 4, kLag = 2;
+  cudaEvent_t ev[kRing];
+  for (int i = 0; i < kRing; ++i) cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+  double best = 1e300;
+  int since_best = 0, launched = 0, status = RISM3D_OK;
+  bool stop = false;
+  while (!stop) {
+    if (L.graph) cudaGraphLaunch(L.exec, c.stream);
+    else launch_iteration<T, V, CLOS>(c, a, plan);
+    cudaMemcpyAsync(&c.h_state[launched % kRing], c.d_state, sizeof(DevState),
+                    cudaMemcpyDeviceToHost, c.stream);
+    cudaEventRecord(ev[launched % kRing], c.stream);
+    ++launched;
+    if (launched > kLag) {
+      int k = (launched - 1 - kLag) % kRing;
+      if (!cuda_ok(c, cudaEventSynchronize(ev[k]), "iteration")) { status = RISM3D_CUDA_ERROR; break; }
+      const DevState &s = c.h_state[k];
+      if (c.prm.verbose && s.done == 0)
+        printf(" Step = %d Reside = %g\n", s.iter, s.rms);
+      if (s.done) stop = true;
+      if (watch_stagnation && !stop) {
+        if (s.rms < 0.9 * best) { best = s.rms; since_best = 0; }
+        else if (++since_best > 30) stop = true;
+      }
+    }
+    if (launched > max_iter + kLag + 2) stop = true;   // hard bound
+  }
+  // drain: one more iteration guarantees the snapshot pass ran
+  if (status == RISM3D_OK) {
+    if (L.graph) cudaGraphLaunch(L.exec, c.stream);
+    else launch_iteration<T, V, CLOS>(c, a, plan);
+    cudaMemcpyAsync(&c.h_state[0], c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream);
+    if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "iteration drain")) status = RISM3D_CUDA_ERROR;
+  }
+  for (int i = 0; i < kRing; ++i) cudaEventDestroy(ev[i]);
+  if (L.exec) cudaGraphExecDestroy(L.exec);
+  iters_out = c.h_state[0].iter;
+  return status;
+}
+
+template <int V, int CLOS>
+int solve_v(Context &c, int chargeup) {
+  const long long n = c.n;
+  const bool mixed = c.prm.precision == RISM3D_MIXED;
+  const int gb = grid_blocks(n);
+  StageParams sp{};
+  for (int v = 0; v < V; ++v) sp.irho[v] = 1.0 / c.rho[v];
+  // stage schedule (iterate.cu:30-47)
+  int cu = chargeup;
+  double cf, cuf = 0.0;
+  const bool restart = !c.t_init.empty();
+  if (restart) { cu = 0; cf = 1.0; }
+  else if (cu == 0) cf = 1.0;
+  else { cuf = 1.0 / cu; cf = 0.0; }
+
+  // AN2 state (anderson.cu:13-32)
+  DevState hs{};
+  hs.count = c.prm.an2_count; hs.binary = 0; hs.m = c.prm.an2_m; hs.mp = c.prm.an2_mp;
+  hs.maxstep = c.prm.maxstep; hs.conv = c.prm.convergence;
+  cudaMemcpyAsync(c.d_state, &hs, sizeof(DevState), cudaMemcpyHostToDevice, c.stream);
+  cudaMemsetAsync(c.d_Y, 0, sizeof(double) * 2 * V * n, c.stream);
+  cudaMemsetAsync(c.d_RP, 0, sizeof(double) * 2 * V * n, c.stream);
+  if (mixed) {
+    cudaMemsetAsync(c.f_Y, 0, sizeof(float) * 2 * V * n, c.stream);
+    cudaMemsetAsync(c.f_RP, 0, sizeof(float) * 2 * V * n, c.stream);
+  }
+  // initial t_SR
+  for (int v = 0; v < V; ++v) sp.qcf[v] = c.qv[v] * cf;
+  cudaMemcpyAsync(c.d_stage, &sp, sizeof(sp), cudaMemcpyHostToDevice, c.stream);
+  double *d_tinit = nullptr;
+  if (restart) {
+    if (!cuda_ok(c, cudaMallocAsync(&d_tinit, sizeof(double) * V * n, c.stream), "alloc") ||
+        !cuda_ok(c, cudaMemcpyAsync(d_tinit, c.t_init.data(), sizeof(double) * V * n, cudaMemcpyHostToDevice, c.stream), "copy"))
+      return RISM3D_CUDA_ERROR;
+  }
+  k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, d_tinit, c.d_fr, c.d_stage, c.d_t);
+  if (d_tinit) cudaFreeAsync(d_tinit, c.stream);
+
+  int total = 0, total32 = 0, status = RISM3D_OK;
+  StageParams *d_step = nullptr;
+  if (!cuda_ok(c, cudaMallocAsync(&d_step, sizeof(StageParams), c.stream), "alloc")) return RISM3D_CUDA_ERROR;
+  for (int s = 0; s <= cu; ++s) {
+    if (s > 0) {                                  // add_tuv (iterate.cu:43-47)
+      double cfn = cf + cuf;
+      if (cfn > 1.0) cfn = 1.0;
+      StageParams step{};
+      for (int v = 0; v < V; ++v) step.qcf[v] = c.qv[v] * (cfn - cf);
+      cudaMemcpyAsync(d_step, &step, sizeof(step), cudaMemcpyHostToDevice, c.stream);
+      k_shift_history<double><<<gb, kThreads, 0, c.stream>>>(n, V, c.d_fr, d_step, c.d_Y);
+      if (mixed) k_shift_history<float><<<gb, kThreads, 0, c.stream>>>(n, V, c.d_fr, d_step, c.f_Y);
+      cf = cfn;
+    }
+    for (int v = 0; v < V; ++v) sp.qcf[v] = c.qv[v] * cf;
+    cudaMemcpyAsync(c.d_stage, &sp, sizeof(sp), cudaMemcpyHostToDevice, c.stream);
+    k_stage_u<<<gb, kThreads, 0, c.stream>>>(n, V, c.d_u, c.d_e, c.d_stage, c.d_U, mixed ? c.f_U : nullptr);
+    if (c.prm.verbose) printf("relaxing 3D UV RISM: Charge Up Factor = %g\n", cf);
+    int left = c.prm.maxstep;
+    if (mixed) {
+      // FP32 bulk: t/history to FP32, iterate to the switch point or until
+      // progress stalls, then promote back to FP64 for the polish.
+      const long long vn = (long long)V * n;
+      k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(vn, c.d_t, c.f_t);
+      k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.d_Y, c.f_Y);
+      k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.d_RP, c.f_RP);
+      double sw = c.prm.mixed_switch > 0 ? c.prm.mixed_switch : 5.0 * c.prm.convergence;
+      if (sw < c.prm.convergence) sw = c.prm.convergence;
+      int it32 = 0;
+      int st = iterate_phase<float, V, CLOS>(c, c.plan32, c.f_t, c.f_U, c.f_Y, c.f_RP,
+                                            c.f_buf, false, sw, left, true, it32);
+      if (st != RISM3D_OK) { status = st; break; }
+      DevState s32;
+      cudaMemcpy(&s32, c.d_state, sizeof(s32), cudaMemcpyDeviceToHost);
+      total32 += it32;
+      total += it32;
+      left -= it32;
+      if (s32.done == 2) {
+        // FP32 diverged: restart this stage in FP64 from the stage start
+        k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, nullptr, c.d_fr, c.d_stage, c.d_t);
+      } else {
+        k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(vn, c.f_t, c.d_t);
+        k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.f_Y, c.d_Y);
+        k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.f_RP, c.d_RP);
+      }
+      if (left < 1) left = 1;
+    }
+    int it = 0;
+    int st = iterate_phase<double, V, CLOS>(c, c.plan64, c.d_t, c.d_U, c.d_Y, c.d_RP,
+                                           c.d_buf, true, c.prm.convergence, left, false, it);
+    if (st != RISM3D_OK) { status = st; break; }
+    total += it;
+    DevState fs;
+    cudaMemcpy(&fs, c.d_state, sizeof(fs), cudaMemcpyDeviceToHost);
+    c.res.rms = fs.rms;
+    if (fs.done == 2) {                    // iterate.cu:74-75: report, go on
+      if (c.prm.verbose) printf("Calculation diverged.\n");
+      status = RISM3D_DIVERGED;
+    } else if (fs.done != 1) {             // iterate.cu:76-79: stop charging
+      if (c.prm.verbose) printf("3D UV RISM: reached limit # of relaxation steps: %d\n", c.prm.maxstep);
+      status = RISM3D_NOT_CONVERGED;
+      break;
+    }
+  }
+  cudaFreeAsync(d_step, c.stream);
+  c.cf_final = cf;
+  c.res.iterations = total;
+  c.res.iterations_fp32 = total32;
+  c.res.status = status;
+  if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "solve")) return RISM3D_CUDA_ERROR;
+  return (status == RISM3D_CUDA_ERROR || status == RISM3D_CUFFT_ERROR) ? status : RISM3D_OK;
+}
+
+template <int V>
+int solve_c(Context &c, int cu) {
+  return c.prm.closure == RISM3D_KH ? solve_v<V, 0>(c, cu) : solve_v<V, 1>(c, cu);
+}
+
+}  // namespace
+
+int build_twiddles(Context &c) {
+  std::vector<double2> tw(c.nx + c.ny + c.nz);
+  std::vector<float2> twf(tw.size());
+  int off = 0;
+  for (int d = 0; d < 3; ++d) {
+    int nd = d == 0 ? c.nx : (d == 1 ? c.ny : c.nz);
+    for (int i = 0; i < nd; ++i) {
+      double a = kPi / nd * (i - nd / 2);
+      tw[off + i] = make_double2(cos(a), -sin(a));
+      twf[off + i] = make_float2((float)cos(a), (float)-sin(a));
+    }
+    off += nd;
+  }
+  if (!cuda_ok(c, cudaMemcpyAsync(c.d_tw, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice, c.stream), "twiddles") ||
+      !cuda_ok(c, cudaMemcpyAsync(c.d_twf, twf.data(), sizeof(float2) * twf.size(), cudaMemcpyHostToDevice, c.stream), "twiddles") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "twiddles"))
+    return RISM3D_CUDA_ERROR;
+  return RISM3D_OK;
+}
+
+// Natural cubic spline of every chi_ab table (same tridiagonal sweep as
+// spline.cc:4-43), uploaded as [knot][ab][y c0 c1 c2].
+int upload_chi(Context &c) {
+  const int V = c.natv, nt = c.ntab;
+  c.chi.ntab = nt;
+  c.chi.dk = kPi / (c.xdr * nt);                 // solvent_read.cc:82
+  // largest |k| on the grid must be inside the table (solvent_spline.cu:18-21)
+  double kx = 2.0 * kPi * (c.nx / 2.0 - 0.5) / c.prm.box[0];
+  double ky = 2.0 * kPi * (c.ny / 2.0 - 0.5) / c.prm.box[1];
+  double kz = 2.0 * kPi * (c.nz / 2.0 - 0.5) / c.prm.box[2];
+  double kmax = sqrt(kx * kx + ky * ky + kz * kz);
+  if (kmax > c.chi.dk * nt) {
+    c.err = "insufficient maximal T tabulated";
+    return RISM3D_BAD_INPUT;
+  }
+  std::vector<double> xp(nt);
+  for (int i = 0; i < nt; ++i) xp[i] = c.chi.dk * (i + 1);
+  std::vector<double> tab((size_t)nt * V * V * 4, 0.0);
+  std::vector<double> a(nt), b(nt), cc(nt), d(nt), s(nt);
+  for (int va = 0; va < V; ++va)
+    for (int vb = 0; vb < V; ++vb) {
+      const double *yp = &c.xvv_host[((size_t)va * V + vb) * nt];
+      const int m = nt - 2;
+      for (int k = 1; k <= m; ++k) {
+        double hl = xp[k] - xp[k - 1], hr = xp[k + 1] - xp[k];
+        a[k] = hl / (hl + hr);
+        b[k] = 1 - a[k];
+        double q1 = (yp[k + 1] - yp[k]) / hr, q2 = (yp[k] - yp[k - 1]) / hl;
+        cc[k] = 6.0 * ((q1 - q2) / (hl + hr));
+        d[k] = 2.0;
+      }
+      for (int k = 1; k < m; ++k) {
+        b[k] = b[k] / d[k];
+        cc[k] = cc[k] / d[k];
+        d[k + 1] = d[k + 1] - a[k + 1] * b[k];
+        cc[k + 1] = cc[k + 1] - a[k + 1] * cc[k];
+      }
+      s[m] = cc[m] / d[m];
+      for (int k = m - 1; k >= 1; --k) s[k] = cc[k] - b[k] * s[k + 1];
+      s[0] = s[m + 1] = 0.0;
+      for (int k = 0; k < nt; ++k) {
+        double *o = &tab[((size_t)k * V * V + va * V + vb) * 4];
+        o[0] = yp[k];
+        if (k <= m) {
+          double h = xp[k + 1] - xp[k];
+          double c1 = s[k] / 2.0;
+          double c2 = (s[k + 1] - s[k]) / (6.0 * h);
+          o[1] = (yp[k + 1] - yp[k]) / h - c1 * h - c2 * h * h;
+          o[2] = c1;
+          o[3] = c2;
+        }
+      }
+    }
+  if (c.chi.d_coef) cudaFree(c.chi.d_coef);
+  if (!cuda_ok(c, cudaMalloc(&c.chi.d_coef, sizeof(double) * tab.size()), "chi alloc") ||
+      !cuda_ok(c, cudaMemcpyAsync(c.chi.d_coef, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c.stream), "chi copy") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "chi"))
+    return RISM3D_CUDA_ERROR;
+  return RISM3D_OK;
+}
+
+int run_solve(Context &c, int chargeup) {
+  switch (c.natv) {
+    case 1: return solve_c<1>(c, chargeup);
+    case 2: return solve_c<2>(c, chargeup);
+    case 3: return solve_c<3>(c, chargeup);
+    case 4: return solve_c<4>(c, chargeup);
+    case 5: return solve_c<5>(c, chargeup);
+    case 6: return solve_c<6>(c, chargeup);
+    case 7: return solve_c<7>(c, chargeup);
+    case 8: return solve_c<8>(c, chargeup);
+  }
+  c.err = "unsupported number of solvent sites";
+  return RISM3D_UNSUPPORTED_SHAPE;
+}
+
+}  // namespace rism3d

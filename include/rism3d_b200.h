@@ -1,0 +1,186 @@
+/*
+ * rism3d_b200 -- B200-native 3D-RISM solver, C ABI.
+ *
+ * Drop-in for the solve path of rismical-dev/3D-RISM-CUDA (src-cuda/).  The
+ * reference has no library API: its public surface is the C++ class
+ * RISM3D with initialize / iterate / output (rism3d.h:25-27), driven by
+ * main (main.cu:6-64), plus its file formats.  This header gives
+ *   (1) rism3d_initialize / rism3d_iterate / rism3d_output: the same three
+ *       steps with the same arguments, reading and writing the same files;
+ *   (2) an array-level API (create / set_solvent / set_solute / solve /
+ *       forces / grad / get_grid / solve_batch / destroy) so that callers
+ *       can drive a solve from memory without files.
+ * Plain C types only: pointers, sizes, POD structs.  Every call returns a
+ * status code; no call exits the process (the reference calls exit(1) on
+ * bad input, e.g. read_input.cu:31-32, solvent_read.cc:16-19).
+ *
+ * Units follow the reference: lengths in Angstrom, solute/solvent epsilon
+ * in J/mol, charges in e, solvent densities in molecules/A^3, energies
+ * reported in J/mol, PMV in L/mol, pressure in J/m^3.
+ */
+#ifndef RISM3D_B200_H
+#define RISM3D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RISM3D_MAX_SITES 8
+
+/* status codes */
+enum {
+  RISM3D_OK = 0,
+  RISM3D_BAD_INPUT = 1,          /* malformed file / argument */
+  RISM3D_UNSUPPORTED_SHAPE = 2,  /* grid not a multiple of 4, too many sites */
+  RISM3D_CUDA_ERROR = 3,
+  RISM3D_CUFFT_ERROR = 4,
+  RISM3D_DIVERGED = 5,           /* non-finite residual (iterate.cu:54-57) */
+  RISM3D_NOT_CONVERGED = 6,      /* maxstep reached (iterate.cu:76-79) */
+  RISM3D_NO_DEVICE = 7,
+  RISM3D_BAD_STATE = 8           /* call out of order */
+};
+
+enum { RISM3D_KH = 0, RISM3D_HNC = 1 };          /* read_input.cu:37-44 */
+enum { RISM3D_FP64 = 0, RISM3D_MIXED = 1 };      /* arithmetic of the iteration */
+
+/* grids returned by rism3d_get_grid, each natv * N doubles (site-major,
+ * x fastest: ip = ix + nx*(iy + ny*iz)) unless noted */
+enum {
+  RISM3D_GRID_G = 0,    /* g_uv(r) (the .guv payload, output_guv.cu)       */
+  RISM3D_GRID_H = 1,    /* h_uv(r) from the OZ step (output_huv.cu)        */
+  RISM3D_GRID_C = 2,    /* c_uv(r) = h - t (output_cuv.cu)                  */
+  RISM3D_GRID_T = 3,    /* t_uv(r) (the .tuv payload, write_tuv.cu)        */
+  RISM3D_GRID_U = 4,    /* beta u_LJ per site (cal_LJ.cu)                   */
+  RISM3D_GRID_E = 5,    /* beta sum q/r, N doubles (cal_Coulomb.cu)         */
+  RISM3D_GRID_FR = 6,   /* beta long-range part, N doubles                  */
+  RISM3D_GRID_QV = 7    /* sum_v rho_v q_v g_v, N doubles (cal_qv.cu)       */
+};
+
+typedef struct {
+  int grid[3];            /* nx ny nz, each a multiple of 4 (fft3d.cu:71-94) */
+  double box[3];          /* Angstrom */
+  int closure;            /* RISM3D_KH / RISM3D_HNC */
+  double convergence;     /* rms residual target (iterate.cu:58) */
+  int maxstep;
+  int an2_count;          /* Picard steps before AN2 (anderson.cu:43-49) */
+  double an2_m;           /* AN2 mixing factor */
+  double an2_mp;          /* AN2 bias on the newer slot */
+  int precision;          /* RISM3D_FP64 or RISM3D_MIXED */
+  double mixed_switch;    /* MIXED: leave FP32 once rms <= this (0 = auto) */
+  int device;             /* CUDA ordinal (main.cu:57) */
+  int verbose;            /* 1: print " Step = n Reside = r" like iterate.cu:63 */
+} rism3d_params;
+
+typedef struct {
+  int natv;
+  int natom;
+  double sfe_sc;          /* SFE_SC, J/mol (KH functional for KH, HNC for HNC) */
+  double sfe_sc_hnc;      /* SFE_SC_HNC (reported for KH only) */
+  double sfe_gf;          /* SFE_GF */
+  double sfec_sc[RISM3D_MAX_SITES];
+  double sfec_sc_hnc[RISM3D_MAX_SITES];
+  double sfec_gf[RISM3D_MAX_SITES];
+  double pmv;             /* L/mol */
+  double pressure;        /* J/m^3 */
+  double correction;      /* J/mol, -P * PMV */
+  double se, se_lj, se_es;/* solute-solvent energy, J/mol */
+  double rms;             /* final residual */
+  int iterations;         /* all iterations (all stages, both precisions) */
+  int iterations_fp32;    /* of which in FP32 (MIXED) */
+  int status;             /* RISM3D_OK / DIVERGED / NOT_CONVERGED */
+  double ms_setup;        /* potential grids + chi table (device time) */
+  double ms_iterate;
+  double ms_observe;
+} rism3d_result;
+
+typedef struct rism3d_ctx rism3d_ctx;
+
+/* ---- array-level API ---------------------------------------------------
+ * Replaces: RISM3D::initialize's file readers + cal_potential
+ * (initialize.cu:4-13), RISM3D::iterate (iterate.cu:6-90) and the
+ * observables of RISM3D::output (output.cu:6-62). */
+
+/* Allocate a context on params->device.  Replaces the implicit RISM3D
+ * constructor + Cell::setup (cell.cc:8-22) + FFT3D::initialize
+ * (fft3d.cu:4-19). */
+int rism3d_create(const rism3d_params *params, rism3d_ctx **ctx);
+
+/* Solvent sites after merging equivalent sites (solvent_read.cc:68-80):
+ * rho in molecules/A^3, chi table xvv[natv][natv][ntab] at
+ * k_i = (i+1) pi / (dr ntab), row b fastest (solvent_read.cc:51-58).
+ * Replaces Solvent::read + Solvent::spline (solvent_spline.cu:8-91). */
+int rism3d_set_solvent(rism3d_ctx *ctx, int natv, const double *rho,
+                       const double *q, const double *sig, const double *eps,
+                       double temperature, double xt, int ntab, double dr,
+                       const double *xvv);
+
+/* Solute atoms, coordinates already placed in the cell (the reference
+ * centres them in read_input.cu:80-82; rism3d_initialize does the same).
+ * Replaces Solute::init/setup_cuda (solute.cu:5-56) and computes the
+ * potential grids of cal_potential (cal_potential.cu:3-14). */
+int rism3d_set_solute(rism3d_ctx *ctx, int natom, const double *sig,
+                      const double *eps, const double *q, const double *xyz);
+
+/* Optional restart guess t_uv[natv][N] (read_tuv.cu:6-34).  NULL clears. */
+int rism3d_set_tuv(rism3d_ctx *ctx, const double *tuv);
+
+/* Solve with `chargeup` charge-up stages (main.cu -c; iterate.cu:34-47)
+ * and evaluate mu_ex (cal_exchem.cu), PMV (cal_pmv.cu), pressure
+ * (cal_pressure.cu) and SE (cal_euv.cu). */
+int rism3d_solve(rism3d_ctx *ctx, int chargeup, rism3d_result *result);
+
+/* Per (site, atom) solute-solvent energies euv[2][natv][natom] (LJ then
+ * ES, J/mol, already times dv; cal_euv.cu:7-33 + output_euv.cu). */
+int rism3d_euv(rism3d_ctx *ctx, double *euv);
+
+/* cal_grad forces (cal_grad.cu:8-48 + output_grad.cu): dulj[natom][3],
+ * due[natom][3] in J/mol/A, already times dv. */
+int rism3d_forces(rism3d_ctx *ctx, double *dulj, double *due);
+
+/* Adjoint: d(SFE_SC)/d(parameter) in J/mol per unit, by back-propagating
+ * rho_v g_v(r) through the potential-grid kernel with per-atom potentials
+ * recomputed.  Any output pointer may be NULL.  dmu_dR is [natom][3]. */
+int rism3d_grad(rism3d_ctx *ctx, double *dmu_dq, double *dmu_dsig,
+                double *dmu_deps, double *dmu_dR);
+
+/* Copy a result grid to host memory (see RISM3D_GRID_*). */
+int rism3d_get_grid(rism3d_ctx *ctx, int which, double *host);
+
+/* Batched small solutes (no reference counterpart; the reference solves
+ * one solute per process).  Solute m has natoms[m] atoms starting at
+ * atom offset off[m] in the concatenated arrays, a cubic grid
+ * grids[m]^3 and cubic box boxes[m].  results[m] receives its result. */
+int rism3d_solve_batch(rism3d_ctx *ctx, int nmol, const int *natoms,
+                       const int *grids, const double *boxes,
+                       const double *sig, const double *eps, const double *q,
+                       const double *xyz, rism3d_result *results);
+
+void rism3d_destroy(rism3d_ctx *ctx);
+
+/* Last error message of ctx (or of the last failed create when ctx is
+ * NULL). */
+const char *rism3d_last_error(const rism3d_ctx *ctx);
+
+/* ---- file-driven API: the three public RISM3D methods -------------------
+ * rism3d_initialize == RISM3D::initialize(control, structure, esp, hs,
+ * centering, q0) (initialize.cu:4-13): reads the .inp (and optional
+ * structure file), the .xvk named in it, centres the solute, zeroes the
+ * charges when q0, and computes the potential grids.  esp (ESP cube) and
+ * hs (RMDFT hard-sphere file) must be NULL or "" in this build.
+ * `device` selects the GPU (main.cu -d) and `precision` the arithmetic. */
+int rism3d_initialize(rism3d_ctx **ctx, const char *control,
+                      const char *structure, const char *esp, const char *hs,
+                      int centering, int q0, int device, int precision);
+
+/* RISM3D::iterate(cu) (iterate.cu:6-90), including the .tuv restart read
+ * when <basename>.tuv exists and the ksave writes. */
+int rism3d_iterate(rism3d_ctx *ctx, int chargeup);
+
+/* RISM3D::output() (output.cu:6-62): writes .xmu/.xmu0, .gra, .guv, .huv,
+ * .cuv, .euv, .qv according to the control file's outlist letters. */
+int rism3d_output(rism3d_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RISM3D_B200_H */

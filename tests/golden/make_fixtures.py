@@ -1,0 +1,40 @@
+"""Copies the reference's own example inputs and golden outputs into
+tests/golden/ (run once in the build container, where the reference tree is
+mounted; the GPU box only sees the committed copies).
+
+Inputs: example/test{1..4}.inp (+ the _c/_s split form of test1),
+example/h2o_vv.xvk.  Goldens: example/test{1..4}.xmu (written by an older
+reference build; see the tolerance notes in tests/test_oracle_golden.py).
+Also writes tight-convergence variants (``*_tight.inp``, conv 1e-9) used to
+compare solutions at the fixed point rather than at the 1e-6 stopping point.
+"""
+import os
+import shutil
+import sys
+
+SRC = "/root/reference/example"
+DST = os.path.dirname(os.path.abspath(__file__))
+
+FILES = ["test1.inp", "test2.inp", "test3.inp", "test4.inp", "test1_c", "test1_s",
+         "h2o_vv.xvk", "test1.xmu", "test2.xmu", "test3.xmu", "test4.xmu"]
+
+
+def tighten(src, dst, conv="1.0e-9"):
+    tok_lines = open(src).read().split("\n")
+    # line 4 (index 3) holds "convergence maxstep" (read_input.cu:46)
+    parts = tok_lines[3].split()
+    tok_lines[3] = " %s   %s" % (conv, parts[1])
+    open(dst, "w").write("\n".join(tok_lines))
+
+
+def main():
+    if not os.path.isdir(SRC):
+        sys.exit("reference examples not mounted")
+    for f in FILES:
+        shutil.copyfile(os.path.join(SRC, f), os.path.join(DST, f))
+    for name in ("test1", "test2"):
+        tighten(os.path.join(DST, name + ".inp"), os.path.join(DST, name + "_tight.inp"))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,58 @@
+"""Runs the reference executable (oracle/_ref/3drism-cuda, built from the
+reference's own sources for sm_100a) on the committed inputs and records its
+.xmu outputs, iteration counts and wall times.  Run on a GPU box:
+
+    python tests/golden/run_reference.py OUTDIR [case ...]
+
+The .xmu files it writes are copied into tests/golden/ref_b200/ as the
+authoritative parity pins (the example .xmu files come from an older build).
+"""
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+BIN = os.path.join(ROOT, "oracle", "_ref", "3drism-cuda")
+
+CASES = ["test1", "test1_tight", "test2", "test2_tight", "test3", "test4",
+         "cfg0_chain12", "cfg1_globule300", "cfg2_protein846_kh"]
+
+
+def run(case, outdir):
+    d = os.path.join(outdir, case)
+    os.makedirs(d, exist_ok=True)
+    shutil.copyfile(os.path.join(HERE, case + ".inp"), os.path.join(d, case + ".inp"))
+    shutil.copyfile(os.path.join(HERE, "h2o_vv.xvk"), os.path.join(d, "h2o_vv.xvk"))
+    t0 = time.perf_counter()
+    p = subprocess.run(["timeout", "900", BIN, case + ".inp"], cwd=d,
+                       capture_output=True, text=True)
+    wall = time.perf_counter() - t0
+    open(os.path.join(d, "stdout.log"), "w").write(p.stdout + p.stderr)
+    steps = [int(m.group(1)) for m in re.finditer(r"Step = (\d+)", p.stdout)]
+    res = {"case": case, "rc": p.returncode, "wall_s": wall,
+           "iterations": len(steps)}
+    xmu = os.path.join(d, case + ".xmu")
+    if os.path.exists(xmu):
+        res["xmu"] = open(xmu).read()
+    return res
+
+
+def main():
+    outdir = sys.argv[1]
+    cases = sys.argv[2:] or CASES
+    out = []
+    for c in cases:
+        r = run(c, outdir)
+        print(json.dumps({k: v for k, v in r.items() if k != "xmu"}), flush=True)
+        out.append(r)
+    json.dump(out, open(os.path.join(outdir, "summary.json"), "w"), indent=1)
+    return 0 if all(r["rc"] == 0 for r in out) else 1
+
+
+if __name__ == "__main__":
+    sys.exit(main())

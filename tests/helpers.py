@@ -1,0 +1,39 @@
+"""Shared test helpers: build a case once, feed identical arrays to the
+oracle (CPU FP64 restatement) and to the product (C ABI)."""
+import os
+
+import numpy as np
+
+from conftest import GOLDEN
+from oracle import formats as F
+from oracle import oracle as O
+
+KCAL = 4184.0
+MU_TOL = 0.01 * KCAL          # 0.01 kcal/mol in J/mol (the parity target)
+
+
+def load_case(name, **over):
+    """Case from a control file in tests/golden (centred like the reference)."""
+    case, ctrl, sol = O.case_from_inp(os.path.join(GOLDEN, name + ".inp"),
+                                      xvk=os.path.join(GOLDEN, "h2o_vv.xvk"))
+    for k, v in over.items():
+        setattr(case, k, v)
+    return case, ctrl, sol
+
+
+def product_solver(case, precision=0, **kw):
+    import rism3d_b200 as R
+    s = R.Solver(case.grid, case.box, closure=case.closure, convergence=case.conv,
+                 maxstep=case.maxstep, an2=(case.count, case.m, case.mp),
+                 precision=precision, **kw)
+    s.set_solvent_obj(case.sv)
+    s.set_solute(case.sig, case.eps, case.q, case.xyz)
+    return s
+
+
+def ref_xmu(name):
+    return F.parse_xmu(os.path.join(GOLDEN, "ref_b200", name + ".xmu"))
+
+
+def rel_err(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))

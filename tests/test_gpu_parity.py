@@ -1,0 +1,87 @@
+"""GPU parity: the CUDA solve path (through the C ABI) against the CPU FP64
+oracle on identical inputs, and against the reference executable's own
+outputs recorded on a B200 (tests/golden/ref_b200).
+
+Tolerances: mu_ex within 0.01 kcal/mol (41.84 J/mol) and g(r) within 1e-4
+relative, as the solve path requires; tighter informative bounds where
+both sides run the same FP64 algorithm."""
+import numpy as np
+import pytest
+
+from helpers import MU_TOL, load_case, product_solver, ref_xmu, rel_err
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def test1_oracle():
+    case, _, _ = load_case("test1")
+    return case, O.solve(case, want_grids=True)
+
+
+def test_potential_grids_match_oracle():
+    case, _, _ = load_case("cfg0_chain12")
+    u, e, fr, fk = O.potentials(case)
+    s = product_solver(case)
+    import rism3d_b200 as R
+    assert rel_err(s.grid_array(R.GRID_U), u) < 1e-11
+    assert rel_err(s.grid_array(R.GRID_FR)[0], fr) < 1e-11
+    assert rel_err(s.grid_array(R.GRID_E)[0], e) < 1e-11
+    s.close()
+
+
+def test_fp64_solve_test1_matches_oracle_and_reference(test1_oracle):
+    case, o = test1_oracle
+    s = product_solver(case)
+    r = s.solve()
+    ref = ref_xmu("test1")
+    # same algorithm, same stopping rule: identical iteration count
+    assert abs(r["iterations"] - o["iterations"]) <= 1
+    assert abs(r["sfe_sc"] - o["sfe_sc"]) < 1.0
+    assert abs(r["sfe_gf"] - o["sfe_gf"]) < 1.0
+    assert abs(r["sfe_sc"] - ref["SFE_SC"]) < MU_TOL
+    assert abs(r["sfe_sc_hnc"] - ref["SFE_SC_HNC"]) < MU_TOL
+    assert abs(r["sfe_gf"] - ref["SFE_GF"]) < MU_TOL
+    assert abs(r["pmv"] - ref["PMV"]) < 1e-4
+    assert abs(r["se"] - ref["SE"]) < 1.0
+    import rism3d_b200 as R
+    g = s.grid_array(R.GRID_G)
+    assert rel_err(g, o["g"]) < 1e-4
+    h = s.grid_array(R.GRID_H)
+    assert rel_err(h, o["h"]) < 1e-4
+    s.close()
+
+
+def test_fp64_solve_test2_matches_reference():
+    case, _, _ = load_case("test2")
+    s = product_solver(case)
+    r = s.solve()
+    ref = ref_xmu("test2")
+    assert abs(r["sfe_sc"] - ref["SFE_SC"]) < MU_TOL
+    assert abs(r["sfe_gf"] - ref["SFE_GF"]) < MU_TOL
+    assert abs(r["pmv"] - ref["PMV"]) < 1e-4
+    assert abs(r["correction"] - ref["Correction_Term"]) < 1.0
+    s.close()
+
+
+def test_mixed_precision_within_target(test1_oracle):
+    case, o = test1_oracle
+    import rism3d_b200 as R
+    s = product_solver(case, precision=R.MIXED)
+    r = s.solve()
+    assert r["iterations_fp32"] > 0
+    assert abs(r["sfe_sc"] - o["sfe_sc"]) < MU_TOL
+    assert rel_err(s.grid_array(R.GRID_G), o["g"]) < 1e-4
+    s.close()
+
+
+def test_forces_match_oracle(test1_oracle):
+    case, o = test1_oracle
+    s = product_solver(case)
+    s.solve()
+    dulj, due = s.forces()
+    dv = case.box[0] * case.box[1] * case.box[2] / case.n
+    assert np.allclose(dulj, o["dulj"] * dv, rtol=1e-6, atol=1e-6)
+    assert np.allclose(due, o["due"] * dv, rtol=1e-6, atol=1e-6)
+    s.close()
