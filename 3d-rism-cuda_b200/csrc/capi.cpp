@@ -39,7 +39,7 @@ void free_device(Context &c) {
   void *ptrs[] = {c.d_u, c.d_e, c.d_fr, c.d_fkh, c.d_atoms, c.d_tw, c.d_twf,
                   c.d_U, c.d_t, c.d_Y, c.d_RP, c.d_buf, c.d_h, c.d_g,
                   c.f_U, c.f_t, c.f_Y, c.f_RP, c.f_buf, c.d_part, c.d_state,
-                  c.d_stage, c.d_obs, c.d_atom_part, c.chi.d_coef};
+                  c.d_stage, c.d_obs, c.d_atom_part, c.chi.d_coef, c.d_xs};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   c.d_u = c.d_e = c.d_fr = nullptr; c.d_fkh = nullptr; c.d_atoms = nullptr;
@@ -48,6 +48,7 @@ void free_device(Context &c) {
   c.f_U = c.f_t = c.f_Y = c.f_RP = nullptr; c.f_buf = nullptr;
   c.d_part = nullptr; c.d_state = nullptr; c.d_stage = nullptr; c.d_obs = nullptr;
   c.d_atom_part = nullptr; c.chi.d_coef = nullptr; c.natom_part_cap = 0;
+  c.d_xs = nullptr; c.nxs = 0;
   if (c.h_state) cudaFreeHost(c.h_state);
   c.h_state = nullptr;
   if (c.plan64) cufftDestroy(c.plan64);
@@ -150,6 +151,10 @@ int rism3d_create(const rism3d_params *p, rism3d_ctx **out) {
     }
     if (!(p->box[d] > 0)) { g_create_err = "box must be positive"; return RISM3D_BAD_INPUT; }
   }
+  if ((long long)p->grid[0] * p->grid[1] * p->grid[2] >= (1LL << 31)) {
+    g_create_err = "grid has 2^31 points or more";
+    return RISM3D_UNSUPPORTED_SHAPE;
+  }
   if (p->closure != RISM3D_KH && p->closure != RISM3D_HNC) {
     g_create_err = "Unexpected closure switch";
     return RISM3D_BAD_INPUT;
@@ -170,8 +175,16 @@ int rism3d_create(const rism3d_params *p, rism3d_ctx **out) {
   Context &c = x->c;
   c.prm = *p;
   c.dev = p->device;
-  if (cudaSetDevice(c.dev) != cudaSuccess || cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaSetDevice(c.dev) != cudaSuccess) {
     g_create_err = "cannot initialise the CUDA device";
+    delete x;
+    return RISM3D_CUDA_ERROR;
+  }
+  if (p->stream) {
+    c.stream = (cudaStream_t)p->stream;
+    c.own_stream = false;
+  } else if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    g_create_err = "cannot create a CUDA stream";
     delete x;
     return RISM3D_CUDA_ERROR;
   }
@@ -198,7 +211,7 @@ int rism3d_create(const rism3d_params *p, rism3d_ctx **out) {
   if (!ok || build_twiddles(c) != RISM3D_OK) {
     g_create_err = c.err;
     free_device(c);
-    cudaStreamDestroy(c.stream);
+    if (c.own_stream) cudaStreamDestroy(c.stream);
     delete x;
     return RISM3D_CUDA_ERROR;
   }
@@ -363,8 +376,31 @@ void rism3d_destroy(rism3d_ctx *x) {
     if (t->a) cudaEventDestroy(t->a);
     if (t->b) cudaEventDestroy(t->b);
   }
-  if (c.stream) cudaStreamDestroy(c.stream);
+  if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);
   delete x;
+}
+
+int rism3d_refresh_potentials(rism3d_ctx *x) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (!c.have_solute) { c.err = "no solute"; return RISM3D_BAD_STATE; }
+  cudaEventRecord(c.tm_setup.a, c.stream);
+  int rc = compute_potentials(c);
+  cudaEventRecord(c.tm_setup.b, c.stream);
+  c.solved = false;
+  c.have_forces = false;
+  return rc;
+}
+
+long long rism3d_kernel_launches(const rism3d_ctx *x) { return x ? x->c.launches : 0; }
+
+int rism3d_time_kernel(rism3d_ctx *x, int which, int reps, double *ms) {
+  if (!x || !ms || reps < 1) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (!c.have_solute) { c.err = "no solute"; return RISM3D_BAD_STATE; }
+  return time_kernel(c, which, reps, ms);
 }
 
 const char *rism3d_last_error(const rism3d_ctx *x) {

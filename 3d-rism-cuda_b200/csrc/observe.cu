@@ -192,6 +192,7 @@ int observe_v(Context &c) {
   else
     k_observe<V, 1><<<nb, kThreads, 0, c.stream>>>(c.n, c.d_h, c.d_t, c.d_fr, c.d_stage, c.d_part, nb);
   k_reduce_rows<<<4 * V, 256, 0, c.stream>>>(c.d_part, nb, c.d_obs);
+  c.launches += 2;
   std::vector<double> s(4 * V);
   if (!cuda_ok(c, cudaMemcpyAsync(s.data(), c.d_obs, sizeof(double) * 4 * V, cudaMemcpyDeviceToHost, c.stream), "observe") ||
       !cuda_ok(c, cudaStreamSynchronize(c.stream), "observe"))
@@ -252,6 +253,7 @@ int atoms_v(Context &c, bool forces) {
       chunk, c.d_atom_part, forces ? 1 : 0);
   double *sum = c.d_atom_part + (size_t)nchunk * A * NA;
   k_sum_chunks<<<(A * NA + 255) / 256, 256, 0, c.stream>>>(c.d_atom_part, nchunk, A, NA, sum);
+  c.launches += 2;
   std::vector<double> h((size_t)A * NA);
   if (!cuda_ok(c, cudaGetLastError(), "atom integrals") ||
       !cuda_ok(c, cudaMemcpyAsync(h.data(), sum, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream), "atom integrals") ||

@@ -160,6 +160,26 @@ void launch_r(Context &c, const SiteLJ &sl, double ikbt, double ubeta) {
 
 }  // namespace
 
+int launch_potential_r(Context &c) {
+  SiteLJ sl{};
+  for (int v = 0; v < c.natv; ++v) { sl.sig[v] = c.sigv[v]; sl.eps[v] = c.epsv[v]; }
+  const double ikbt = 1.0 / (kAvogadro * kBoltzmann * c.temper);
+  const double ubeta = kHartree * kBohr / (kBoltzmann * c.temper);
+  switch (c.natv) {
+    case 1: launch_r<1>(c, sl, ikbt, ubeta); break;
+    case 2: launch_r<2>(c, sl, ikbt, ubeta); break;
+    case 3: launch_r<3>(c, sl, ikbt, ubeta); break;
+    case 4: launch_r<4>(c, sl, ikbt, ubeta); break;
+    case 5: launch_r<5>(c, sl, ikbt, ubeta); break;
+    case 6: launch_r<6>(c, sl, ikbt, ubeta); break;
+    case 7: launch_r<7>(c, sl, ikbt, ubeta); break;
+    case 8: launch_r<8>(c, sl, ikbt, ubeta); break;
+    default: return RISM3D_UNSUPPORTED_SHAPE;
+  }
+  c.launches += 1;
+  return RISM3D_OK;
+}
+
 int compute_potentials(Context &c) {
   SiteLJ sl{};
   for (int v = 0; v < c.natv; ++v) { sl.sig[v] = c.sigv[v]; sl.eps[v] = c.epsv[v]; }
@@ -182,6 +202,7 @@ int compute_potentials(Context &c) {
       c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], c.d_atoms,
       c.natom, ubeta, c.d_fkh);
   if (!cuda_ok(c, cudaGetLastError(), "k_potential_k")) return RISM3D_CUDA_ERROR;
+  c.launches += 2;
   return RISM3D_OK;
 }
 

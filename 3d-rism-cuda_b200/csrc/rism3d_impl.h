@@ -56,6 +56,25 @@ struct ChiTable {
   double *d_coef = nullptr;  // [ntab][natv*natv][4]
 };
 
+// Division by a runtime constant d >= 1 for dividends x < 2^31 by
+// multiply-high and shift (Granlund & Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994, round-up variant):
+// s = ceil(log2 d), m = floor(2^32 (2^s - d) / d) + 1, q = (mulhi(x,m) + x) >> s.
+struct FastDiv {
+  unsigned d = 1, m = 1, s = 0;
+  FastDiv() = default;
+  explicit FastDiv(unsigned dd) : d(dd) {
+    s = 0;
+    while ((1ull << s) < dd) ++s;
+    m = (unsigned)(((1ull << 32) * ((1ull << s) - dd)) / dd + 1);
+  }
+#ifdef __CUDACC__
+  __device__ __forceinline__ unsigned div(unsigned x) const {
+    return (__umulhi(x, m) + x) >> s;
+  }
+#endif
+};
+
 struct Timer {
   cudaEvent_t a = nullptr, b = nullptr;
 };
@@ -65,6 +84,8 @@ struct Context {
   std::string err;
   int dev = 0;
   cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  long long launches = 0;      // kernels of this library launched so far
 
   // cell (cell.cc:8-22)
   int nx = 0, ny = 0, nz = 0;
@@ -77,6 +98,10 @@ struct Context {
   double temper = 0, xt = 0;
   bool have_solvent = false;
   ChiTable chi;
+  // cubic cells: chi_ab tabulated per s = ox^2 + oy^2 + oz^2 (odd o_d), so
+  // |k| = (pi/L) sqrt(s) and the table index is (s - 3) / 8
+  double *d_xs = nullptr;    // [nidx][V*V] or null (general cells: spline)
+  int nxs = 0;
   std::vector<double> xvv_host;
   int ntab = 0;
   double xdr = 0;
@@ -88,7 +113,7 @@ struct Context {
 
   // device grids
   double *d_u = nullptr;     // [V][N] beta u_LJ
-  double *d_e = nullptr;     // [N]   beta sum q/r
+  double *d_e = nullptr;     // [N]   beta sum q e^-r / r (short-range Coulomb)
   double *d_fr = nullptr;    // [N]   beta long-range part
   double2 *d_fkh = nullptr;  // [N/2] beta fk on the owner half of k space
   double *d_atoms = nullptr; // [A][8] x y z q sig eps pad
@@ -143,6 +168,7 @@ struct Context {
 // ---- kernels/launchers (implemented in the .cu files) ----
 int build_twiddles(Context &c);
 int compute_potentials(Context &c);               // potential.cu
+int launch_potential_r(Context &c);               // potential.cu (timing hook)
 int upload_chi(Context &c);                       // solver.cu
 int run_solve(Context &c, int chargeup);          // solver.cu
 int compute_observables(Context &c);              // observe.cu
@@ -150,6 +176,7 @@ int compute_atom_integrals(Context &c, bool forces);  // observe.cu
 int compute_adjoint(Context &c, double *dq, double *dsig, double *deps,
                     double *dR);                  // adjoint.cu
 int fetch_grid(Context &c, int which, double *host);
+int time_kernel(Context &c, int which, int reps, double *ms);   // solver.cu
 void free_device(Context &c);
 
 bool cuda_ok(Context &c, cudaError_t e, const char *what);

@@ -44,6 +44,8 @@ template <typename T>
 struct IterArgs {
   long long n;
   int nx, ny, nz;
+  FastDiv fdx, fdy;         // division by nx and ny
+  const double *xs;         // chi table per odd-square sum (cubic cells) or null
   typename Cx<T>::t *buf;   // [P][N]
   T *t, *U, *Y, *RP;        // t, U: [V][N]; Y, RP: [2][V][N]
   double *hout, *gout;      // final snapshot, [V][N] (may be null)
@@ -74,6 +76,55 @@ template <> __device__ __forceinline__ float2 mk<float2>(double x, double y) {
   return make_float2((float)x, (float)y);
 }
 
+// Vector access to PTS (1 or 2) consecutive points of a real or complex
+// array; point pairs start at even indices, so 2-wide accesses are aligned.
+template <typename T> struct V2;
+template <> struct V2<float> { typedef float2 t; typedef float4 c; };
+template <> struct V2<double> { typedef double2 t; typedef double4 c; };
+
+template <int PTS, typename T>
+__device__ __forceinline__ void ldr(const T *__restrict__ p, T (&o)[PTS]) {
+  if (PTS == 1) {
+    o[0] = p[0];
+  } else {
+    const typename V2<T>::t w = *reinterpret_cast<const typename V2<T>::t *>(p);
+    o[0] = w.x;
+    o[PTS - 1] = w.y;
+  }
+}
+template <int PTS, typename T>
+__device__ __forceinline__ void str(T *__restrict__ p, const T (&o)[PTS]) {
+  if (PTS == 1) {
+    p[0] = o[0];
+  } else {
+    typename V2<T>::t w;
+    w.x = o[0];
+    w.y = o[PTS - 1];
+    *reinterpret_cast<typename V2<T>::t *>(p) = w;
+  }
+}
+template <int PTS, typename C>
+__device__ __forceinline__ void ldc(const C *__restrict__ p, C (&o)[PTS]) {
+#pragma unroll
+  for (int k = 0; k < PTS; ++k) o[k] = p[k];
+}
+template <int PTS, typename C>
+__device__ __forceinline__ void stc(C *__restrict__ p, const C (&o)[PTS]) {
+#pragma unroll
+  for (int k = 0; k < PTS; ++k) p[k] = o[k];
+}
+// FP32 complex pairs move as one 16-byte access
+template <>
+__device__ __forceinline__ void ldc<2, float2>(const float2 *__restrict__ p, float2 (&o)[2]) {
+  const float4 w = *reinterpret_cast<const float4 *>(p);
+  o[0] = make_float2(w.x, w.y);
+  o[1] = make_float2(w.z, w.w);
+}
+template <>
+__device__ __forceinline__ void stc<2, float2>(float2 *__restrict__ p, const float2 (&o)[2]) {
+  *reinterpret_cast<float4 *>(p) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+}
+
 __device__ __forceinline__ double fexp(double x) { return exp(x); }
 __device__ __forceinline__ float fexp(float x) { return expf(x); }
 
@@ -87,179 +138,143 @@ __device__ __forceinline__ T closure(T x) {
 // Point index -> (ix, iy, iz), +-1 checkerboard dir = (-1)^(ix+iy+iz)
 // (set_ir, fft3d.cu:86-94) and dkf = exp(-i pi sum x_d/n_d)
 // (set_kf, fft3d.cu:71-83) as a product of three per-axis phases.
+__device__ __forceinline__ void split_index(long long j, const FastDiv &fdx,
+                                            const FastDiv &fdy, int &ix, int &iy,
+                                            int &iz) {
+  const unsigned u = (unsigned)j;                 // N < 2^31
+  const unsigned r = fdx.div(u);
+  ix = (int)(u - r * fdx.d);
+  iz = (int)fdy.div(r);
+  iy = (int)(r - (unsigned)iz * fdy.d);
+}
+
 template <typename C>
-__device__ __forceinline__ void point_phase(long long j, int nx, int ny,
-                                            const C *tw, int &ix, int &iy,
-                                            int &iz, int &dir, C &dkf) {
-  long long r = j / nx;
-  ix = (int)(j - r * nx);
-  iy = (int)(r % ny);
-  iz = (int)(r / ny);
+__device__ __forceinline__ void point_phase(long long j, const FastDiv &fdx,
+                                            const FastDiv &fdy, const C *tw,
+                                            int &ix, int &iy, int &iz, int &dir,
+                                            C &dkf) {
+  split_index(j, fdx, fdy, ix, iy, iz);
   dir = ((ix + iy + iz) & 1) ? -1 : 1;
+  const int nx = (int)fdx.d, ny = (int)fdy.d;
   dkf = cmul(cmul(tw[ix], tw[nx + iy]), tw[nx + ny + iz]);
 }
 
 // ---------------------------------------------------------------- pass A
-template <typename T, int V, int CLOS>
-__global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a) {
+// One straight-line body per update mode (the mode is device state, read
+// once per thread): every load of a point is issued before any store.  Each
+// thread handles PTS adjacent points (2 for FP32, so each thread keeps as
+// many bytes in flight as the FP64 version).
+template <typename T, int V, int CLOS, int MODE, int PTS>
+__device__ __forceinline__ void pass_a_body(const IterArgs<T> &a, int slot, T s1, T s2, T m) {
   typedef typename Cx<T>::t C;
   constexpr int P = (V + 1) / 2;
-  const DevState *st = a.st;
-  const int done = st->done;
-  if (done && st->after_done > 0) return;     // past the snapshot: idle
-  const int mode = st->mode;
-  const int slot = st->upd_slot;
-  const T s1 = (T)st->s1, s2 = (T)st->s2, m = (T)st->m;
   const long long n = a.n;
-  const bool need_h = (mode != 0) || done;
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
-       j += (long long)gridDim.x * blockDim.x) {
-    int ix, iy, iz, dir;
-    C dkf;
-    point_phase(j, a.nx, a.ny, a.tw, ix, iy, iz, dir, dkf);
-    T h[V];
-    if (need_h) {
-      // inverse post-twiddle (timekb, fft3d.cu:52-60): (1/V) dir conj(dkf)
-      const T sc = (T)a.invvol * (T)dir;
-      C w = mk<C>(dkf.x * sc, -dkf.y * sc);
+  C *__restrict__ buf = a.buf;
+  T *__restrict__ tt = a.t;
+  const T *__restrict__ UU = a.U;
+  T *__restrict__ Y = a.Y;
+  T *__restrict__ RP = a.RP;
+  const C *__restrict__ tw = a.tw;
+  for (long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * PTS; j < n;
+       j += (long long)gridDim.x * blockDim.x * PTS) {
+    C zb[P][PTS];
+    T tv[V][PTS], Uv[V][PTS], y0[V][PTS], y1[V][PTS];
+    if (MODE != 0) {
 #pragma unroll
-      for (int p = 0; p < P; ++p) {
-        C z = cmul(a.buf[(size_t)p * n + j], w);
-        h[2 * p] = z.x;
-        if (2 * p + 1 < V) h[2 * p + 1] = z.y;
-      }
+      for (int p = 0; p < P; ++p) ldc<PTS>(buf + (size_t)p * n + j, zb[p]);
     }
-    T cc[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-      const size_t iv = (size_t)v * n + j;
-      const T t = a.t[iv];
-      const T U = a.U[iv];
-      T tn = t;
-      if (need_h) {
-        const T gold = closure<CLOS>(t - U);
-        const T R = h[v] + T(1) - gold;          // tr, calculate_cuda.cu:64
-        if (done) {
-          if (a.hout) { a.hout[iv] = (double)h[v]; a.gout[iv] = (double)gold; }
-        }
-        if (mode == 1) {                         // newdt0 (Picard)
-          a.Y[(size_t)slot * V * n + iv] = t + m * R;
-          a.RP[(size_t)slot * V * n + iv] = R;
-          tn = t + R;
-        } else if (mode == 2) {                  // newdt (AN2)
-          const T y = t + m * R;
-          const T y0 = a.Y[iv];
-          const T y1 = a.Y[(size_t)V * n + iv];
-          tn = y + s1 * (y0 - y) + s2 * (y1 - y);
-          a.Y[(size_t)slot * V * n + iv] = y;
-          a.RP[(size_t)slot * V * n + iv] = R;
-        }
-        if (mode != 0 && (!done || done == 3)) a.t[iv] = tn;
+      ldr<PTS>(tt + (size_t)v * n + j, tv[v]);
+      ldr<PTS>(UU + (size_t)v * n + j, Uv[v]);
+      if (MODE == 2) {
+        ldr<PTS>(Y + (size_t)v * n + j, y0[v]);
+        ldr<PTS>(Y + (size_t)(V + v) * n + j, y1[v]);
       }
-      // closure + c_SR (kh/hnc + trm1mt, calculate_cuda.cu:1-29)
-      const T g = closure<CLOS>(tn - U);
-      cc[v] = g - T(1) - tn;
     }
-    if (done) continue;
+    int ix, iy, iz, dir0;
+    C dkf[PTS];
+    point_phase(j, a.fdx, a.fdy, tw, ix, iy, iz, dir0, dkf[0]);
+    if (PTS == 2) dkf[PTS - 1] = cmul(cmul(tw[ix + 1], tw[a.nx + iy]), tw[a.nx + a.ny + iz]);
+    T tn[V][PTS];
+    if (MODE != 0) {
+      T yw[V][PTS], rw[V][PTS];
+#pragma unroll
+      for (int k = 0; k < PTS; ++k) {
+        const int dir = (k & 1) ? -dir0 : dir0;
+        // inverse post-twiddle (timekb, fft3d.cu:52-60): (1/V) dir conj(dkf)
+        const T sc = (T)a.invvol * (T)dir;
+        const C w = mk<C>(dkf[k].x * sc, -dkf[k].y * sc);
+        T h[V];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          C z = cmul(zb[p][k], w);
+          h[2 * p] = z.x;
+          if (2 * p + 1 < V) h[2 * p + 1] = z.y;
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const T R = h[v] + T(1) - closure<CLOS>(tv[v][k] - Uv[v][k]);   // tr
+          rw[v][k] = R;
+          if (MODE == 1) {                       // newdt0 (Picard)
+            yw[v][k] = tv[v][k] + m * R;
+            tn[v][k] = tv[v][k] + R;
+          } else {                               // newdt (AN2)
+            const T y = tv[v][k] + m * R;
+            yw[v][k] = y;
+            tn[v][k] = y + s1 * (y0[v][k] - y) + s2 * (y1[v][k] - y);
+          }
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const size_t iv = (size_t)v * n + j;
+        str<PTS>(Y + (size_t)slot * V * n + iv, yw[v]);
+        str<PTS>(RP + (size_t)slot * V * n + iv, rw[v]);
+        str<PTS>(tt + iv, tn[v]);
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+#pragma unroll
+        for (int k = 0; k < PTS; ++k) tn[v][k] = tv[v][k];
+    }
+    // closure + c_SR (kh/hnc + trm1mt, calculate_cuda.cu:1-29) and the
     // forward pre-twiddle (timekf, fft3d.cu:41-49): dir * dkf * (c_a + i c_b)
-    const C wf = mk<C>(dkf.x * dir, dkf.y * dir);
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-      C z;
-      z.x = cc[2 * p];
-      z.y = (2 * p + 1 < V) ? cc[2 * p + 1] : T(0);
-      a.buf[(size_t)p * n + j] = cmul(z, wf);
+      C out[PTS];
+#pragma unroll
+      for (int k = 0; k < PTS; ++k) {
+        const int dir = (k & 1) ? -dir0 : dir0;
+        const C wf = mk<C>(dkf[k].x * dir, dkf[k].y * dir);
+        C z;
+        z.x = closure<CLOS>(tn[2 * p][k] - Uv[2 * p][k]) - T(1) - tn[2 * p][k];
+        z.y = (2 * p + 1 < V)
+                  ? closure<CLOS>(tn[2 * p + 1][k] - Uv[2 * p + 1][k]) - T(1) - tn[2 * p + 1][k]
+                  : T(0);
+        out[k] = cmul(z, wf);
+      }
+      stc<PTS>(buf + (size_t)p * n + j, out);
     }
   }
 }
 
-// ---------------------------------------------------------------- pass K
-template <typename T, int V>
-__global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a) {
-  typedef typename Cx<T>::t C;
-  constexpr int P = (V + 1) / 2;
-  if (a.st->done) return;
-  const long long n = a.n, nh = n / 2;
-  const StageParams *sp = a.sp;
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nh;
-       j += (long long)gridDim.x * blockDim.x) {
-    const long long jm = n - 1 - j;             // k(jm) = -k(j)
-    long long r = j / a.nx;
-    const int ix = (int)(j - r * a.nx);
-    const int iy = (int)(r % a.ny), iz = (int)(r / a.ny);
-    const int dir = ((ix + iy + iz) & 1) ? -1 : 1;
-    // set_g (initialize_g.cu:58-62)
-    const double kx = 2.0 * kPi * (ix - a.nx / 2.0 + 0.5) / a.bx;
-    const double ky = 2.0 * kPi * (iy - a.ny / 2.0 + 0.5) / a.by;
-    const double kz = 2.0 * kPi * (iz - a.nz / 2.0 + 0.5) / a.bz;
-    const double kk = sqrt(kx * kx + ky * ky + kz * kz);
-    const double2 fk = a.fkh[j];
-    // unpack the site pairs and finish the forward transform
-    // (timeirvol * dv, fft3d.cu:32) and subtract q cf fk (mqvfk)
-    C F[V];
-    const T sc = (T)(a.dv * 0.5 * dir);
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-      const C y = a.buf[(size_t)p * n + j];
-      const C ym = a.buf[(size_t)p * n + jm];
-      const double qa = sp->qcf[2 * p];
-      F[2 * p] = mk<C>(sc * (y.x - ym.x) - qa * fk.x, sc * (y.y + ym.y) - qa * fk.y);
-      if (2 * p + 1 < V) {
-        const double qb = sp->qcf[2 * p + 1];
-        F[2 * p + 1] = mk<C>(sc * (y.y - ym.y) - qb * fk.x, -sc * (y.x + ym.x) - qb * fk.y);
-      }
-    }
-    // chi_ab(|k|): natural spline on knots k_i = dk (i+1), bisection
-    // semantics of splint.cc:9-16 reproduced on the uniform knots
-    int k0 = (int)(kk / a.dk) - 1;
-    k0 = k0 < 0 ? 0 : (k0 > a.ntab - 2 ? a.ntab - 2 : k0);
-    while (k0 < a.ntab - 2 && a.dk * (k0 + 2) <= kk) ++k0;
-    while (k0 > 0 && a.dk * (k0 + 1) > kk) --k0;
-    const double tt = kk - a.dk * (k0 + 1);
-    const double *cf = a.chi + (size_t)k0 * V * V * 4;
-    C H[V];
-#pragma unroll
-    for (int va = 0; va < V; ++va) {
-      T hr = 0, hi = 0;
-#pragma unroll
-      for (int vb = 0; vb < V; ++vb) {
-        const double *q = cf + (va * V + vb) * 4;
-        const T x = (T)(((q[3] * tt + q[2]) * tt + q[1]) * tt + q[0]);
-        hr += F[vb].x * x;                       // oz, calculate_cuda.cu:44-58
-        hi += F[vb].y * x;
-      }
-      H[va] = mk<C>(hr, hi);
-    }
-    // repack for the inverse: dir (h_a + i h_b) at k and its mirror
-    // (timeirvol before the inverse, fft3d.cu:34)
-    const T d = (T)dir;
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-      const C ha = H[2 * p];
-      const C hb = (2 * p + 1 < V) ? H[2 * p + 1] : mk<C>(0.0, 0.0);
-      a.buf[(size_t)p * n + j] = mk<C>(d * (ha.x - hb.y), d * (ha.y + hb.x));
-      a.buf[(size_t)p * n + jm] = mk<C>(-d * (ha.x + hb.y), -d * (hb.x - ha.y));
-    }
-  }
-}
-
-// ---------------------------------------------------------------- pass R
+// First pass after the loop stopped: snapshot h (Re of the last OZ) and g
+// (closure of the t used in that cycle), and when maxstep ended the loop
+// apply the pending update as the reference does (iterate.cu:61 runs
+// ma->calculate before the step bound is tested).
 template <typename T, int V, int CLOS>
-__global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a) {
+__device__ void pass_a_final(const IterArgs<T> &a, int mode, int done, int slot, T s1,
+                             T s2, T m) {
   typedef typename Cx<T>::t C;
   constexpr int P = (V + 1) / 2;
-  __shared__ double red[kThreads / 32][6];
-  const DevState *st = a.st;
-  if (st->done) return;
-  const bool gram = st->count <= 0;
   const long long n = a.n;
-  const StageParams *sp = a.sp;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
   for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
        j += (long long)gridDim.x * blockDim.x) {
     int ix, iy, iz, dir;
     C dkf;
-    point_phase(j, a.nx, a.ny, a.tw, ix, iy, iz, dir, dkf);
+    point_phase(j, a.fdx, a.fdy, a.tw, ix, iy, iz, dir, dkf);
     const T sc = (T)a.invvol * (T)dir;
     const C w = mk<C>(dkf.x * sc, -dkf.y * sc);
     T h[V];
@@ -272,18 +287,196 @@ __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a) {
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const size_t iv = (size_t)v * n + j;
-      const T g = closure<CLOS>(a.t[iv] - a.U[iv]);
-      const double R = (double)(h[v] + T(1) - g);
-      acc[0] += R * R;                          // cal_rms.cu:18
-      if (gram) {                               // theta30, anderson_cuda.cu:33-39
-        const double w8 = sp->irho[v];
-        const double d0 = R - (double)a.RP[iv];
-        const double d1 = R - (double)a.RP[(size_t)V * n + iv];
-        acc[1] += w8 * R * d0;
-        acc[2] += w8 * R * d1;
-        acc[3] += w8 * d0 * d0;
-        acc[4] += w8 * d0 * d1;
-        acc[5] += w8 * d1 * d1;
+      const T t = a.t[iv];
+      const T gold = closure<CLOS>(t - a.U[iv]);
+      if (a.hout) { a.hout[iv] = (double)h[v]; a.gout[iv] = (double)gold; }
+      if (done == 3 && mode != 0) {
+        const T R = h[v] + T(1) - gold;
+        const T y = t + m * R;
+        T tn = t + R;
+        if (mode == 2) tn = y + s1 * (a.Y[iv] - y) + s2 * (a.Y[(size_t)V * n + iv] - y);
+        a.Y[(size_t)slot * V * n + iv] = y;
+        a.RP[(size_t)slot * V * n + iv] = R;
+        a.t[iv] = tn;
+      }
+    }
+  }
+}
+
+template <typename T, int V, int CLOS>
+__global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a) {
+  const DevState *st = a.st;
+  const int done = st->done;
+  const int mode = st->mode;
+  const int slot = st->upd_slot;
+  const T s1 = (T)st->s1, s2 = (T)st->s2, m = (T)st->m;
+  if (done) {
+    if (st->after_done == 0) pass_a_final<T, V, CLOS>(a, mode, done, slot, s1, s2, m);
+    return;                                     // past the snapshot: idle
+  }
+  constexpr int PTS = sizeof(T) == 4 ? 2 : 1;
+  if (mode == 2) pass_a_body<T, V, CLOS, 2, PTS>(a, slot, s1, s2, m);
+  else if (mode == 1) pass_a_body<T, V, CLOS, 1, PTS>(a, slot, s1, s2, m);
+  else pass_a_body<T, V, CLOS, 0, PTS>(a, slot, s1, s2, m);
+}
+
+// ---------------------------------------------------------------- pass K
+template <typename T, int V>
+__global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a) {
+  typedef typename Cx<T>::t C;
+  constexpr int P = (V + 1) / 2;
+  if (a.st->done) return;
+  const long long n = a.n, nh = n / 2;
+  const StageParams *sp = a.sp;
+  C *__restrict__ buf = a.buf;
+  const double2 *__restrict__ fkh = a.fkh;
+  const double *__restrict__ chi = a.chi;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nh;
+       j += (long long)gridDim.x * blockDim.x) {
+    const long long jm = n - 1 - j;             // k(jm) = -k(j)
+    int ix, iy, iz;
+    split_index(j, a.fdx, a.fdy, ix, iy, iz);
+    const int dir = ((ix + iy + iz) & 1) ? -1 : 1;
+    const double2 fk = fkh[j];
+    // unpack the site pairs and finish the forward transform
+    // (timeirvol * dv, fft3d.cu:32) and subtract q cf fk (mqvfk)
+    C F[V];
+    const T sc = (T)(a.dv * 0.5 * dir);
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const C y = buf[(size_t)p * n + j];
+      const C ym = buf[(size_t)p * n + jm];
+      const double qa = sp->qcf[2 * p];
+      F[2 * p] = mk<C>(sc * (y.x - ym.x) - qa * fk.x, sc * (y.y + ym.y) - qa * fk.y);
+      if (2 * p + 1 < V) {
+        const double qb = sp->qcf[2 * p + 1];
+        F[2 * p + 1] = mk<C>(sc * (y.y - ym.y) - qb * fk.x, -sc * (y.x + ym.x) - qb * fk.y);
+      }
+    }
+    // chi_ab(|k|) (solvent_spline.cu:36-47, applied per point by oz)
+    double X[V * V];
+    if (a.xs) {
+      // cubic cell: |k| = (pi/L) sqrt(s), s = sum of three odd squares
+      const int ox = 2 * ix - a.nx + 1, oy = 2 * iy - a.ny + 1, oz = 2 * iz - a.nz + 1;
+      const unsigned sq = (unsigned)(ox * ox + oy * oy + oz * oz);
+      const double2 *xr = reinterpret_cast<const double2 *>(a.xs + (size_t)((sq - 3u) >> 3) * V * V);
+#pragma unroll
+      for (int ab = 0; ab < V * V / 2; ++ab) {
+        const double2 q = xr[ab];
+        X[2 * ab] = q.x;
+        X[2 * ab + 1] = q.y;
+      }
+      if (V * V % 2) X[V * V - 1] = a.xs[(size_t)((sq - 3u) >> 3) * V * V + V * V - 1];
+    } else {
+      // general cell: natural spline on knots k_i = dk (i+1) with the
+      // bisection semantics of splint.cc:9-16 on uniform knots
+      const double kx = 2.0 * kPi * (ix - a.nx / 2.0 + 0.5) / a.bx;   // set_g
+      const double ky = 2.0 * kPi * (iy - a.ny / 2.0 + 0.5) / a.by;
+      const double kz = 2.0 * kPi * (iz - a.nz / 2.0 + 0.5) / a.bz;
+      const double kk = sqrt(kx * kx + ky * ky + kz * kz);
+      int k0 = (int)(kk / a.dk) - 1;
+      k0 = k0 < 0 ? 0 : (k0 > a.ntab - 2 ? a.ntab - 2 : k0);
+      while (k0 < a.ntab - 2 && a.dk * (k0 + 2) <= kk) ++k0;
+      while (k0 > 0 && a.dk * (k0 + 1) > kk) --k0;
+      const double tt = kk - a.dk * (k0 + 1);
+      const double2 *cf = reinterpret_cast<const double2 *>(chi + (size_t)k0 * V * V * 4);
+#pragma unroll
+      for (int ab = 0; ab < V * V; ++ab) {
+        const double2 lo = cf[2 * ab], hi2 = cf[2 * ab + 1];
+        X[ab] = ((hi2.y * tt + hi2.x) * tt + lo.y) * tt + lo.x;
+      }
+    }
+    C H[V];
+#pragma unroll
+    for (int va = 0; va < V; ++va) {
+      T hr = 0, hi = 0;
+#pragma unroll
+      for (int vb = 0; vb < V; ++vb) {
+        const T x = (T)X[va * V + vb];
+        hr += F[vb].x * x;                       // oz, calculate_cuda.cu:44-58
+        hi += F[vb].y * x;
+      }
+      H[va] = mk<C>(hr, hi);
+    }
+    // repack for the inverse: dir (h_a + i h_b) at k and its mirror
+    // (timeirvol before the inverse, fft3d.cu:34)
+    const T d = (T)dir;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const C ha = H[2 * p];
+      const C hb = (2 * p + 1 < V) ? H[2 * p + 1] : mk<C>(0.0, 0.0);
+      buf[(size_t)p * n + j] = mk<C>(d * (ha.x - hb.y), d * (ha.y + hb.x));
+      buf[(size_t)p * n + jm] = mk<C>(-d * (ha.x + hb.y), -d * (hb.x - ha.y));
+    }
+  }
+}
+
+// ---------------------------------------------------------------- pass R
+template <typename T, int V, int CLOS>
+__global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a) {
+  typedef typename Cx<T>::t C;
+  constexpr int P = (V + 1) / 2;
+  constexpr int PTS = sizeof(T) == 4 ? 2 : 1;
+  __shared__ double red[kThreads / 32][6];
+  const DevState *st = a.st;
+  if (st->done) return;
+  const bool gram = st->count <= 0;
+  const long long n = a.n;
+  const StageParams *sp = a.sp;
+  const C *__restrict__ buf = a.buf;
+  const T *__restrict__ tt = a.t;
+  const T *__restrict__ UU = a.U;
+  const T *__restrict__ RP = a.RP;
+  const C *__restrict__ tw = a.tw;
+  double w8[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) w8[v] = sp->irho[v];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * PTS; j < n;
+       j += (long long)gridDim.x * blockDim.x * PTS) {
+    C zb[P][PTS];
+    T tv[V][PTS], Uv[V][PTS], r0[V][PTS], r1[V][PTS];
+#pragma unroll
+    for (int p = 0; p < P; ++p) ldc<PTS>(buf + (size_t)p * n + j, zb[p]);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      ldr<PTS>(tt + (size_t)v * n + j, tv[v]);
+      ldr<PTS>(UU + (size_t)v * n + j, Uv[v]);
+      if (gram) {
+        ldr<PTS>(RP + (size_t)v * n + j, r0[v]);
+        ldr<PTS>(RP + (size_t)(V + v) * n + j, r1[v]);
+      }
+    }
+    int ix, iy, iz, dir0;
+    C dkf[PTS];
+    point_phase(j, a.fdx, a.fdy, tw, ix, iy, iz, dir0, dkf[0]);
+    if (PTS == 2) dkf[PTS - 1] = cmul(cmul(tw[ix + 1], tw[a.nx + iy]), tw[a.nx + a.ny + iz]);
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) {
+      const int dir = (k & 1) ? -dir0 : dir0;
+      const T sc = (T)a.invvol * (T)dir;
+      const C w = mk<C>(dkf[k].x * sc, -dkf[k].y * sc);
+      T h[V];
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        C z = cmul(zb[p][k], w);
+        h[2 * p] = z.x;
+        if (2 * p + 1 < V) h[2 * p + 1] = z.y;
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const T g = closure<CLOS>(tv[v][k] - Uv[v][k]);
+        const double R = (double)(h[v] + T(1) - g);
+        acc[0] += R * R;                          // cal_rms.cu:18
+        if (gram) {                               // theta30, anderson_cuda.cu:33-39
+          const double d0 = R - (double)r0[v][k];
+          const double d1 = R - (double)r1[v][k];
+          acc[1] += w8[v] * R * d0;
+          acc[2] += w8[v] * R * d1;
+          acc[3] += w8[v] * d0 * d0;
+          acc[4] += w8[v] * d0 * d1;
+          acc[5] += w8[v] * d1 * d1;
+        }
       }
     }
   }
@@ -433,6 +626,8 @@ template <typename T>
 IterArgs<T> make_args(Context &c, bool fp64) {
   IterArgs<T> a{};
   a.n = c.n; a.nx = c.nx; a.ny = c.ny; a.nz = c.nz;
+  a.fdx = FastDiv((unsigned)c.nx); a.fdy = FastDiv((unsigned)c.ny);
+  a.xs = c.d_xs;
   a.invvol = 1.0 / c.vol; a.dv = c.dv;
   a.fkh = c.d_fkh; a.chi = c.chi.d_coef; a.ntab = c.chi.ntab; a.dk = c.chi.dk;
   a.bx = c.prm.box[0]; a.by = c.prm.box[1]; a.bz = c.prm.box[2];
@@ -505,6 +700,7 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
   while (!stop) {
     if (L.graph) cudaGraphLaunch(L.exec, c.stream);
     else launch_iteration<T, V, CLOS>(c, a, plan);
+    c.launches += 4;
     cudaMemcpyAsync(&c.h_state[launched % kRing], c.d_state, sizeof(DevState),
                     cudaMemcpyDeviceToHost, c.stream);
     cudaEventRecord(ev[launched % kRing], c.stream);
@@ -527,6 +723,7 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
   if (status == RISM3D_OK) {
     if (L.graph) cudaGraphLaunch(L.exec, c.stream);
     else launch_iteration<T, V, CLOS>(c, a, plan);
+    c.launches += 4;
     cudaMemcpyAsync(&c.h_state[0], c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream);
     if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "iteration drain")) status = RISM3D_CUDA_ERROR;
   }
@@ -572,6 +769,7 @@ int solve_v(Context &c, int chargeup) {
       return RISM3D_CUDA_ERROR;
   }
   k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, d_tinit, c.d_fr, c.d_stage, c.d_t);
+  c.launches += 1;
   if (d_tinit) cudaFreeAsync(d_tinit, c.stream);
 
   int total = 0, total32 = 0, status = RISM3D_OK;
@@ -585,12 +783,17 @@ int solve_v(Context &c, int chargeup) {
       for (int v = 0; v < V; ++v) step.qcf[v] = c.qv[v] * (cfn - cf);
       cudaMemcpyAsync(d_step, &step, sizeof(step), cudaMemcpyHostToDevice, c.stream);
       k_shift_history<double><<<gb, kThreads, 0, c.stream>>>(n, V, c.d_fr, d_step, c.d_Y);
-      if (mixed) k_shift_history<float><<<gb, kThreads, 0, c.stream>>>(n, V, c.d_fr, d_step, c.f_Y);
+      c.launches += 1;
+      if (mixed) {
+        k_shift_history<float><<<gb, kThreads, 0, c.stream>>>(n, V, c.d_fr, d_step, c.f_Y);
+        c.launches += 1;
+      }
       cf = cfn;
     }
     for (int v = 0; v < V; ++v) sp.qcf[v] = c.qv[v] * cf;
     cudaMemcpyAsync(c.d_stage, &sp, sizeof(sp), cudaMemcpyHostToDevice, c.stream);
     k_stage_u<<<gb, kThreads, 0, c.stream>>>(n, V, c.d_u, c.d_e, c.d_stage, c.d_U, mixed ? c.f_U : nullptr);
+    c.launches += 1;
     if (c.prm.verbose) printf("relaxing 3D UV RISM: Charge Up Factor = %g\n", cf);
     int left = c.prm.maxstep;
     if (mixed) {
@@ -600,6 +803,7 @@ int solve_v(Context &c, int chargeup) {
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(vn, c.d_t, c.f_t);
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.d_Y, c.f_Y);
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.d_RP, c.f_RP);
+      c.launches += 3;
       double sw = c.prm.mixed_switch > 0 ? c.prm.mixed_switch : 5.0 * c.prm.convergence;
       if (sw < c.prm.convergence) sw = c.prm.convergence;
       int it32 = 0;
@@ -614,10 +818,12 @@ int solve_v(Context &c, int chargeup) {
       if (s32.done == 2) {
         // FP32 diverged: restart this stage in FP64 from the stage start
         k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, nullptr, c.d_fr, c.d_stage, c.d_t);
+        c.launches += 1;
       } else {
         k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(vn, c.f_t, c.d_t);
         k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.f_Y, c.d_Y);
         k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.f_RP, c.d_RP);
+        c.launches += 3;
       }
       if (left < 1) left = 1;
     }
@@ -645,6 +851,61 @@ int solve_v(Context &c, int chargeup) {
   c.res.status = status;
   if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "solve")) return RISM3D_CUDA_ERROR;
   return (status == RISM3D_CUDA_ERROR || status == RISM3D_CUFFT_ERROR) ? status : RISM3D_OK;
+}
+
+template <typename T, int V, int CLOS>
+int time_kernel_t(Context &c, int which, int reps, double *ms) {
+  const bool fp64 = sizeof(T) == 8;
+  IterArgs<T> a = make_args<T>(c, fp64);
+  if (fp64) {
+    a.buf = (typename Cx<T>::t *)c.d_buf; a.t = (T *)c.d_t; a.U = (T *)c.d_U;
+    a.Y = (T *)c.d_Y; a.RP = (T *)c.d_RP;
+  } else {
+    if (!c.f_buf) { c.err = "FP32 kernels need a MIXED context"; return RISM3D_BAD_STATE; }
+    a.buf = (typename Cx<T>::t *)c.f_buf; a.t = (T *)c.f_t; a.U = (T *)c.f_U;
+    a.Y = (T *)c.f_Y; a.RP = (T *)c.f_RP;
+  }
+  a.tw = (const typename Cx<T>::t *)(fp64 ? (void *)c.d_tw : (void *)c.d_twf);
+  DevState saved, run;
+  cudaMemcpy(&saved, c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost);
+  run = saved;
+  run.done = 0; run.after_done = 0; run.mode = 2; run.count = 0; run.upd_slot = 0;
+  run.s1 = 0.25; run.s2 = 0.25;
+  cudaMemcpy(c.d_state, &run, sizeof(DevState), cudaMemcpyHostToDevice);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int ba = grid_blocks(a.n), bk = grid_blocks(a.n / 2);
+  cudaEventRecord(e0, c.stream);
+  for (int r = 0; r < reps; ++r) {
+    switch (which % 10) {
+      case 0: k_pass_a<T, V, CLOS><<<ba, kThreads, 0, c.stream>>>(a); break;
+      case 1: k_kspace<T, V><<<bk, kThreads, 0, c.stream>>>(a); break;
+      default: k_pass_r<T, V, CLOS><<<a.nblocks, kThreads, 0, c.stream>>>(a); break;
+    }
+  }
+  cudaEventRecord(e1, c.stream);
+  c.launches += reps;
+  cudaError_t e = cudaEventSynchronize(e1);
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaMemcpy(c.d_state, &saved, sizeof(DevState), cudaMemcpyHostToDevice);
+  c.solved = false;
+  c.have_forces = false;
+  if (!cuda_ok(c, e, "time_kernel")) return RISM3D_CUDA_ERROR;
+  *ms = t / reps;
+  return RISM3D_OK;
+}
+
+template <int V>
+int time_c(Context &c, int which, int reps, double *ms) {
+  const bool kh = c.prm.closure == RISM3D_KH;
+  if (which < 10) return kh ? time_kernel_t<double, V, 0>(c, which, reps, ms)
+                            : time_kernel_t<double, V, 1>(c, which, reps, ms);
+  return kh ? time_kernel_t<float, V, 0>(c, which, reps, ms)
+            : time_kernel_t<float, V, 1>(c, which, reps, ms);
 }
 
 template <int V>
@@ -727,12 +988,72 @@ int upload_chi(Context &c) {
         }
       }
     }
+  // Cubic cells: evaluate the spline once per distinct |k|^2 (the sorted
+  // unique-|k| table of initialize_g.cu:31-43, indexed directly).
+  if (c.d_xs) { cudaFree(c.d_xs); c.d_xs = nullptr; c.nxs = 0; }
+  if (c.nx == c.ny && c.nx == c.nz && c.prm.box[0] == c.prm.box[1] &&
+      c.prm.box[0] == c.prm.box[2]) {
+    const long long nm = c.nx - 1;
+    const int nidx = (int)((3 * nm * nm - 3) / 8 + 1);
+    std::vector<double> xs((size_t)nidx * V * V);
+    for (int idx = 0; idx < nidx; ++idx) {
+      const double kk = kPi / c.prm.box[0] * sqrt((double)(8LL * idx + 3));
+      int klo = 0, khi = nt - 1;                               // splint.cc:9-16
+      while (khi - klo > 1) {
+        int k = (khi + klo) >> 1;
+        if (xp[k] > kk) khi = k; else klo = k;
+      }
+      const double t = kk - xp[klo];
+      for (int ab = 0; ab < V * V; ++ab) {
+        const double *o = &tab[((size_t)klo * V * V + ab) * 4];
+        xs[(size_t)idx * V * V + ab] = ((o[3] * t + o[2]) * t + o[1]) * t + o[0];
+      }
+    }
+    if (!cuda_ok(c, cudaMalloc(&c.d_xs, sizeof(double) * xs.size()), "chi table alloc") ||
+        !cuda_ok(c, cudaMemcpy(c.d_xs, xs.data(), sizeof(double) * xs.size(), cudaMemcpyHostToDevice), "chi table copy"))
+      return RISM3D_CUDA_ERROR;
+    c.nxs = nidx;
+  }
   if (c.chi.d_coef) cudaFree(c.chi.d_coef);
   if (!cuda_ok(c, cudaMalloc(&c.chi.d_coef, sizeof(double) * tab.size()), "chi alloc") ||
       !cuda_ok(c, cudaMemcpyAsync(c.chi.d_coef, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c.stream), "chi copy") ||
       !cuda_ok(c, cudaStreamSynchronize(c.stream), "chi"))
     return RISM3D_CUDA_ERROR;
   return RISM3D_OK;
+}
+
+int time_kernel(Context &c, int which, int reps, double *ms) {
+  if (which == 20) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c.stream);
+    for (int r = 0; r < reps; ++r) launch_potential_r(c);
+    cudaEventRecord(e1, c.stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!cuda_ok(c, e, "time_kernel")) return RISM3D_CUDA_ERROR;
+    *ms = t / reps;
+    return RISM3D_OK;
+  }
+  if (!(which >= 0 && which <= 2) && !(which >= 10 && which <= 12)) {
+    c.err = "unknown kernel id";
+    return RISM3D_BAD_INPUT;
+  }
+  switch (c.natv) {
+    case 1: return time_c<1>(c, which, reps, ms);
+    case 2: return time_c<2>(c, which, reps, ms);
+    case 3: return time_c<3>(c, which, reps, ms);
+    case 4: return time_c<4>(c, which, reps, ms);
+    case 5: return time_c<5>(c, which, reps, ms);
+    case 6: return time_c<6>(c, which, reps, ms);
+    case 7: return time_c<7>(c, which, reps, ms);
+    case 8: return time_c<8>(c, which, reps, ms);
+  }
+  return RISM3D_UNSUPPORTED_SHAPE;
 }
 
 int run_solve(Context &c, int chargeup) {

@@ -24,7 +24,8 @@ GRID_G, GRID_H, GRID_C, GRID_T, GRID_U, GRID_E, GRID_FR, GRID_QV = range(8)
 EXPORTS = ["rism3d_create", "rism3d_set_solvent", "rism3d_set_solute", "rism3d_set_tuv",
            "rism3d_solve", "rism3d_euv", "rism3d_forces", "rism3d_grad", "rism3d_get_grid",
            "rism3d_solve_batch", "rism3d_destroy", "rism3d_last_error",
-           "rism3d_initialize", "rism3d_iterate", "rism3d_output"]
+           "rism3d_initialize", "rism3d_iterate", "rism3d_output",
+           "rism3d_refresh_potentials", "rism3d_kernel_launches", "rism3d_time_kernel"]
 
 
 class RismError(RuntimeError):
@@ -37,7 +38,8 @@ class Params(C.Structure):
     _fields_ = [("grid", C.c_int * 3), ("box", C.c_double * 3), ("closure", C.c_int),
                 ("convergence", C.c_double), ("maxstep", C.c_int), ("an2_count", C.c_int),
                 ("an2_m", C.c_double), ("an2_mp", C.c_double), ("precision", C.c_int),
-                ("mixed_switch", C.c_double), ("device", C.c_int), ("verbose", C.c_int)]
+                ("mixed_switch", C.c_double), ("device", C.c_int), ("verbose", C.c_int),
+                ("stream", C.c_void_p)]
 
 
 class Result(C.Structure):
@@ -91,6 +93,10 @@ def lib():
                                         C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int]
         L.rism3d_iterate.argtypes = [vp, C.c_int]
         L.rism3d_output.argtypes = [vp]
+        L.rism3d_refresh_potentials.argtypes = [vp]
+        L.rism3d_kernel_launches.argtypes = [vp]
+        L.rism3d_kernel_launches.restype = C.c_longlong
+        L.rism3d_time_kernel.argtypes = [vp, C.c_int, C.c_int, d]
         _lib = L
     return _lib
 
@@ -108,7 +114,7 @@ class Solver:
 
     def __init__(self, grid, box, closure=KH, convergence=1e-6, maxstep=10000,
                  an2=(2, 0.6, 0.2), precision=FP64, mixed_switch=0.0, device=0,
-                 verbose=0):
+                 verbose=0, stream=None):
         L = lib()
         p = Params()
         p.grid[:] = [int(g) for g in grid]
@@ -116,6 +122,7 @@ class Solver:
         p.closure, p.convergence, p.maxstep = closure, convergence, maxstep
         p.an2_count, p.an2_m, p.an2_mp = int(an2[0]), float(an2[1]), float(an2[2])
         p.precision, p.mixed_switch, p.device, p.verbose = precision, mixed_switch, device, verbose
+        p.stream = stream
         h = C.c_void_p()
         rc = L.rism3d_create(C.byref(p), C.byref(h))
         if rc != OK:
@@ -179,6 +186,17 @@ class Solver:
         dR = np.zeros((self.natom, 3))
         self._check(lib().rism3d_grad(self.h, _dp(dq), _dp(ds), _dp(de), _dp(dR)))
         return dq, ds, de, dR
+
+    def refresh_potentials(self):
+        self._check(lib().rism3d_refresh_potentials(self.h))
+
+    def kernel_launches(self):
+        return int(lib().rism3d_kernel_launches(self.h))
+
+    def time_kernel(self, which, reps):
+        ms = np.zeros(1)
+        self._check(lib().rism3d_time_kernel(self.h, which, reps, _dp(ms)))
+        return float(ms[0])
 
     def close(self):
         if getattr(self, "h", None):

@@ -69,6 +69,9 @@ typedef struct {
   double mixed_switch;    /* MIXED: leave FP32 once rms <= this (0 = auto) */
   int device;             /* CUDA ordinal (main.cu:57) */
   int verbose;            /* 1: print " Step = n Reside = r" like iterate.cu:63 */
+  void *stream;           /* caller-owned cudaStream_t for all work; NULL: the
+                             context creates its own (the reference uses the
+                             legacy default stream) */
 } rism3d_params;
 
 typedef struct {
@@ -142,6 +145,22 @@ int rism3d_forces(rism3d_ctx *ctx, double *dulj, double *due);
  * recomputed.  Any output pointer may be NULL.  dmu_dR is [natom][3]. */
 int rism3d_grad(rism3d_ctx *ctx, double *dmu_dq, double *dmu_dsig,
                 double *dmu_deps, double *dmu_dR);
+
+/* Recompute the potential grids from the solute already on the device
+ * (no host->device traffic); the next rism3d_solve starts from them. */
+int rism3d_refresh_potentials(rism3d_ctx *ctx);
+
+/* Kernels of this library launched by ctx so far (cuFFT's own kernels are
+ * not counted). */
+long long rism3d_kernel_launches(const rism3d_ctx *ctx);
+
+/* Measurement hook: launch one kernel `reps` times back to back on the
+ * context stream and report the mean device time per launch (CUDA events).
+ * which: 0/1/2 = FP64 pass A / pass K / pass R, 10/11/12 = the FP32
+ * versions (MIXED contexts), 20 = real-space potential kernel.  The
+ * iteration kernels run on the current state with an AN2 update armed, so
+ * the stored solution is invalid afterwards (solve again to restore it). */
+int rism3d_time_kernel(rism3d_ctx *ctx, int which, int reps, double *ms_per_launch);
 
 /* Copy a result grid to host memory (see RISM3D_GRID_*). */
 int rism3d_get_grid(rism3d_ctx *ctx, int which, double *host);
