@@ -51,6 +51,11 @@ void free_device(Context &c) {
   c.d_xs = nullptr; c.nxs = 0;
   if (c.h_state) cudaFreeHost(c.h_state);
   c.h_state = nullptr;
+  if (c.graph64) cudaGraphExecDestroy(c.graph64);
+  if (c.graph32) cudaGraphExecDestroy(c.graph32);
+  c.graph64 = c.graph32 = nullptr;
+  if (c.d_count) cudaFree(c.d_count);
+  c.d_count = nullptr;
   if (c.plan64) cufftDestroy(c.plan64);
   if (c.plan32) cufftDestroy(c.plan32);
   c.plan64 = c.plan32 = 0;
@@ -60,7 +65,9 @@ void free_device(Context &c) {
 int fetch_grid(Context &c, int which, double *host) {
   const size_t n = (size_t)c.n, V = (size_t)c.natv;
   auto get = [&](const double *d, double *h, size_t cnt) {
-    return cuda_ok(c, cudaMemcpy(h, d, sizeof(double) * cnt, cudaMemcpyDeviceToHost), "get_grid");
+    return cuda_ok(c, cudaMemcpyAsync(h, d, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c.stream),
+                   "get_grid") &&
+           cuda_ok(c, cudaStreamSynchronize(c.stream), "get_grid");
   };
   switch (which) {
     case RISM3D_GRID_U: return get(c.d_u, host, V * n) ? RISM3D_OK : RISM3D_CUDA_ERROR;
@@ -203,7 +210,9 @@ int rism3d_create(const rism3d_params *p, rism3d_ctx **out) {
             cuda_ok(c, cudaHostAlloc(&c.h_state, sizeof(DevState) * 4, cudaHostAllocDefault), "alloc pinned");
   long long nb = (c.n + 255) / 256;
   c.nred_blocks = (int)(nb < 148 * 8 ? nb : 148 * 8);
-  ok = ok && cuda_ok(c, cudaMalloc(&c.d_part, sizeof(double) * 64 * c.nred_blocks), "alloc partials");
+  ok = ok && cuda_ok(c, cudaMalloc(&c.d_part, sizeof(double) * 64 * c.nred_blocks), "alloc partials") &&
+       cuda_ok(c, cudaMalloc(&c.d_count, sizeof(unsigned)), "alloc counter") &&
+       cuda_ok(c, cudaMemset(c.d_count, 0, sizeof(unsigned)), "zero counter");
   for (Timer *t : {&c.tm_setup, &c.tm_iter, &c.tm_obs}) {
     cudaEventCreate(&t->a);
     cudaEventCreate(&t->b);

@@ -33,6 +33,7 @@ struct DevState {
   int binary;      // AN2 ping-pong bit for the following update
   int count;       // Picard warm-up steps left
   int maxstep;
+  int measure;     // 1: the finalize only records the sums (kernel timing)
   double conv;
   double m, mp;    // AN2 mixing factor and bias
   double s1, s2;   // AN2 coefficients for the next update
@@ -143,6 +144,9 @@ struct Context {
 
   cufftHandle plan64 = 0, plan32 = 0;
   bool plans_ok = false;
+  // one captured iteration per precision, reused by every solve
+  cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
+  unsigned *d_count = nullptr;  // pass-R block counter (last block finalizes)
 
   // restart guess
   std::vector<double> t_init;

@@ -13,9 +13,10 @@
 //   FFT inverse
 //   pass R  (k_pass_r)   post-twiddle, closure, residual R = h + 1 - g,
 //                        FP64 block sums of R^2 and the five AN2 Gram terms
-//   finalize (k_finalize) fixed-order reduction of the block sums, rms,
-//                        convergence / divergence / maxstep decision, 2x2
-//                        AN2 solve -- all on the device, no host sync.
+//   finalize             (last block of pass R) fixed-order reduction of the
+//                        block sums, rms, convergence / divergence / maxstep
+//                        decision, 2x2 AN2 solve -- on the device, no host
+//                        sync, no extra launch.
 //
 // The state variable is the short-range indirect correlation
 // t_SR = t - q_v cf fr.  The closure exponent -u - q cf e + t equals
@@ -60,6 +61,7 @@ struct IterArgs {
   const StageParams *sp;
   double *part;
   int nblocks;
+  unsigned *count;          // blocks of pass R done (reset by the last one)
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -412,14 +414,21 @@ __global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a) {
 }
 
 // ---------------------------------------------------------------- pass R
+__device__ void finalize_block(DevState *st, const double *part, int nblocks,
+                               double nv_points);
+
 template <typename T, int V, int CLOS>
 __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a) {
   typedef typename Cx<T>::t C;
   constexpr int P = (V + 1) / 2;
   constexpr int PTS = sizeof(T) == 4 ? 2 : 1;
   __shared__ double red[kThreads / 32][6];
-  const DevState *st = a.st;
-  if (st->done) return;
+  __shared__ bool last;
+  DevState *st = a.st;
+  if (st->done) {                                // loop stopped: count idle cycles
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->after_done += 1;
+    return;
+  }
   const bool gram = st->count <= 0;
   const long long n = a.n;
   const StageParams *sp = a.sp;
@@ -495,34 +504,43 @@ __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a) {
     for (int w = 0; w < kThreads / 32; ++w) s += red[w][threadIdx.x];
     a.part[(size_t)threadIdx.x * a.nblocks + blockIdx.x] = s;
   }
+  // the last block to finish reduces all block sums and steers the loop
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(a.count, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_block(st, a.part, a.nblocks, (double)n * V);
+  if (threadIdx.x == 0) *a.count = 0u;
 }
 
 // ------------------------------------------------------------- finalize
-// Fixed-order reduction of the pass-R block sums, then the host logic of
-// iterate.cu:52-62 and AN2::calculate (anderson.cu:35-63) on one thread.
-__global__ void k_finalize(DevState *st, const double *part, int nblocks,
-                           double nv_points) {
-  __shared__ double red[6][256];
-  if (st->done) {
-    if (threadIdx.x == 0) st->after_done += 1;
-    return;
-  }
-  for (int k = 0; k < 6; ++k) {
-    double s = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += part[(size_t)k * nblocks + b];
-    red[k][threadIdx.x] = s;
-  }
+// Run by the last block of pass R to finish: fixed-order reduction of the
+// block sums, then the host logic of iterate.cu:52-62 and AN2::calculate
+// (anderson.cu:35-63) on one thread -- no separate launch, no host sync.
+__device__ void finalize_block(DevState *st, const double *part, int nblocks,
+                               double nv_points) {
+  __shared__ double red[6][kThreads];
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s[k] += __ldcg(part + (size_t)k * nblocks + b);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) red[k][threadIdx.x] = s[k];
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if ((int)threadIdx.x < w)
+#pragma unroll
       for (int k = 0; k < 6; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
     __syncthreads();
   }
   if (threadIdx.x != 0) return;
   for (int k = 0; k < 6; ++k) st->sums[k] = red[k][0];
-  st->iter += 1;
   const double rms = sqrt(red[0][0] / nv_points);
   st->rms = rms;
+  if (st->measure) return;
+  st->iter += 1;
   if (!isfinite(rms)) { st->done = 2; st->mode = 0; return; }  // iterate.cu:54-57
   if (rms <= st->conv) { st->done = 1; st->mode = 0; return; } // :58-59
   if (st->count > 0) {                                         // anderson.cu:43-49
@@ -618,7 +636,6 @@ void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
     cufftExecC2C(plan, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
   }
   k_pass_r<T, V, CLOS><<<a.nblocks, kThreads, 0, c.stream>>>(a);
-  k_finalize<<<1, 256, 0, c.stream>>>(a.st, a.part, a.nblocks, (double)a.n * V);
   (void)sizeof(C);
 }
 
@@ -632,42 +649,35 @@ IterArgs<T> make_args(Context &c, bool fp64) {
   a.fkh = c.d_fkh; a.chi = c.chi.d_coef; a.ntab = c.chi.ntab; a.dk = c.chi.dk;
   a.bx = c.prm.box[0]; a.by = c.prm.box[1]; a.bz = c.prm.box[2];
   a.st = c.d_state; a.sp = c.d_stage; a.part = c.d_part; a.nblocks = c.nred_blocks;
+  a.count = c.d_count;
   (void)fp64;
   return a;
 }
 
-struct Loop {
-  cudaGraphExec_t exec = nullptr;
-  bool graph = false;
-};
-
-// One captured iteration per precision; falls back to direct launches if
-// capture of the cuFFT calls is refused.
+// Capture one iteration (passes, cuFFT, and the fused finalize) as a CUDA
+// graph, once per context and precision; every later solve relaunches it.
+// If capture of the cuFFT calls is refused, the loop launches directly.
 template <typename T, int V, int CLOS>
-int capture(Context &c, const IterArgs<T> &a, cufftHandle plan, Loop &L) {
+cudaGraphExec_t capture(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
   if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
-    L.graph = false;
-    return RISM3D_OK;
+    return nullptr;
   }
   launch_iteration<T, V, CLOS>(c, a, plan);
   cudaError_t e = cudaStreamEndCapture(c.stream, &g);
   if (e != cudaSuccess || !g) {
     cudaGetLastError();
-    L.graph = false;
-    return RISM3D_OK;
+    return nullptr;
   }
-  e = cudaGraphInstantiate(&L.exec, g, 0);
+  e = cudaGraphInstantiate(&x, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    L.exec = nullptr;
-    L.graph = false;
-    return RISM3D_OK;
+    return nullptr;
   }
-  L.graph = true;
-  return RISM3D_OK;
+  return x;
 }
 
 template <typename T, int V, int CLOS>
@@ -689,8 +699,8 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
   if (!cuda_ok(c, cudaMemcpyAsync(c.d_state, &hs, sizeof(DevState), cudaMemcpyHostToDevice, c.stream), "state write"))
     return RISM3D_CUDA_ERROR;
   if (!cufft_ok(c, cufftSetStream(plan, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
-  Loop L;
-  capture<T, V, CLOS>(c, a, plan, L);
+  cudaGraphExec_t &gx = (sizeof(T) == 8) ? c.graph64 : c.graph32;
+  if (!gx) gx = capture<T, V, CLOS>(c, a, plan);
   const int kRing = 4, kLag = 2;
   cudaEvent_t ev[kRing];
   for (int i = 0; i < kRing; ++i) cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
@@ -698,9 +708,9 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
   int since_best = 0, launched = 0, status = RISM3D_OK;
   bool stop = false;
   while (!stop) {
-    if (L.graph) cudaGraphLaunch(L.exec, c.stream);
+    if (gx) cudaGraphLaunch(gx, c.stream);
     else launch_iteration<T, V, CLOS>(c, a, plan);
-    c.launches += 4;
+    c.launches += 3;
     cudaMemcpyAsync(&c.h_state[launched % kRing], c.d_state, sizeof(DevState),
                     cudaMemcpyDeviceToHost, c.stream);
     cudaEventRecord(ev[launched % kRing], c.stream);
@@ -721,14 +731,13 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
   }
   // drain: one more iteration guarantees the snapshot pass ran
   if (status == RISM3D_OK) {
-    if (L.graph) cudaGraphLaunch(L.exec, c.stream);
+    if (gx) cudaGraphLaunch(gx, c.stream);
     else launch_iteration<T, V, CLOS>(c, a, plan);
-    c.launches += 4;
+    c.launches += 3;
     cudaMemcpyAsync(&c.h_state[0], c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream);
     if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "iteration drain")) status = RISM3D_CUDA_ERROR;
   }
   for (int i = 0; i < kRing; ++i) cudaEventDestroy(ev[i]);
-  if (L.exec) cudaGraphExecDestroy(L.exec);
   iters_out = c.h_state[0].iter;
   return status;
 }
@@ -867,9 +876,11 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
   }
   a.tw = (const typename Cx<T>::t *)(fp64 ? (void *)c.d_tw : (void *)c.d_twf);
   DevState saved, run;
+  if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "time_kernel")) return RISM3D_CUDA_ERROR;
   cudaMemcpy(&saved, c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost);
   run = saved;
   run.done = 0; run.after_done = 0; run.mode = 2; run.count = 0; run.upd_slot = 0;
+  run.measure = 1;
   run.s1 = 0.25; run.s2 = 0.25;
   cudaMemcpy(c.d_state, &run, sizeof(DevState), cudaMemcpyHostToDevice);
   cudaEvent_t e0, e1;
@@ -988,6 +999,9 @@ int upload_chi(Context &c) {
         }
       }
     }
+  // the captured iteration graphs embed the table pointers
+  if (c.graph64) { cudaGraphExecDestroy(c.graph64); c.graph64 = nullptr; }
+  if (c.graph32) { cudaGraphExecDestroy(c.graph32); c.graph32 = nullptr; }
   // Cubic cells: evaluate the spline once per distinct |k|^2 (the sorted
   // unique-|k| table of initialize_g.cu:31-43, indexed directly).
   if (c.d_xs) { cudaFree(c.d_xs); c.d_xs = nullptr; c.nxs = 0; }

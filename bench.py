@@ -1,0 +1,375 @@
+"""Benchmark: seconds per 256^3 KH 3D-RISM solve on one B200 (and N replicas).
+
+Workload: the protein-scale synthetic solute (846 atoms, compact random
+chain, Rg ~15 A, sigma 3.0-3.8 A, charges N(0, 0.3) shifted to net zero;
+seed 2) on a 256^3 grid in a 128 A cubic cell, KH closure, AN2 (2 0.6 0.2),
+convergence 1e-6, in the reference's TIP3P-like water (h2o_vv.xvk).  One
+step = one complete solve: potential grids, the iteration to convergence,
+and the .xmu observables (mu_ex SC/SC_HNC/GF, PMV, pressure, SE).
+
+  value  device time per solve, mixed precision (FP32 bulk + FP64 polish),
+         solute already on the device, CUDA events on the solve stream
+  e2e    the same through the C ABI from host arrays: rism3d_set_solute
+         (host -> device) + rism3d_solve (result struct -> host), wall clock
+  fp64   the plain FP64 solve (same algorithm as the reference) for the
+         mixed-vs-FP64 speed-up and the |d mu_ex| check (<= 0.01 kcal/mol)
+
+--impl reference runs the reference executable (built from its own sources
+for sm_100a into oracle/_ref) on the same control file, whole-process wall
+time as in the reference README; without that binary it falls back to the
+CPU FP64 oracle.  Multi-GPU: one independent solve per rank (replicas, no
+collective on the solve path); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "3d-rism-cuda_b200"))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+WORKLOADS = {"protein846": "cfg2_protein846_kh", "globule300": "cfg1_globule300"}
+WORKLOAD = WORKLOADS["protein846"]
+METRIC = ("s per 256^3 KH solve, mixed vs FP64 at <=0.01 kcal/mol d(mu_ex); "
+          "batch solves/s")
+KCAL = 4184.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-iters", type=int, default=2,
+                   help="iterations in the CPU-oracle sample")
+    p.add_argument("--workload", default="protein846", choices=sorted(WORKLOADS),
+                   help="protein846: 256^3 (the metric's workload); globule300: the "
+                        "128^3 case, used for profiler captures that must stay small")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+             "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 8
+                          for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# -------------------------------------------------------------- workload
+def workload():
+    from oracle import formats as F
+    ctrl, sol = F.read_control(os.path.join(GOLDEN, WORKLOAD + ".inp"))
+    sv = F.read_xvk(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    return ctrl, sol, sv
+
+
+def iter_bytes_per_point(V, s):
+    """Algorithmic HBM bytes per grid point of each pass (V sites, element
+    size s; complex site pairs; fk is FP64 complex on half the points)."""
+    return {"pass_a": 9 * V * s, "pass_k": 2 * V * s + 8, "pass_r": 5 * V * s}
+
+
+def survey_bytes_per_iter(n, V, s):
+    """N (31 V s + 5 s + 4): minimal fused pipeline of the per-site design."""
+    return n * (31 * V * s + 5 * s + 4)
+
+
+def read_traffic(kernel):
+    """Per-point DRAM traffic of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if len(f) >= 2 and f[0] == kernel:
+            try:
+                return float(f[1])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------- our arm
+def run_ours(args, rank, world, dist):
+    import numpy as np
+    import torch
+    import rism3d_b200 as R
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()          # all solver work and the events
+    ctrl, sol, sv = workload()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+
+    def make(prec):
+        s = R.Solver(ctrl.grid, ctrl.box, closure=ctrl.closure, convergence=ctrl.conv,
+                     maxstep=ctrl.maxstep, an2=(ctrl.count, ctrl.m, ctrl.mp),
+                     precision=prec, device=dev, stream=stream.cuda_stream)
+        s.set_solvent_obj(sv)
+        s.set_solute(sol.sig, sol.eps, sol.q, sol.xyz)
+        return s
+
+    def barrier():
+        if dist:
+            import torch.distributed as D
+            D.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        import torch.distributed as D
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        D.all_reduce(t, op=D.ReduceOp.MAX)
+        return float(t.item())
+
+    mixed = make(R.MIXED)
+    fp64 = make(R.FP64)
+    # warm-up (plans, graphs, caches)
+    for _ in range(args.warmup):
+        mixed.refresh_potentials(); rm = mixed.solve()
+    fp64.refresh_potentials(); r64 = fp64.solve()
+
+    # ---- timed: device-resident solves, mixed precision
+    clk = Clocks(dev)
+    barrier(); torch.cuda.synchronize()
+    l0 = mixed.kernel_launches()
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res = []
+    for _ in range(args.steps):
+        mixed.refresh_potentials()
+        res.append(mixed.solve())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier()
+    launches = mixed.kernel_launches() - l0
+    ms_mixed = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    rm = res[-1]
+
+    # ---- FP64 plain solve (the reference algorithm), same protocol
+    barrier(); torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        fp64.refresh_potentials(); r64 = fp64.solve()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_fp64 = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+
+    # ---- e2e through the C ABI from host buffers
+    import ctypes
+    h2d = 8 * 6 * len(sol.q)               # sig, eps, q, x, y, z per atom
+    d2h = ctypes.sizeof(R.Result)          # the result struct
+    barrier(); torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        mixed.set_solute(sol.sig, sol.eps, sol.q, sol.xyz)
+        re2e = mixed.solve()
+    torch.cuda.synchronize()
+    s_e2e = max_over_ranks(time.perf_counter() - t0) / args.steps
+
+    # ---- live roofline of the dominant streaming kernels (CUDA events on
+    # the solve stream; run after the results were read)
+    n = ctrl.grid[0] * ctrl.grid[1] * ctrl.grid[2]
+    V = sv.natv
+    bpp32 = iter_bytes_per_point(V, 4)
+    bpp64 = iter_bytes_per_point(V, 8)
+    kern = {}
+    for name, kid, bpp in (("pass_a_fp32", 10, bpp32["pass_a"]), ("pass_k_fp32", 11, bpp32["pass_k"]),
+                           ("pass_r_fp32", 12, bpp32["pass_r"])):
+        ms = mixed.time_kernel(kid, 20)
+        kern[name] = {"ms": ms, "gbs": bpp * n / ms / 1e6}
+    for name, kid, bpp in (("pass_a_fp64", 0, bpp64["pass_a"]), ("pass_k_fp64", 1, bpp64["pass_k"]),
+                           ("pass_r_fp64", 2, bpp64["pass_r"])):
+        ms = fp64.time_kernel(kid, 20)
+        kern[name] = {"ms": ms, "gbs": bpp * n / ms / 1e6}
+    mixed.close(); fp64.close()
+    dom = "pass_a_fp32"
+    achieved = kern[dom]["gbs"]
+    traffic_pp = read_traffic("k_pass_a_fp32")
+    dmu = abs(rm["sfe_sc"] - r64["sfe_sc"])
+    out = {
+        "metric": METRIC, "value": ms_mixed / 1e3 / world, "unit": "s/solve",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": ("protein-like solute, 846 atoms, 256^3 grid, 128 A cell, KH, "
+                                "AN2 2/0.6/0.2, conv 1e-6, TIP3P-like water (h2o_vv.xvk)")
+                   if WORKLOAD == WORKLOADS["protein846"] else
+                   ("globular solute, 300 atoms, 128^3 grid, 64 A cell, KH, AN2 2/0.6/0.2, "
+                    "conv 1e-6, TIP3P-like water (h2o_vv.xvk)"),
+                   "grid": list(ctrl.grid), "box": list(ctrl.box), "natom": len(sol.q),
+                   "natv": V, "precision": "FP32 bulk + FP64 polish",
+                   "l2": "state ~5 GB per solve >> 126 MB L2 (no flush needed)",
+                   "parallelism": "replicas" if world > 1 else "1 GPU"},
+        "fp64": {"s_per_solve": ms_fp64 / 1e3 / world, "iterations": r64["iterations"],
+                 "sfe_sc": r64["sfe_sc"]},
+        "mixed": {"iterations": rm["iterations"], "iterations_fp32": rm["iterations_fp32"],
+                  "sfe_sc": rm["sfe_sc"], "ms_setup": rm["ms_setup"],
+                  "ms_iterate": rm["ms_iterate"], "ms_observe": rm["ms_observe"]},
+        "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
+        "dmu_mixed_vs_fp64_j_per_mol": dmu, "dmu_within_0.01kcal": dmu <= 0.01 * KCAL,
+        "e2e": {"value": s_e2e / world, "unit": "s/solve", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "k_pass_a<float> (FP32 pass A: AN2 update + "
+                     "closure + forward pack)", "achieved": achieved, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "traffic": None if traffic_pp is None else traffic_pp * n,
+                     "algorithmic_bytes_per_launch": bpp32["pass_a"] * n,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
+        "kernels": kern,
+        "bytes_per_iteration": {"fp64": sum(bpp64.values()) * n, "fp32": sum(bpp32.values()) * n,
+                                "survey_formula_fp64": survey_bytes_per_iter(n, V, 8)},
+        "clocks": clocks,
+    }
+    return out
+
+
+# ------------------------------------------------------------ CPU oracle
+def cpu_baseline(args):
+    """The CPU FP64 OpenMP oracle on a bounded sample of the same solve:
+    full potential setup, `cpu_iters` iterations and the observables, then
+    seconds per solve = setup + iterations_of_the_FP64_solve * per-iteration
+    + observables."""
+    from oracle import oracle as O
+    ctrl, sol, sv = workload()
+    case = O.Case(ctrl.grid, ctrl.box, sv, sol.sig, sol.eps, sol.q, sol.xyz,
+                  ctrl.closure, ctrl.conv, args.cpu_iters, ctrl.count, ctrl.m, ctrl.mp)
+    r = O.solve(case)
+    ref_iters = json.load(open(os.path.join(GOLDEN, "ref_b200", "summary.json")))[WORKLOAD]["iterations"]
+    per_it = r["t_iter"] / max(1, r["iterations"])
+    value = r["t_setup"] + per_it * ref_iters + r["t_obs"]
+    return {"value": value, "unit": "s/solve", "cores": O.lib().oracle_num_threads(),
+            "kind": "port",
+            "sample": "oracle: potentials + %d iterations + observables, extrapolated to the "
+                      "%d iterations of the FP64 solve (%.2f s/iteration)"
+                      % (r["iterations"], ref_iters, per_it)}
+
+
+# -------------------------------------------------------- reference arm
+def run_reference(args):
+    binp = os.path.join(ROOT, "oracle", "_ref", "3drism-cuda")
+    if not os.path.exists(binp):
+        cb = cpu_baseline(args)
+        return {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "s/solve",
+                "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": False,
+                "note": "reference executable not built; CPU FP64 oracle port instead",
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "s/solve", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+    work = tempfile.mkdtemp(prefix="rism_ref_")
+    shutil.copyfile(os.path.join(GOLDEN, WORKLOAD + ".inp"), os.path.join(work, WORKLOAD + ".inp"))
+    shutil.copyfile(os.path.join(GOLDEN, "h2o_vv.xvk"), os.path.join(work, "h2o_vv.xvk"))
+    times, iters, out = [], None, ""
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        p = subprocess.run([binp, WORKLOAD + ".inp"], cwd=work, capture_output=True, text=True,
+                           timeout=600)
+        dt = time.perf_counter() - t0
+        if p.returncode != 0:
+            raise RuntimeError("reference run failed: " + p.stderr[-500:])
+        iters = len(re.findall(r"Step = \d+", p.stdout))
+        out = open(os.path.join(work, WORKLOAD + ".xmu")).read()
+        if i >= args.warmup:
+            times.append(dt)
+    sfe = float(re.search(r"SFE_SC=\s*(\S+)", out).group(1))
+    v = sum(times) / len(times)
+    shutil.rmtree(work, ignore_errors=True)
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "s/solve", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "same control file, reference 3drism-cuda (FP64, AN2) built "
+                                   "from its own sources for sm_100a, whole-process wall time",
+                       "iterations": iters, "sfe_sc": sfe},
+            "cpu_baseline": {"value": v, "unit": "s/solve", "cores": 1, "kind": "reference",
+                             "sample": "whole reference executable per step (1 host thread "
+                                       "driving the same B200)"},
+            "e2e": {"value": v, "unit": "s/solve", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    global WORKLOAD
+    args = parse()
+    WORKLOAD = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = world > 1
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return 0
+    if dist:
+        import datetime
+        import torch
+        import torch.distributed as D
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out = run_ours(args, rank, world, dist)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(args)
+        print(json.dumps(out))
+    if dist:
+        import torch.distributed as D
+        D.barrier()
+        D.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -47,6 +47,7 @@ class OracleResult(C.Structure):
         ("se", C.c_double), ("se_lj", C.c_double), ("se_es", C.c_double),
         ("correction", C.c_double), ("rms", C.c_double),
         ("iterations", C.c_int), ("status", C.c_int),
+        ("t_setup", C.c_double), ("t_iter", C.c_double), ("t_obs", C.c_double),
     ]
 
 

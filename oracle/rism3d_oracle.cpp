@@ -466,6 +466,7 @@ extern "C" int oracle_solve(const OracleInput *in, OracleResult *out,
   const size_t n = P.n;
   if (nv < 1 || nv > ORACLE_MAXV) return -2;
   memset(out, 0, sizeof(*out));
+  double w0 = omp_get_wtime();
 
   // --- setup: potentials, chi, FFT (initialize.cu:4-13) ---
   std::vector<double> u((size_t)nv * n), e(n), fr(n);
@@ -476,6 +477,8 @@ extern "C" int oracle_solve(const OracleInput *in, OracleResult *out,
   int nga;
   if (chi_table(P, indga, xu, nga)) return -3;
   Shifted3D fft(P.nx, P.ny, P.nz, in->bx, in->by, in->bz);
+  double w1 = omp_get_wtime();
+  out->t_setup = w1 - w0;
 
   // --- iterate (iterate.cu:6-90) ---
   std::vector<cd> guv((size_t)nv * n), huv((size_t)nv * n);
@@ -634,6 +637,8 @@ extern "C" int oracle_solve(const OracleInput *in, OracleResult *out,
   out->iterations = total;
   out->rms = rms;
   out->status = status;
+  double w2 = omp_get_wtime();
+  out->t_iter = w2 - w1;
 
   // --- observables (output.cu:6-62) ---
   const double ibeta = kAvogadro * kBoltzmann * in->temper;
@@ -739,5 +744,6 @@ extern "C" int oracle_solve(const OracleInput *in, OracleResult *out,
   if (h_out)
     for (size_t i = 0; i < (size_t)nv * n; ++i) h_out[i] = huv[i].real();
   if (t_out) std::copy(t.begin(), t.end(), t_out);
+  out->t_obs = omp_get_wtime() - w2;
   return 0;
 }

@@ -61,6 +61,7 @@ typedef struct {
   double rms;
   int iterations;                 /* total over charge-up stages */
   int status;                     /* 0 converged, 1 diverged, 2 maxstep */
+  double t_setup, t_iter, t_obs;  /* wall seconds: potentials+chi, loop, output */
 } OracleResult;
 
 /* Full solve + observables.  Optional outputs (may be NULL):
