@@ -87,15 +87,19 @@ constexpr int kAtomsPerBlock = 128;
 constexpr int kPtsTile = 128;
 
 // part layout: [chunk][atom][2V + 6]: SE_LJ[v], SE_ES[v] (rho_v applied),
-// grad LJ xyz, grad ES xyz (sum over v of rho_v * ...).
-template <int V>
+// grad LJ xyz, grad ES xyz (sum over v of rho_v * ...).  One FP64 rsqrt per
+// (point, atom) gives 1/r, r and 1/r^2; the cutoff r < sigma_uv/2 of the
+// reference is tested on r, with the correctly rounded sqrt only for points
+// within 1e-12 of the cutoff radius.
+template <int V, int GRAD>
 __global__ void __launch_bounds__(kAtomsPerBlock)
 k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
                  const double *__restrict__ g, const double *__restrict__ atoms,
                  int natom, SiteAll sv, double cc, long long chunk,
-                 double *part, int want_grad) {
+                 double *part) {
   constexpr int NA = 2 * V + 6;
-  __shared__ double px[kPtsTile], py[kPtsTile], pz[kPtsTile], pg[V][kPtsTile];
+  __shared__ double4 pp[kPtsTile];          // x y z
+  __shared__ double pg[V][kPtsTile];
   const long long n = (long long)nx * ny * nz;
   const int ia = blockIdx.x * kAtomsPerBlock + threadIdx.x;
   const bool live = ia < natom;
@@ -104,13 +108,15 @@ k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
     const double *a = atoms + 8 * (size_t)ia;
     X = a[0]; Y = a[1]; Z = a[2]; qu = a[3]; su = a[4]; eu = a[5];
   }
-  double sg[V], ep[V], qq[V], hs[V];
+  double s6v[V], e4[V], qq[V], hs[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) {
-    sg[v] = (su + sv.sig[v]) * 0.5;          // cal_LJ.cu:28
-    ep[v] = sqrt(eu * sv.eps[v]);            // cal_LJ.cu:29
+    const double sg = (su + sv.sig[v]) * 0.5;  // cal_LJ.cu:28
+    const double sg2 = sg * sg;
+    s6v[v] = sg2 * sg2 * sg2;
+    e4[v] = 4.0 * sqrt(eu * sv.eps[v]);        // cal_LJ.cu:29
     qq[v] = qu * sv.q[v] * cc;
-    hs[v] = sg[v] * 0.5;
+    hs[v] = sg * 0.5;
   }
   double acc[NA];
 #pragma unroll
@@ -120,17 +126,16 @@ k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
   for (long long base = j0; base < j1; base += kPtsTile) {
     __syncthreads();
     for (int i = threadIdx.x; i < kPtsTile; i += blockDim.x) {
-      long long j = base + i;
+      const long long j = base + i;
       if (j < j1) {
-        long long r = j / nx;
-        int ix = (int)(j - r * nx), iy = (int)(r % ny), iz = (int)(r / ny);
-        px[i] = (ix - nx / 2) * drx;       // cal_euv.cu:45-47
-        py[i] = (iy - ny / 2) * dry;
-        pz[i] = (iz - nz / 2) * drz;
+        const long long r = j / nx;
+        const int ix = (int)(j - r * nx), iy = (int)(r % ny), iz = (int)(r / ny);
+        pp[i] = make_double4((ix - nx / 2) * drx, (iy - ny / 2) * dry,   // cal_euv.cu:45-47
+                             (iz - nz / 2) * drz, 0.0);
 #pragma unroll
         for (int v = 0; v < V; ++v) pg[v][i] = g[(size_t)v * n + j];
       } else {
-        px[i] = py[i] = pz[i] = 1.0e30;
+        pp[i] = make_double4(1.0e30, 1.0e30, 1.0e30, 0.0);
 #pragma unroll
         for (int v = 0; v < V; ++v) pg[v][i] = 0.0;
       }
@@ -139,20 +144,25 @@ k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
     if (!live) continue;
     const int m = (int)min((long long)kPtsTile, j1 - base);
     for (int i = 0; i < m; ++i) {
-      const double dx = px[i] - X, dy = py[i] - Y, dz = pz[i] - Z;
+      const double4 p = pp[i];
+      const double dx = p.x - X, dy = p.y - Y, dz = p.z - Z;
       const double r2 = dx * dx + dy * dy + dz * dz;
-      const double r1 = sqrt(r2);
+      const double ri = rsqrt(r2);
+      const double r1 = r2 * ri;
+      const double ir2 = ri * ri;
+      const double ir6 = ir2 * ir2 * ir2;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        if (r1 < hs[v]) continue;            // cutoff r < sigma/2
+        bool inside = !(r1 >= hs[v]);           // r = 0 gives NaN: inside
+        if (fabs(r1 - hs[v]) < 1.0e-12 * hs[v]) inside = sqrt(r2) < hs[v];
+        if (inside) continue;                 // cutoff r < sigma/2
         const double gv = pg[v][i];
-        const double rs2i = sg[v] * sg[v] / r2;
-        const double rs6i = rs2i * rs2i * rs2i;
-        acc[v] += ep[v] * 4.0 * rs6i * (rs6i - 1.0) * gv;
-        acc[V + v] += qq[v] / r1 * gv;
-        if (want_grad) {
-          const double ulj = ep[v] * 24.0 * rs6i / r2 * (2.0 * rs6i - 1.0) * gv * sv.rho[v];
-          const double uco = qq[v] / (r2 * r1) * gv * sv.rho[v];
+        const double rs6i = s6v[v] * ir6;
+        acc[v] += e4[v] * rs6i * (rs6i - 1.0) * gv;
+        acc[V + v] += qq[v] * ri * gv;
+        if (GRAD) {
+          const double ulj = 6.0 * e4[v] * rs6i * ir2 * (2.0 * rs6i - 1.0) * gv * sv.rho[v];
+          const double uco = qq[v] * ri * ir2 * gv * sv.rho[v];
           acc[2 * V + 0] += ulj * dx; acc[2 * V + 1] += ulj * dy; acc[2 * V + 2] += ulj * dz;
           acc[2 * V + 3] += uco * dx; acc[2 * V + 4] += uco * dy; acc[2 * V + 5] += uco * dz;
         }
@@ -248,9 +258,14 @@ int atoms_v(Context &c, bool forces) {
   }
   const double cc = kHartree * kBohr * kAvogadro;            // cal_euv.cu:39
   dim3 grid(tiles, nchunk);
-  k_atom_integrals<V><<<grid, kAtomsPerBlock, 0, c.stream>>>(
-      c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, A, sv, cc,
-      chunk, c.d_atom_part, forces ? 1 : 0);
+  if (forces)
+    k_atom_integrals<V, 1><<<grid, kAtomsPerBlock, 0, c.stream>>>(
+        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, A, sv, cc,
+        chunk, c.d_atom_part);
+  else
+    k_atom_integrals<V, 0><<<grid, kAtomsPerBlock, 0, c.stream>>>(
+        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, A, sv, cc,
+        chunk, c.d_atom_part);
   double *sum = c.d_atom_part + (size_t)nchunk * A * NA;
   k_sum_chunks<<<(A * NA + 255) / 256, 256, 0, c.stream>>>(c.d_atom_part, nchunk, A, NA, sum);
   c.launches += 2;

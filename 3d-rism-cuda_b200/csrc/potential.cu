@@ -28,123 +28,153 @@ struct SiteLJ {
   double eps[kMaxSites];
 };
 
+// Real-space grids.  Each thread owns two neighbouring points along x (one
+// row, the atom tile read once for both); per (point, atom) one FP64 rsqrt
+// gives 1/r, r and 1/r^2.  Beyond 40 A the factor e^-r (< 4.3e-18) is
+// dropped: there the reference's q (1 - e^-r) / r already rounds to q / r.
+constexpr int kPts = 2;
+
 template <int V>
 __global__ void __launch_bounds__(kThreads)
 k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
               const double *__restrict__ atoms, int natom, SiteLJ sites,
               double ikbt, double ubeta, double *__restrict__ u,
               double *__restrict__ esr, double *__restrict__ fr) {
-  __shared__ double sx[kTile], sy[kTile], sz[kTile], sq[kTile];
-  __shared__ double ss2[V][kTile], se4[V][kTile];
+  __shared__ double4 sa[kTile];           // x y z q
+  __shared__ double2 sl[V][kTile];        // sigma_uv^2, 4 eps_uv / kBT
   const long long n = (long long)nx * ny * nz;
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double rx = 0, ry = 0, rz = 0;
-  if (j < n) {
-    int ix = (int)(j % nx);
-    long long r = j / nx;
-    int iy = (int)(r % ny), iz = (int)(r / ny);
-    rx = (ix - nx / 2) * drx;   // cal_LJ.cu:54-56 (integer n/2)
+  const long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * kPts;
+  double rx[kPts], ry = 0, rz = 0;
+  {
+    const long long jj = j < n ? j : 0;
+    const int ix = (int)(jj % nx);
+    const long long r = jj / nx;
+    const int iy = (int)(r % ny), iz = (int)(r / ny);
+    for (int k = 0; k < kPts; ++k) rx[k] = (ix + k - nx / 2) * drx;   // cal_LJ.cu:54-56
     ry = (iy - ny / 2) * dry;
     rz = (iz - nz / 2) * drz;
   }
-  double acc[V];
+  double acc[kPts][V], afr[kPts], aes[kPts];
 #pragma unroll
-  for (int v = 0; v < V; ++v) acc[v] = 0.0;
-  double afr = 0.0, aes = 0.0;
+  for (int k = 0; k < kPts; ++k) {
+    afr[k] = aes[k] = 0.0;
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[k][v] = 0.0;
+  }
   const double cut2 = 1.0e-4;   // (1e-2)^2, cal_LJ.cu:11-12
   for (int t0 = 0; t0 < natom; t0 += kTile) {
     __syncthreads();
     for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
-      int ia = t0 + i;
+      const int ia = t0 + i;
       if (ia < natom) {
         const double *a = atoms + 8 * (size_t)ia;
-        sx[i] = a[0]; sy[i] = a[1]; sz[i] = a[2]; sq[i] = a[3];
+        sa[i] = make_double4(a[0], a[1], a[2], a[3]);
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-          double s = (a[4] + sites.sig[v]) * 0.5;      // cal_LJ.cu:28
-          ss2[v][i] = s * s;
-          se4[v][i] = 4.0 * sqrt(a[5] * sites.eps[v]) * ikbt;  // :29, :38
+          const double sg = (a[4] + sites.sig[v]) * 0.5;                 // cal_LJ.cu:28
+          sl[v][i] = make_double2(sg * sg, 4.0 * sqrt(a[5] * sites.eps[v]) * ikbt);  // :29, :38
         }
-      } else {
-        sx[i] = sy[i] = sz[i] = 1.0e30; sq[i] = 0.0;
-#pragma unroll
-        for (int v = 0; v < V; ++v) { ss2[v][i] = 0.0; se4[v][i] = 0.0; }
       }
     }
     __syncthreads();
     const int m = min(kTile, natom - t0);
     for (int i = 0; i < m; ++i) {
-      double dx = rx - sx[i], dy = ry - sy[i], dz = rz - sz[i];
-      double r2 = dx * dx + dy * dy + dz * dz;
-      double r2c = r2 < cut2 ? cut2 : r2;
-      double ir2 = 1.0 / r2c;
+      const double4 at = sa[i];
+      const double dy = ry - at.y, dz = rz - at.z;
+      const double dyz = dy * dy + dz * dz;
 #pragma unroll
-      for (int v = 0; v < V; ++v) {
-        double s2 = ss2[v][i] * ir2;
-        double s6 = s2 * s2 * s2;
-        acc[v] += se4[v][i] * s6 * (s6 - 1.0);
-      }
-      double ra = sqrt(r2);
-      if (ra >= 1.0e-5) {                 // cal_Coulomb.cu:114-120
-        double qr = sq[i] / ra;
-        double em1 = expm1(-ra);          // e^-r - 1
-        afr -= qr * em1;                  // q (1 - e^-r) / r
-        aes += qr * (em1 + 1.0);          // q e^-r / r
-      } else {
-        afr += sq[i];
-        aes -= sq[i];
+      for (int k = 0; k < kPts; ++k) {
+        const double dx = rx[k] - at.x;
+        const double r2 = dx * dx + dyz;
+        const double ri = rsqrt(r2);
+        const double ir2 = r2 < cut2 ? 1.0 / cut2 : ri * ri;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const double2 p = sl[v][i];
+          const double s2 = p.x * ir2;
+          const double s6 = s2 * s2 * s2;
+          acc[k][v] += p.y * s6 * (s6 - 1.0);
+        }
+        const double ra = r2 > 0.0 ? r2 * ri : 0.0;
+        if (ra >= 1.0e-5) {                 // cal_Coulomb.cu:114-120
+          const double qr = at.w * ri;
+          if (ra < 40.0) {
+            const double em1 = expm1(-ra);  // e^-r - 1
+            afr[k] -= qr * em1;             // q (1 - e^-r) / r
+            aes[k] += qr * (em1 + 1.0);     // q e^-r / r
+          } else {
+            afr[k] += qr;
+          }
+        } else {
+          afr[k] += at.w;
+          aes[k] -= at.w;
+        }
       }
     }
   }
-  if (j < n) {
 #pragma unroll
-    for (int v = 0; v < V; ++v) u[(size_t)v * n + j] = acc[v];
-    fr[j] = afr * ubeta;
-    esr[j] = aes * ubeta;
+  for (int k = 0; k < kPts; ++k) {
+    if (j + k >= n) break;
+#pragma unroll
+    for (int v = 0; v < V; ++v) u[(size_t)v * n + j + k] = acc[k][v];
+    fr[j + k] = afr[k] * ubeta;
+    esr[j + k] = aes[k] * ubeta;
   }
 }
 
-// fk on the owner half j < N/2 (cal_Coulomb.cu:125-149; k from set_g,
-// initialize_g.cu:58-60).
+// Per-atom phase rows e^{-i k_d R_d} for the three axes (k from set_g,
+// initialize_g.cu:58-60): ph[u][0..nx+ny+nz).
+__global__ void k_phase_rows(int nx, int ny, int nz, double bx, double by, double bz,
+                             const double *__restrict__ atoms, int natom,
+                             double2 *__restrict__ ph) {
+  const int L = nx + ny + nz;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)natom * L) return;
+  const int u = (int)(idx / L), i = (int)(idx % L);
+  double k, R;
+  if (i < nx) { k = 2.0 * kPi * (i - nx / 2.0 + 0.5) / bx; R = atoms[8 * (size_t)u + 0]; }
+  else if (i < nx + ny) { k = 2.0 * kPi * (i - nx - ny / 2.0 + 0.5) / by; R = atoms[8 * (size_t)u + 1]; }
+  else { k = 2.0 * kPi * (i - nx - ny - nz / 2.0 + 0.5) / bz; R = atoms[8 * (size_t)u + 2]; }
+  double s, c;
+  sincos(k * R, &s, &c);
+  ph[idx] = make_double2(c, -s);
+}
+
+// fk on the owner half j < N/2 (cal_Coulomb.cu:125-149): the phase
+// e^{-ik.R} is the product of the three per-axis rows.
 __global__ void __launch_bounds__(kThreads)
 k_potential_k(int nx, int ny, int nz, double bx, double by, double bz,
               const double *__restrict__ atoms, int natom, double ubeta,
-              double2 *__restrict__ fkh) {
-  __shared__ double sx[kTile], sy[kTile], sz[kTile], sq[kTile];
+              const double2 *__restrict__ ph, double2 *__restrict__ fkh) {
+  __shared__ double sq[kTile];
   const long long nh = (long long)nx * ny * nz / 2;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double kx = 0, ky = 0, kz = 0;
-  if (j < nh) {
-    int ix = (int)(j % nx);
-    long long r = j / nx;
-    int iy = (int)(r % ny), iz = (int)(r / ny);
-    kx = 2.0 * kPi * (ix - nx / 2.0 + 0.5) / bx;
-    ky = 2.0 * kPi * (iy - ny / 2.0 + 0.5) / by;
-    kz = 2.0 * kPi * (iz - nz / 2.0 + 0.5) / bz;
-  }
-  double rk2 = kx * kx + ky * ky + kz * kz;
-  double rk4i = 1.0 / (rk2 * (rk2 + 1.0));
+  const long long jj = j < nh ? j : 0;
+  const int ix = (int)(jj % nx);
+  const long long r = jj / nx;
+  const int iy = (int)(r % ny), iz = (int)(r / ny);
+  const double kx = 2.0 * kPi * (ix - nx / 2.0 + 0.5) / bx;
+  const double ky = 2.0 * kPi * (iy - ny / 2.0 + 0.5) / by;
+  const double kz = 2.0 * kPi * (iz - nz / 2.0 + 0.5) / bz;
+  const double rk2 = kx * kx + ky * ky + kz * kz;
+  const double rk4i = 1.0 / (rk2 * (rk2 + 1.0));
+  const int L = nx + ny + nz;
   double re = 0.0, im = 0.0;
   for (int t0 = 0; t0 < natom; t0 += kTile) {
     __syncthreads();
     for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
-      int ia = t0 + i;
-      if (ia < natom) {
-        const double *a = atoms + 8 * (size_t)ia;
-        sx[i] = a[0]; sy[i] = a[1]; sz[i] = a[2]; sq[i] = a[3];
-      } else {
-        sx[i] = sy[i] = sz[i] = 0.0; sq[i] = 0.0;
-      }
+      const int ia = t0 + i;
+      sq[i] = ia < natom ? 4.0 * kPi * atoms[8 * (size_t)ia + 3] : 0.0;
     }
     __syncthreads();
     const int m = min(kTile, natom - t0);
     for (int i = 0; i < m; ++i) {
-      double ruk = kx * sx[i] + ky * sy[i] + kz * sz[i];
-      double s, c;
-      sincos(ruk, &s, &c);
-      double tmp = 4.0 * kPi * sq[i];
-      re += tmp * c;
-      im -= tmp * s;
+      const double2 *row = ph + (size_t)(t0 + i) * L;
+      const double2 px = row[ix], py = row[nx + iy], pz = row[nx + ny + iz];
+      const double yzr = py.x * pz.x - py.y * pz.y, yzi = py.x * pz.y + py.y * pz.x;
+      const double cr = px.x * yzr - px.y * yzi, ci = px.x * yzi + px.y * yzr;
+      re += sq[i] * cr;      // + 4 pi q cos(k.R)
+      im += sq[i] * ci;      // - 4 pi q sin(k.R)
     }
   }
   if (j < nh) fkh[j] = make_double2(re * rk4i * ubeta, im * rk4i * ubeta);
@@ -152,7 +182,7 @@ k_potential_k(int nx, int ny, int nz, double bx, double by, double bz,
 
 template <int V>
 void launch_r(Context &c, const SiteLJ &sl, double ikbt, double ubeta) {
-  long long blocks = (c.n + kThreads - 1) / kThreads;
+  long long blocks = (c.n / kPts + kThreads - 1) / kThreads;
   k_potential_r<V><<<(unsigned)blocks, kThreads, 0, c.stream>>>(
       c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.natom, sl,
       ikbt, ubeta, c.d_u, c.d_e, c.d_fr);
@@ -197,12 +227,19 @@ int compute_potentials(Context &c) {
     default: c.err = "unsupported number of solvent sites"; return RISM3D_UNSUPPORTED_SHAPE;
   }
   if (!cuda_ok(c, cudaGetLastError(), "k_potential_r")) return RISM3D_CUDA_ERROR;
+  const long long L = c.nx + c.ny + c.nz;
+  double2 *ph = nullptr;
+  if (!cuda_ok(c, cudaMallocAsync(&ph, sizeof(double2) * L * c.natom, c.stream), "phase rows"))
+    return RISM3D_CUDA_ERROR;
+  k_phase_rows<<<(unsigned)((L * c.natom + 255) / 256), 256, 0, c.stream>>>(
+      c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], c.d_atoms, c.natom, ph);
   long long blocks = (c.n / 2 + kThreads - 1) / kThreads;
   k_potential_k<<<(unsigned)blocks, kThreads, 0, c.stream>>>(
       c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], c.d_atoms,
-      c.natom, ubeta, c.d_fkh);
+      c.natom, ubeta, ph, c.d_fkh);
+  cudaFreeAsync(ph, c.stream);
   if (!cuda_ok(c, cudaGetLastError(), "k_potential_k")) return RISM3D_CUDA_ERROR;
-  c.launches += 2;
+  c.launches += 3;
   return RISM3D_OK;
 }
 
