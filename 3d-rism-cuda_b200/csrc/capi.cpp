@@ -23,6 +23,8 @@ static std::string g_create_err;
 
 namespace rism3d {
 
+void set_create_error(const std::string &msg) { g_create_err = msg; }
+
 bool cuda_ok(Context &c, cudaError_t e, const char *what) {
   if (e == cudaSuccess) return true;
   c.err = std::string(what) + ": " + cudaGetErrorString(e);

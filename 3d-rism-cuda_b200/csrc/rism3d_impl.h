@@ -184,6 +184,8 @@ int time_kernel(Context &c, int which, int reps, double *ms);   // solver.cu
 void free_device(Context &c);
 
 bool cuda_ok(Context &c, cudaError_t e, const char *what);
+// message returned by rism3d_last_error(NULL) (context-free entry points)
+void set_create_error(const std::string &msg);
 bool cufft_ok(Context &c, cufftResult r, const char *what);
 
 }  // namespace rism3d

@@ -19,7 +19,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["potential.cu", "solver.cu", "observe.cu", "adjoint.cu", "batch.cu",
-           "capi.cpp", "io.cpp"]
+           "noalloc.cu", "capi.cpp", "io.cpp"]
 
 
 def _ccbin():

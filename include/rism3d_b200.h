@@ -176,6 +176,30 @@ int rism3d_solve_batch(rism3d_ctx *ctx, int nmol, const int *natoms,
 
 void rism3d_destroy(rism3d_ctx *ctx);
 
+/* Allocation-free mu_ex / PMV integrals.  No counterpart in the reference
+ * (it has no library API).  For callers that cannot call cudaMalloc where
+ * they need these integrals: a host application whose own pool allocator
+ * has already reserved the free device memory (cudaMalloc would fail or
+ * fragment that pool), or a latency-critical loop that cannot afford
+ * cudaMalloc's implicit device synchronisation.  Inputs are the caller's
+ * device grids h[natv][n] (Re h of the OZ step) and t[natv][n] (absolute
+ * t), rho[natv] on the host; out (host) receives 3*natv+1 doubles:
+ * SFEC_SC[v], SFEC_SC_HNC[v], SFEC_GF[v] in J/mol (output_xmu.cu) and
+ * sum_v rho_v dv int c_v (cal_pmv.cu; PMV = xt (1 - that) N_A kB T).
+ * Work runs on `stream` (NULL: legacy default) and the call returns after
+ * it.  The reduction scratch is one static device array of 148 KiB
+ * (592 blocks x 32 sums), held by every GPU that loads the library until
+ * exit; limit: natv <= 8, n < 2^31 (larger sizes return
+ * RISM3D_UNSUPPORTED_SHAPE).  The first call on a device looks up the
+ * array's device address with that device current -- make that first call
+ * before any stream capture.  All calls share the array and every value a
+ * call reads is written by that same call (nothing needs clearing), so
+ * calls that overlap on the GPU race.  Errors: rism3d_last_error(NULL). */
+int rism3d_exchem_noalloc(int closure, int natv, long long n, double dv,
+                          double temperature, const double *rho,
+                          const double *d_h, const double *d_t, void *stream,
+                          double *out);
+
 /* Last error message of ctx (or of the last failed create when ctx is
  * NULL). */
 const char *rism3d_last_error(const rism3d_ctx *ctx);
