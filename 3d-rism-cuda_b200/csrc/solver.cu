@@ -705,7 +705,7 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
   cudaEvent_t ev[kRing];
   for (int i = 0; i < kRing; ++i) cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
   double best = 1e300;
-  int since_best = 0, launched = 0, status = RISM3D_OK;
+  int since_best = 0, launched = 0, status = RISM3D_OK, printed = 0;
   bool stop = false;
   while (!stop) {
     if (gx) cudaGraphLaunch(gx, c.stream);
@@ -719,8 +719,10 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
       int k = (launched - 1 - kLag) % kRing;
       if (!cuda_ok(c, cudaEventSynchronize(ev[k]), "iteration")) { status = RISM3D_CUDA_ERROR; break; }
       const DevState &s = c.h_state[k];
-      if (c.prm.verbose && s.done == 0)
+      if (c.prm.verbose && s.iter > printed) {       // iterate.cu:63
         printf(" Step = %d Reside = %g\n", s.iter, s.rms);
+        printed = s.iter;
+      }
       if (s.done) stop = true;
       if (watch_stagnation && !stop) {
         if (s.rms < 0.9 * best) { best = s.rms; since_best = 0; }

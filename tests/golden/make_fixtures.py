@@ -27,11 +27,30 @@ def tighten(src, dst, conv="1.0e-9"):
     open(dst, "w").write("\n".join(tok_lines))
 
 
+def subsample_xvk(src, dst, step=4):
+    """Keep every `step`-th chi row (rows step-1, 2 step-1, ...): with the same
+    dr and ntab/step rows, k_i = (i+1) pi / (dr ntab) lands on the kept rows."""
+    lines = open(src).read().split("\n")
+    h = lines[1].split()
+    num, natv, ntab, dr = int(h[1]), int(h[2]), int(h[3]), float(h[4])
+    head = lines[:num + 5]
+    nnew = ntab // step
+    head[1] = "##  %8d%8d%8d  %14.8f  %14.8f" % (num, natv, nnew, dr, 3.141592653589793 / (dr * nnew))
+    data = " ".join(lines[num + 5:]).split()
+    per = natv * natv
+    rows = []
+    for i in range(nnew):
+        k = step * i + step - 1
+        rows.append(" ".join(data[k * per:(k + 1) * per]))
+    open(dst, "w").write("\n".join(head + rows) + "\n")
+
+
 def main():
     if not os.path.isdir(SRC):
         sys.exit("reference examples not mounted")
     for f in FILES:
         shutil.copyfile(os.path.join(SRC, f), os.path.join(DST, f))
+    subsample_xvk(os.path.join(SRC, "naclaq_vv.xvk"), os.path.join(DST, "naclaq_sub4_vv.xvk"))
     for name in ("test1", "test2"):
         tighten(os.path.join(DST, name + ".inp"), os.path.join(DST, name + "_tight.inp"))
 
