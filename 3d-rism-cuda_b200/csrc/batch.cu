@@ -1,8 +1,119 @@
-// Batched small solutes (rism3d_solve_batch).
+// Batched solves of many small solutes (rism3d_solve_batch).  The reference
+// solves one solute per process; here solutes with the same cubic cell are
+// solved together: every pass of the iteration is one launch over all of
+// them (solute = blockIdx.y), one batched cuFFT plan transforms all their
+// site pairs, each solute converges on its own device state word (a
+// finished solute's blocks idle), and the loop is the same captured graph.
+#include <map>
+#include <vector>
+
 #include "rism3d_impl.h"
 
-extern "C" int rism3d_solve_batch(rism3d_ctx *, int, const int *, const int *, const double *,
-                                  const double *, const double *, const double *, const double *,
-                                  rism3d_result *) {
-  return RISM3D_BAD_STATE;
+using namespace rism3d;
+
+struct rism3d_ctx {
+  Context c;
+};
+
+extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, const int *grids,
+                                  const double *boxes, const double *sig, const double *eps,
+                                  const double *q, const double *xyz, rism3d_result *results) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &p = x->c;
+  cudaSetDevice(p.dev);
+  if (!p.have_solvent) { p.err = "set the solvent first"; return RISM3D_BAD_STATE; }
+  if (nmol < 1 || !natoms || !grids || !boxes || !sig || !eps || !q || !xyz || !results) {
+    p.err = "bad batch arguments";
+    return RISM3D_BAD_INPUT;
+  }
+  std::vector<long long> off(nmol + 1, 0);
+  for (int m = 0; m < nmol; ++m) {
+    if (natoms[m] < 1 || grids[m] < 4 || !(boxes[m] > 0)) {
+      p.err = "bad batch entry " + std::to_string(m);
+      return RISM3D_BAD_INPUT;
+    }
+    off[m + 1] = off[m] + natoms[m];
+  }
+  // group by cell
+  std::map<std::pair<int, double>, std::vector<int>> groups;
+  for (int m = 0; m < nmol; ++m) groups[{grids[m], boxes[m]}].push_back(m);
+  int worst = RISM3D_OK;
+  for (auto &kv : groups) {
+    const int grid = kv.first.first;
+    const double box = kv.first.second;
+    const std::vector<int> &mols = kv.second;
+    const int nb = (int)mols.size();
+    Context *ch = nullptr;
+    for (Context::Child &cc : p.children)
+      if (cc.grid == grid && cc.box == box && cc.nb == nb) ch = cc.ctx;
+    if (!ch) {
+      rism3d_params cp = p.prm;
+      cp.grid[0] = cp.grid[1] = cp.grid[2] = grid;
+      cp.box[0] = cp.box[1] = cp.box[2] = box;
+      cp.stream = p.stream;          // children run on the parent's stream
+      cp.verbose = 0;
+      ch = new Context;
+      std::string err;
+      int rc = context_init(*ch, &cp, nb, err);
+      if (rc == RISM3D_OK)
+        rc = context_set_solvent(*ch, p.natv, p.rho, p.qv, p.sigv, p.epsv, p.temper, p.xt,
+                                 p.ntab, p.xdr, p.xvv_host.data());
+      if (rc != RISM3D_OK) {
+        p.err = err.empty() ? ch->err : err;
+        context_release(*ch);
+        delete ch;
+        return rc;
+      }
+      ch->own_stream = false;
+      p.children.push_back({grid, nb, box, ch});
+    }
+    // concatenate the group's atoms
+    std::vector<int> cnt(nb);
+    std::vector<double> s, e, qq, r;
+    for (int b = 0; b < nb; ++b) {
+      const int m = mols[b];
+      cnt[b] = natoms[m];
+      s.insert(s.end(), sig + off[m], sig + off[m + 1]);
+      e.insert(e.end(), eps + off[m], eps + off[m + 1]);
+      qq.insert(qq.end(), q + off[m], q + off[m + 1]);
+      r.insert(r.end(), xyz + 3 * off[m], xyz + 3 * off[m + 1]);
+    }
+    int rc = context_set_atoms(*ch, cnt, s.data(), e.data(), qq.data(), r.data());
+    if (rc == RISM3D_OK) {
+      ch->res = rism3d_result{};
+      ch->bres.assign(nb, rism3d_result{});
+      cudaEventRecord(ch->tm_iter.a, ch->stream);
+      rc = run_solve(*ch, 0);
+      cudaEventRecord(ch->tm_iter.b, ch->stream);
+    }
+    if (rc == RISM3D_OK) {
+      cudaEventRecord(ch->tm_obs.a, ch->stream);
+      rc = compute_observables(*ch);
+      if (rc == RISM3D_OK) rc = compute_atom_integrals(*ch, false);
+      cudaEventRecord(ch->tm_obs.b, ch->stream);
+    }
+    if (rc != RISM3D_OK) {
+      p.err = ch->err;
+      return rc;
+    }
+    cudaStreamSynchronize(ch->stream);
+    float ms_s = 0, ms_i = 0, ms_o = 0;
+    cudaEventElapsedTime(&ms_s, ch->tm_setup.a, ch->tm_setup.b);
+    cudaEventElapsedTime(&ms_i, ch->tm_iter.a, ch->tm_iter.b);
+    cudaEventElapsedTime(&ms_o, ch->tm_obs.a, ch->tm_obs.b);
+    for (int b = 0; b < nb; ++b) {
+      rism3d_result rr = nb == 1 ? ch->res : ch->bres[b];
+      if (nb == 1) { rr.iterations = ch->res.iterations; rr.status = ch->res.status; }
+      rr.natv = p.natv;
+      rr.natom = cnt[b];
+      rr.ms_setup = ms_s;                        // group totals
+      rr.ms_iterate = ms_i;
+      rr.ms_observe = ms_o;
+      results[mols[b]] = rr;
+      if (rr.status != RISM3D_OK && worst == RISM3D_OK) worst = rr.status;
+    }
+    p.launches += ch->launches;
+    ch->launches = 0;
+  }
+  return worst;
 }

@@ -25,6 +25,25 @@ namespace rism3d {
 
 void set_create_error(const std::string &msg) { g_create_err = msg; }
 
+// Free everything a context owns, its batch children included.
+void context_release(Context &c) {
+  cudaSetDevice(c.dev);
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  for (Context::Child &ch : c.children) {
+    context_release(*ch.ctx);
+    delete ch.ctx;
+  }
+  c.children.clear();
+  free_device(c);
+  for (Timer *t : {&c.tm_setup, &c.tm_iter, &c.tm_obs}) {
+    if (t->a) cudaEventDestroy(t->a);
+    if (t->b) cudaEventDestroy(t->b);
+    t->a = t->b = nullptr;
+  }
+  if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);
+  c.stream = nullptr;
+}
+
 bool cuda_ok(Context &c, cudaError_t e, const char *what) {
   if (e == cudaSuccess) return true;
   c.err = std::string(what) + ": " + cudaGetErrorString(e);
@@ -41,7 +60,8 @@ void free_device(Context &c) {
   void *ptrs[] = {c.d_u, c.d_e, c.d_fr, c.d_fkh, c.d_atoms, c.d_tw, c.d_twf,
                   c.d_U, c.d_t, c.d_Y, c.d_RP, c.d_buf, c.d_h, c.d_g,
                   c.f_U, c.f_t, c.f_Y, c.f_RP, c.f_buf, c.d_part, c.d_state,
-                  c.d_stage, c.d_obs, c.d_atom_part, c.chi.d_coef, c.d_xs};
+                  c.d_stage, c.d_obs, c.d_atom_part, c.chi.d_coef, c.d_xs,
+                  c.d_atom_off, c.d_atom_cnt};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   c.d_u = c.d_e = c.d_fr = nullptr; c.d_fkh = nullptr; c.d_atoms = nullptr;
@@ -51,6 +71,7 @@ void free_device(Context &c) {
   c.d_part = nullptr; c.d_state = nullptr; c.d_stage = nullptr; c.d_obs = nullptr;
   c.d_atom_part = nullptr; c.chi.d_coef = nullptr; c.natom_part_cap = 0;
   c.d_xs = nullptr; c.nxs = 0;
+  c.d_atom_off = c.d_atom_cnt = nullptr;
   if (c.h_state) cudaFreeHost(c.h_state);
   c.h_state = nullptr;
   if (c.graph64) cudaGraphExecDestroy(c.graph64);
@@ -115,7 +136,8 @@ int fetch_grid(Context &c, int which, double *host) {
 }  // namespace rism3d
 
 static int alloc_state(Context &c) {
-  const size_t n = (size_t)c.n, V = (size_t)c.natv, P = (V + 1) / 2;
+  // every per-solute grid is [nb][...]
+  const size_t n = (size_t)c.n * c.nb, V = (size_t)c.natv, P = (V + 1) / 2;
   const bool mixed = c.prm.precision == RISM3D_MIXED;
   auto A = [&](void **p, size_t bytes, const char *w) {
     return cuda_ok(c, cudaMalloc(p, bytes), w);
@@ -128,7 +150,7 @@ static int alloc_state(Context &c) {
             A((void **)&c.d_buf, sizeof(double2) * P * n, "alloc buf") &&
             A((void **)&c.d_h, sizeof(double) * V * n, "alloc h") &&
             A((void **)&c.d_g, sizeof(double) * V * n, "alloc g") &&
-            A((void **)&c.d_obs, sizeof(double) * 64, "alloc obs");
+            A((void **)&c.d_obs, sizeof(double) * 64 * c.nb, "alloc obs");
   if (ok && mixed)
     ok = A((void **)&c.f_U, sizeof(float) * V * n, "alloc U32") &&
          A((void **)&c.f_t, sizeof(float) * V * n, "alloc t32") &&
@@ -137,12 +159,14 @@ static int alloc_state(Context &c) {
          A((void **)&c.f_buf, sizeof(float2) * P * n, "alloc buf32");
   if (!ok) return RISM3D_CUDA_ERROR;
   // batched 3D plans over the site pairs; x is the fastest axis
+  // one batched plan over all site pairs of all solutes
   int dims[3] = {c.nz, c.ny, c.nx};
-  if (!cufft_ok(c, cufftPlanMany(&c.plan64, 3, dims, nullptr, 1, (int)n, nullptr, 1, (int)n,
-                                 CUFFT_Z2Z, (int)P), "cufftPlanMany Z2Z"))
+  const int np = (int)c.n, nbat = (int)(P * c.nb);
+  if (!cufft_ok(c, cufftPlanMany(&c.plan64, 3, dims, nullptr, 1, np, nullptr, 1, np,
+                                 CUFFT_Z2Z, nbat), "cufftPlanMany Z2Z"))
     return RISM3D_CUFFT_ERROR;
-  if (mixed && !cufft_ok(c, cufftPlanMany(&c.plan32, 3, dims, nullptr, 1, (int)n, nullptr, 1,
-                                          (int)n, CUFFT_C2C, (int)P), "cufftPlanMany C2C"))
+  if (mixed && !cufft_ok(c, cufftPlanMany(&c.plan32, 3, dims, nullptr, 1, np, nullptr, 1,
+                                          np, CUFFT_C2C, nbat), "cufftPlanMany C2C"))
     return RISM3D_CUFFT_ERROR;
   c.plans_ok = true;
   return RISM3D_OK;
@@ -150,51 +174,51 @@ static int alloc_state(Context &c) {
 
 extern "C" {
 
-int rism3d_create(const rism3d_params *p, rism3d_ctx **out) {
-  if (!p || !out) { g_create_err = "null argument"; return RISM3D_BAD_INPUT; }
-  *out = nullptr;
+}  // extern "C"
+
+namespace rism3d {
+
+// Validate params and set up a context for nb solutes sharing one cell
+// (nb = 1 for rism3d_create; rism3d_solve_batch uses nb > 1).
+int context_init(Context &c, const rism3d_params *p, int nb, std::string &err) {
   for (int d = 0; d < 3; ++d) {
     if (p->grid[d] < 4 || p->grid[d] % 4 != 0 || p->grid[d] > 2048) {
-      g_create_err = "grid sizes must be multiples of 4 in [4, 2048] (half-shifted transform, fft3d.cu)";
+      err = "grid sizes must be multiples of 4 in [4, 2048] (half-shifted transform, fft3d.cu)";
       return RISM3D_UNSUPPORTED_SHAPE;
     }
-    if (!(p->box[d] > 0)) { g_create_err = "box must be positive"; return RISM3D_BAD_INPUT; }
+    if (!(p->box[d] > 0)) { err = "box must be positive"; return RISM3D_BAD_INPUT; }
   }
   if ((long long)p->grid[0] * p->grid[1] * p->grid[2] >= (1LL << 31)) {
-    g_create_err = "grid has 2^31 points or more";
+    err = "grid has 2^31 points or more";
     return RISM3D_UNSUPPORTED_SHAPE;
   }
   if (p->closure != RISM3D_KH && p->closure != RISM3D_HNC) {
-    g_create_err = "Unexpected closure switch";
+    err = "Unexpected closure switch";
     return RISM3D_BAD_INPUT;
   }
-  if (p->maxstep < 1 || !(p->convergence > 0) || p->an2_count < 0) {
-    g_create_err = "bad iteration control";
+  if (p->maxstep < 1 || !(p->convergence > 0) || p->an2_count < 0 || nb < 1) {
+    err = "bad iteration control";
     return RISM3D_BAD_INPUT;
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
-    g_create_err = "no CUDA device";
+    err = "no CUDA device";
     return RISM3D_NO_DEVICE;
   }
-  if (p->device < 0 || p->device >= ndev) { g_create_err = "bad device ordinal"; return RISM3D_NO_DEVICE; }
-  rism3d_ctx *x = new (std::nothrow) rism3d_ctx;
-  if (!x) return RISM3D_BAD_INPUT;
-  Context &c = x->c;
+  if (p->device < 0 || p->device >= ndev) { err = "bad device ordinal"; return RISM3D_NO_DEVICE; }
   c.prm = *p;
   c.dev = p->device;
+  c.nb = nb;
   if (cudaSetDevice(c.dev) != cudaSuccess) {
-    g_create_err = "cannot initialise the CUDA device";
-    delete x;
+    err = "cannot initialise the CUDA device";
     return RISM3D_CUDA_ERROR;
   }
   if (p->stream) {
     c.stream = (cudaStream_t)p->stream;
     c.own_stream = false;
   } else if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
-    g_create_err = "cannot create a CUDA stream";
-    delete x;
+    err = "cannot create a CUDA stream";
     return RISM3D_CUDA_ERROR;
   }
   c.nx = p->grid[0]; c.ny = p->grid[1]; c.nz = p->grid[2];
@@ -202,39 +226,67 @@ int rism3d_create(const rism3d_params *p, rism3d_ctx **out) {
   c.vol = p->box[0] * p->box[1] * p->box[2];             // cell.cc:9-14
   c.dv = c.vol / (double)c.n;
   for (int d = 0; d < 3; ++d) c.dr[d] = p->box[d] / p->grid[d];
-  bool ok = cuda_ok(c, cudaMalloc(&c.d_e, sizeof(double) * c.n), "alloc esr") &&
-            cuda_ok(c, cudaMalloc(&c.d_fr, sizeof(double) * c.n), "alloc fr") &&
-            cuda_ok(c, cudaMalloc(&c.d_fkh, sizeof(double2) * (c.n / 2)), "alloc fk") &&
+  const long long nn = c.n * nb;
+  bool ok = cuda_ok(c, cudaMalloc(&c.d_e, sizeof(double) * nn), "alloc esr") &&
+            cuda_ok(c, cudaMalloc(&c.d_fr, sizeof(double) * nn), "alloc fr") &&
+            cuda_ok(c, cudaMalloc(&c.d_fkh, sizeof(double2) * (nn / 2)), "alloc fk") &&
             cuda_ok(c, cudaMalloc(&c.d_tw, sizeof(double2) * (c.nx + c.ny + c.nz)), "alloc tw") &&
             cuda_ok(c, cudaMalloc(&c.d_twf, sizeof(float2) * (c.nx + c.ny + c.nz)), "alloc tw") &&
-            cuda_ok(c, cudaMalloc(&c.d_state, sizeof(DevState)), "alloc state") &&
+            cuda_ok(c, cudaMalloc(&c.d_state, sizeof(DevState) * nb), "alloc state") &&
             cuda_ok(c, cudaMalloc(&c.d_stage, sizeof(StageParams)), "alloc stage") &&
-            cuda_ok(c, cudaHostAlloc(&c.h_state, sizeof(DevState) * 4, cudaHostAllocDefault), "alloc pinned");
-  long long nb = (c.n + 255) / 256;
-  c.nred_blocks = (int)(nb < 148 * 8 ? nb : 148 * 8);
-  ok = ok && cuda_ok(c, cudaMalloc(&c.d_part, sizeof(double) * 64 * c.nred_blocks), "alloc partials") &&
-       cuda_ok(c, cudaMalloc(&c.d_count, sizeof(unsigned)), "alloc counter") &&
-       cuda_ok(c, cudaMemset(c.d_count, 0, sizeof(unsigned)), "zero counter");
+            cuda_ok(c, cudaHostAlloc(&c.h_state, sizeof(DevState) * 4 * nb, cudaHostAllocDefault), "alloc pinned");
+  long long nbk = (c.n + 255) / 256;
+  c.nred_blocks = (int)(nbk < 148 * 8 ? nbk : 148 * 8);
+  ok = ok && cuda_ok(c, cudaMalloc(&c.d_part, sizeof(double) * 64 * c.nred_blocks * nb), "alloc partials") &&
+       cuda_ok(c, cudaMalloc(&c.d_count, sizeof(unsigned) * nb), "alloc counter") &&
+       cuda_ok(c, cudaMemset(c.d_count, 0, sizeof(unsigned) * nb), "zero counter");
   for (Timer *t : {&c.tm_setup, &c.tm_iter, &c.tm_obs}) {
     cudaEventCreate(&t->a);
     cudaEventCreate(&t->b);
   }
   if (!ok || build_twiddles(c) != RISM3D_OK) {
-    g_create_err = c.err;
+    err = c.err;
     free_device(c);
     if (c.own_stream) cudaStreamDestroy(c.stream);
-    delete x;
+    c.stream = nullptr;
     return RISM3D_CUDA_ERROR;
+  }
+  return RISM3D_OK;
+}
+
+int context_set_solvent(Context &c, int natv, const double *rho, const double *q,
+                        const double *sig, const double *eps, double temperature, double xt,
+                        int ntab, double dr, const double *xvv);
+int context_set_atoms(Context &c, const std::vector<int> &cnt, const double *sig,
+                      const double *eps, const double *q, const double *xyz);
+
+}  // namespace rism3d
+
+extern "C" {
+
+int rism3d_create(const rism3d_params *p, rism3d_ctx **out) {
+  if (!p || !out) { g_create_err = "null argument"; return RISM3D_BAD_INPUT; }
+  *out = nullptr;
+  rism3d_ctx *x = new (std::nothrow) rism3d_ctx;
+  if (!x) return RISM3D_BAD_INPUT;
+  std::string err;
+  int rc = context_init(x->c, p, 1, err);
+  if (rc != RISM3D_OK) {
+    g_create_err = err;
+    delete x;
+    return rc;
   }
   *out = x;
   return RISM3D_OK;
 }
 
-int rism3d_set_solvent(rism3d_ctx *x, int natv, const double *rho, const double *q,
-                       const double *sig, const double *eps, double temperature, double xt,
-                       int ntab, double dr, const double *xvv) {
-  if (!x) return RISM3D_BAD_INPUT;
-  Context &c = x->c;
+}  // extern "C"
+
+namespace rism3d {
+
+int context_set_solvent(Context &c, int natv, const double *rho, const double *q,
+                        const double *sig, const double *eps, double temperature, double xt,
+                        int ntab, double dr, const double *xvv) {
   cudaSetDevice(c.dev);
   if (natv < 1 || natv > kMaxSites) { c.err = "natv must be 1..8"; return RISM3D_UNSUPPORTED_SHAPE; }
   if (!rho || !q || !sig || !eps || !xvv || ntab < 4 || !(dr > 0) || !(temperature > 0) || !(xt > 0)) {
@@ -263,13 +315,24 @@ int rism3d_set_solvent(rism3d_ctx *x, int natv, const double *rho, const double 
   return RISM3D_OK;
 }
 
-int rism3d_set_solute(rism3d_ctx *x, int natom, const double *sig, const double *eps,
-                      const double *q, const double *xyz) {
-  if (!x) return RISM3D_BAD_INPUT;
-  Context &c = x->c;
+// Atoms of the nb solutes, concatenated (cnt[b] atoms each), then the
+// potential grids of every solute.
+int context_set_atoms(Context &c, const std::vector<int> &cnt, const double *sig,
+                      const double *eps, const double *q, const double *xyz) {
   cudaSetDevice(c.dev);
   if (!c.have_solvent) { c.err = "set the solvent first"; return RISM3D_BAD_STATE; }
-  if (natom < 1 || !sig || !eps || !q || !xyz) { c.err = "bad solute arguments"; return RISM3D_BAD_INPUT; }
+  if ((int)cnt.size() != c.nb || !sig || !eps || !q || !xyz) {
+    c.err = "bad solute arguments";
+    return RISM3D_BAD_INPUT;
+  }
+  int natom = 0;
+  c.atom_off.assign(c.nb, 0);
+  c.atom_cnt = cnt;
+  for (int b = 0; b < c.nb; ++b) {
+    if (cnt[b] < 1) { c.err = "every solute needs at least one atom"; return RISM3D_BAD_INPUT; }
+    c.atom_off[b] = natom;
+    natom += cnt[b];
+  }
   c.natom = natom;
   c.sig.assign(sig, sig + natom);
   c.eps.assign(eps, eps + natom);
@@ -287,8 +350,16 @@ int rism3d_set_solute(rism3d_ctx *x, int natom, const double *sig, const double 
   }
   if (c.d_atoms) cudaFree(c.d_atoms);
   c.d_atoms = nullptr;
+  if (!c.d_atom_off &&
+      (!cuda_ok(c, cudaMalloc(&c.d_atom_off, sizeof(int) * c.nb), "alloc atom offsets") ||
+       !cuda_ok(c, cudaMalloc(&c.d_atom_cnt, sizeof(int) * c.nb), "alloc atom counts")))
+    return RISM3D_CUDA_ERROR;
   if (!cuda_ok(c, cudaMalloc(&c.d_atoms, sizeof(double) * pack.size()), "alloc atoms") ||
       !cuda_ok(c, cudaMemcpyAsync(c.d_atoms, pack.data(), sizeof(double) * pack.size(),
+                                  cudaMemcpyHostToDevice, c.stream), "copy atoms") ||
+      !cuda_ok(c, cudaMemcpyAsync(c.d_atom_off, c.atom_off.data(), sizeof(int) * c.nb,
+                                  cudaMemcpyHostToDevice, c.stream), "copy atoms") ||
+      !cuda_ok(c, cudaMemcpyAsync(c.d_atom_cnt, c.atom_cnt.data(), sizeof(int) * c.nb,
                                   cudaMemcpyHostToDevice, c.stream), "copy atoms"))
     return RISM3D_CUDA_ERROR;
   cudaEventRecord(c.tm_setup.a, c.stream);
@@ -300,6 +371,24 @@ int rism3d_set_solute(rism3d_ctx *x, int natom, const double *sig, const double 
   c.solved = false;
   c.have_forces = false;
   return RISM3D_OK;
+}
+
+}  // namespace rism3d
+
+extern "C" {
+
+int rism3d_set_solvent(rism3d_ctx *x, int natv, const double *rho, const double *q,
+                       const double *sig, const double *eps, double temperature, double xt,
+                       int ntab, double dr, const double *xvv) {
+  if (!x) return RISM3D_BAD_INPUT;
+  return context_set_solvent(x->c, natv, rho, q, sig, eps, temperature, xt, ntab, dr, xvv);
+}
+
+int rism3d_set_solute(rism3d_ctx *x, int natom, const double *sig, const double *eps,
+                      const double *q, const double *xyz) {
+  if (!x) return RISM3D_BAD_INPUT;
+  if (natom < 1) { x->c.err = "bad solute arguments"; return RISM3D_BAD_INPUT; }
+  return context_set_atoms(x->c, std::vector<int>(1, natom), sig, eps, q, xyz);
 }
 
 int rism3d_set_tuv(rism3d_ctx *x, const double *t) {
@@ -379,15 +468,7 @@ int rism3d_get_grid(rism3d_ctx *x, int which, double *host) {
 
 void rism3d_destroy(rism3d_ctx *x) {
   if (!x) return;
-  Context &c = x->c;
-  cudaSetDevice(c.dev);
-  if (c.stream) cudaStreamSynchronize(c.stream);
-  free_device(c);
-  for (Timer *t : {&c.tm_setup, &c.tm_iter, &c.tm_obs}) {
-    if (t->a) cudaEventDestroy(t->a);
-    if (t->b) cudaEventDestroy(t->b);
-  }
-  if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);
+  context_release(x->c);
   delete x;
 }
 

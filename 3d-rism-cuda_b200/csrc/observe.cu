@@ -10,6 +10,7 @@
 // cal_grad gradients (cal_grad.cu:51-145) for ALL atoms in one launch: one
 // atom per thread, grid points streamed through shared memory (the
 // reference launches one full-grid kernel + Thrust reductions per pair).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -26,6 +27,11 @@ k_observe(long long n, const double *__restrict__ h, const double *__restrict__ 
           const double *__restrict__ fr, const StageParams *sp, double *part,
           int nblocks) {
   constexpr int NS = 4 * V;
+  // solute blockIdx.y
+  h += (size_t)blockIdx.y * V * n;
+  t += (size_t)blockIdx.y * V * n;
+  fr += (size_t)blockIdx.y * n;
+  part += (size_t)blockIdx.y * NS * nblocks;
   __shared__ double red[kThreads / 32][NS];
   double acc[NS];
 #pragma unroll
@@ -94,10 +100,16 @@ constexpr int kPtsTile = 128;
 template <int V, int GRAD>
 __global__ void __launch_bounds__(kAtomsPerBlock)
 k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
-                 const double *__restrict__ g, const double *__restrict__ atoms,
-                 int natom, SiteAll sv, double cc, long long chunk,
-                 double *part) {
+                 const double *__restrict__ g, const double *__restrict__ atoms_all,
+                 const int *__restrict__ aoff, const int *__restrict__ acnt, int natom_tot,
+                 SiteAll sv, double cc, long long chunk, double *part) {
   constexpr int NA = 2 * V + 6;
+  // solute blockIdx.z: its atoms against its own g; partials indexed by the
+  // global atom number
+  const int sb = blockIdx.z;
+  const double *__restrict__ atoms = atoms_all + 8 * (size_t)aoff[sb];
+  const int natom = acnt[sb];
+  g += (size_t)sb * V * (size_t)nx * ny * nz;
   __shared__ double4 pp[kPtsTile];          // x y z
   __shared__ double pg[V][kPtsTile];
   const long long n = (long long)nx * ny * nz;
@@ -170,7 +182,7 @@ k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
     }
   }
   if (live) {
-    double *o = part + ((size_t)blockIdx.y * natom + ia) * NA;
+    double *o = part + ((size_t)blockIdx.y * natom_tot + aoff[sb] + ia) * NA;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       o[v] = acc[v] * sv.rho[v];
@@ -193,54 +205,59 @@ __global__ void k_sum_chunks(const double *part, int nchunk, int natom, int na,
 
 template <int V>
 int observe_v(Context &c) {
-  const int nb = c.nred_blocks;
+  const int nb = c.nred_blocks, B = c.nb;
   StageParams sp{};
   for (int v = 0; v < V; ++v) sp.qcf[v] = c.qv[v] * c.cf_final;
   cudaMemcpyAsync(c.d_stage, &sp, sizeof(sp), cudaMemcpyHostToDevice, c.stream);
   if (c.prm.closure == RISM3D_KH)
-    k_observe<V, 0><<<nb, kThreads, 0, c.stream>>>(c.n, c.d_h, c.d_t, c.d_fr, c.d_stage, c.d_part, nb);
+    k_observe<V, 0><<<dim3(nb, B), kThreads, 0, c.stream>>>(c.n, c.d_h, c.d_t, c.d_fr, c.d_stage, c.d_part, nb);
   else
-    k_observe<V, 1><<<nb, kThreads, 0, c.stream>>>(c.n, c.d_h, c.d_t, c.d_fr, c.d_stage, c.d_part, nb);
-  k_reduce_rows<<<4 * V, 256, 0, c.stream>>>(c.d_part, nb, c.d_obs);
+    k_observe<V, 1><<<dim3(nb, B), kThreads, 0, c.stream>>>(c.n, c.d_h, c.d_t, c.d_fr, c.d_stage, c.d_part, nb);
+  k_reduce_rows<<<4 * V * B, 256, 0, c.stream>>>(c.d_part, nb, c.d_obs);
   c.launches += 2;
-  std::vector<double> s(4 * V);
-  if (!cuda_ok(c, cudaMemcpyAsync(s.data(), c.d_obs, sizeof(double) * 4 * V, cudaMemcpyDeviceToHost, c.stream), "observe") ||
+  std::vector<double> s((size_t)4 * V * B);
+  if (!cuda_ok(c, cudaMemcpyAsync(s.data(), c.d_obs, sizeof(double) * s.size(), cudaMemcpyDeviceToHost, c.stream), "observe") ||
       !cuda_ok(c, cudaStreamSynchronize(c.stream), "observe"))
     return RISM3D_CUDA_ERROR;
   const double ibeta = kAvogadro * kBoltzmann * c.temper;   // output_xmu.cu:19
-  rism3d_result &r = c.res;
-  r.natv = V;
-  r.natom = c.natom;
-  r.sfe_sc = r.sfe_sc_hnc = r.sfe_gf = 0.0;
-  double cuv = 0.0;
-  for (int v = 0; v < V; ++v) {
-    r.sfec_sc[v] = ibeta * s[4 * v + 0] * c.rho[v] * c.dv;
-    r.sfec_sc_hnc[v] = ibeta * s[4 * v + 1] * c.rho[v] * c.dv;
-    r.sfec_gf[v] = ibeta * s[4 * v + 2] * c.rho[v] * c.dv;
-    r.sfe_sc += r.sfec_sc[v];
-    r.sfe_sc_hnc += r.sfec_sc_hnc[v];
-    r.sfe_gf += r.sfec_gf[v];
-    cuv += s[4 * v + 3] * c.rho[v];
-  }
-  cuv *= c.dv;
-  const double pmv = c.xt * (1.0 - cuv) * ibeta;             // cal_pmv.cu:18-19
   double pres = 0.0;                                         // cal_pressure.cu
   for (int v = 0; v < V; ++v) pres += c.rho[v];
   pres *= 1.0e30 / kAvogadro;
   pres = 0.5 * (pres + 1.0 / (c.xt * ibeta));
-  r.pmv = pmv * 1000.0;
-  r.pressure = ibeta * pres;
-  r.correction = -pres * pmv * ibeta;                        // output_xmu.cu:21
+  for (int b = 0; b < B; ++b) {
+    rism3d_result &r = (B == 1) ? c.res : c.bres[b];
+    const double *sb = &s[(size_t)b * 4 * V];
+    r.natv = V;
+    r.natom = (B == 1) ? c.natom : c.atom_cnt[b];
+    r.sfe_sc = r.sfe_sc_hnc = r.sfe_gf = 0.0;
+    double cuv = 0.0;
+    for (int v = 0; v < V; ++v) {
+      r.sfec_sc[v] = ibeta * sb[4 * v + 0] * c.rho[v] * c.dv;
+      r.sfec_sc_hnc[v] = ibeta * sb[4 * v + 1] * c.rho[v] * c.dv;
+      r.sfec_gf[v] = ibeta * sb[4 * v + 2] * c.rho[v] * c.dv;
+      r.sfe_sc += r.sfec_sc[v];
+      r.sfe_sc_hnc += r.sfec_sc_hnc[v];
+      r.sfe_gf += r.sfec_gf[v];
+      cuv += sb[4 * v + 3] * c.rho[v];
+    }
+    cuv *= c.dv;
+    const double pmv = c.xt * (1.0 - cuv) * ibeta;           // cal_pmv.cu:18-19
+    r.pmv = pmv * 1000.0;
+    r.pressure = ibeta * pres;
+    r.correction = -pres * pmv * ibeta;                      // output_xmu.cu:21
+  }
   return RISM3D_OK;
 }
 
 template <int V>
 int atoms_v(Context &c, bool forces) {
   constexpr int NA = 2 * V + 6;
-  const int A = c.natom;
-  const int tiles = (A + kAtomsPerBlock - 1) / kAtomsPerBlock;
+  const int A = c.natom;            // all solutes
+  int amax = 0;
+  for (int x : c.atom_cnt) amax = std::max(amax, x);
+  const int tiles = (amax + kAtomsPerBlock - 1) / kAtomsPerBlock;
   // enough chunks to fill the GPU a few times over
-  int nchunk = (148 * 8 + tiles - 1) / tiles;
+  int nchunk = (148 * 8 + tiles * c.nb - 1) / (tiles * c.nb);
   if (nchunk < 1) nchunk = 1;
   long long chunk = (c.n + nchunk - 1) / nchunk;
   chunk = ((chunk + kPtsTile - 1) / kPtsTile) * kPtsTile;
@@ -257,15 +274,15 @@ int atoms_v(Context &c, bool forces) {
     sv.sig[v] = c.sigv[v]; sv.eps[v] = c.epsv[v]; sv.q[v] = c.qv[v]; sv.rho[v] = c.rho[v];
   }
   const double cc = kHartree * kBohr * kAvogadro;            // cal_euv.cu:39
-  dim3 grid(tiles, nchunk);
+  dim3 grid(tiles, nchunk, c.nb);
   if (forces)
     k_atom_integrals<V, 1><<<grid, kAtomsPerBlock, 0, c.stream>>>(
-        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, A, sv, cc,
-        chunk, c.d_atom_part);
+        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, c.d_atom_off,
+        c.d_atom_cnt, A, sv, cc, chunk, c.d_atom_part);
   else
     k_atom_integrals<V, 0><<<grid, kAtomsPerBlock, 0, c.stream>>>(
-        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, A, sv, cc,
-        chunk, c.d_atom_part);
+        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, c.d_atom_off,
+        c.d_atom_cnt, A, sv, cc, chunk, c.d_atom_part);
   double *sum = c.d_atom_part + (size_t)nchunk * A * NA;
   k_sum_chunks<<<(A * NA + 255) / 256, 256, 0, c.stream>>>(c.d_atom_part, nchunk, A, NA, sum);
   c.launches += 2;
@@ -274,6 +291,20 @@ int atoms_v(Context &c, bool forces) {
       !cuda_ok(c, cudaMemcpyAsync(h.data(), sum, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream), "atom integrals") ||
       !cuda_ok(c, cudaStreamSynchronize(c.stream), "atom integrals"))
     return RISM3D_CUDA_ERROR;
+  if (c.nb > 1) {                   // per-solute SE totals (batched solves)
+    for (int b = 0; b < c.nb; ++b) {
+      double slj = 0.0, ses = 0.0;
+      for (int u = c.atom_off[b]; u < c.atom_off[b] + c.atom_cnt[b]; ++u)
+        for (int v = 0; v < V; ++v) {
+          slj += h[(size_t)u * NA + v] * c.dv;
+          ses += h[(size_t)u * NA + V + v] * c.dv;
+        }
+      c.bres[b].se_lj = slj;
+      c.bres[b].se_es = ses;
+      c.bres[b].se = slj + ses;
+    }
+    return RISM3D_OK;
+  }
   c.euv.assign((size_t)2 * V * A, 0.0);
   double slj = 0.0, ses = 0.0;
   for (int u = 0; u < A; ++u)

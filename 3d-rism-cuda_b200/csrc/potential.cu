@@ -37,12 +37,19 @@ constexpr int kPts = 2;
 template <int V>
 __global__ void __launch_bounds__(kThreads)
 k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
-              const double *__restrict__ atoms, int natom, SiteLJ sites,
-              double ikbt, double ubeta, double *__restrict__ u,
-              double *__restrict__ esr, double *__restrict__ fr) {
+              const double *__restrict__ atoms_all, const int *__restrict__ aoff,
+              const int *__restrict__ acnt, SiteLJ sites, double ikbt, double ubeta,
+              double *__restrict__ u, double *__restrict__ esr, double *__restrict__ fr) {
   __shared__ double4 sa[kTile];           // x y z q
   __shared__ double2 sl[V][kTile];        // sigma_uv^2, 4 eps_uv / kBT
   const long long n = (long long)nx * ny * nz;
+  // solute blockIdx.y: its atoms and its [V][N] / [N] grids
+  const int sb = blockIdx.y;
+  const double *__restrict__ atoms = atoms_all + 8 * (size_t)aoff[sb];
+  const int natom = acnt[sb];
+  u += (size_t)sb * V * n;
+  esr += (size_t)sb * n;
+  fr += (size_t)sb * n;
   const long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * kPts;
   double rx[kPts], ry = 0, rz = 0;
   {
@@ -144,10 +151,16 @@ __global__ void k_phase_rows(int nx, int ny, int nz, double bx, double by, doubl
 // e^{-ik.R} is the product of the three per-axis rows.
 __global__ void __launch_bounds__(kThreads)
 k_potential_k(int nx, int ny, int nz, double bx, double by, double bz,
-              const double *__restrict__ atoms, int natom, double ubeta,
-              const double2 *__restrict__ ph, double2 *__restrict__ fkh) {
+              const double *__restrict__ atoms_all, const int *__restrict__ aoff,
+              const int *__restrict__ acnt, double ubeta,
+              const double2 *__restrict__ ph_all, double2 *__restrict__ fkh) {
   __shared__ double sq[kTile];
   const long long nh = (long long)nx * ny * nz / 2;
+  const int sb = blockIdx.y;
+  const double *__restrict__ atoms = atoms_all + 8 * (size_t)aoff[sb];
+  const int natom = acnt[sb];
+  const double2 *__restrict__ ph = ph_all + (size_t)aoff[sb] * (nx + ny + nz);
+  fkh += (size_t)sb * nh;
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long jj = j < nh ? j : 0;
   const int ix = (int)(jj % nx);
@@ -183,8 +196,8 @@ k_potential_k(int nx, int ny, int nz, double bx, double by, double bz,
 template <int V>
 void launch_r(Context &c, const SiteLJ &sl, double ikbt, double ubeta) {
   long long blocks = (c.n / kPts + kThreads - 1) / kThreads;
-  k_potential_r<V><<<(unsigned)blocks, kThreads, 0, c.stream>>>(
-      c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.natom, sl,
+  k_potential_r<V><<<dim3((unsigned)blocks, c.nb), kThreads, 0, c.stream>>>(
+      c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.d_atom_off, c.d_atom_cnt, sl,
       ikbt, ubeta, c.d_u, c.d_e, c.d_fr);
 }
 
@@ -234,9 +247,9 @@ int compute_potentials(Context &c) {
   k_phase_rows<<<(unsigned)((L * c.natom + 255) / 256), 256, 0, c.stream>>>(
       c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], c.d_atoms, c.natom, ph);
   long long blocks = (c.n / 2 + kThreads - 1) / kThreads;
-  k_potential_k<<<(unsigned)blocks, kThreads, 0, c.stream>>>(
+  k_potential_k<<<dim3((unsigned)blocks, c.nb), kThreads, 0, c.stream>>>(
       c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], c.d_atoms,
-      c.natom, ubeta, ph, c.d_fkh);
+      c.d_atom_off, c.d_atom_cnt, ubeta, ph, c.d_fkh);
   cudaFreeAsync(ph, c.stream);
   if (!cuda_ok(c, cudaGetLastError(), "k_potential_k")) return RISM3D_CUDA_ERROR;
   c.launches += 3;

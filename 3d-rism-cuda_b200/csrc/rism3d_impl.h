@@ -88,6 +88,8 @@ struct Context {
   bool own_stream = true;
   long long launches = 0;      // kernels of this library launched so far
 
+  // solutes solved together on this context (same cell; rism3d_solve_batch)
+  int nb = 1;
   // cell (cell.cc:8-22)
   int nx = 0, ny = 0, nz = 0;
   long long n = 0;
@@ -117,7 +119,10 @@ struct Context {
   double *d_e = nullptr;     // [N]   beta sum q e^-r / r (short-range Coulomb)
   double *d_fr = nullptr;    // [N]   beta long-range part
   double2 *d_fkh = nullptr;  // [N/2] beta fk on the owner half of k space
-  double *d_atoms = nullptr; // [A][8] x y z q sig eps pad
+  double *d_atoms = nullptr; // [A][8] x y z q sig eps pad (all solutes)
+  int *d_atom_off = nullptr; // [nb] first atom of each solute
+  int *d_atom_cnt = nullptr; // [nb] atoms of each solute
+  std::vector<int> atom_off, atom_cnt;
   double2 *d_tw = nullptr;   // twiddle rows: [nx] [ny] [nz] exp(-i pi x/n)
   float2 *d_twf = nullptr;
 
@@ -155,6 +160,7 @@ struct Context {
   bool solved = false;
   double cf_final = 1.0;
   rism3d_result res{};
+  std::vector<rism3d_result> bres;   // per solute when nb > 1
   std::vector<double> euv;       // [2][V][A] (x dv)
   std::vector<double> dulj, due; // [A][3] (x dv)
   bool have_forces = false;
@@ -167,6 +173,15 @@ struct Context {
   std::vector<double> sig_in, eps_in, q_in, xyz_in;  // as read (pre-shift)
 
   Timer tm_setup, tm_iter, tm_obs;
+
+  // batched solves: one child context per (grid, box, count) group, kept for
+  // reuse by later batches (buffers, plans and captured graphs)
+  struct Child {
+    int grid = 0, nb = 0;
+    double box = 0;
+    Context *ctx = nullptr;
+  };
+  std::vector<Child> children;
 };
 
 // ---- kernels/launchers (implemented in the .cu files) ----
@@ -182,6 +197,13 @@ int compute_adjoint(Context &c, double *dq, double *dsig, double *deps,
 int fetch_grid(Context &c, int which, double *host);
 int time_kernel(Context &c, int which, int reps, double *ms);   // solver.cu
 void free_device(Context &c);
+int context_init(Context &c, const rism3d_params *p, int nb, std::string &err);
+int context_set_solvent(Context &c, int natv, const double *rho, const double *q,
+                        const double *sig, const double *eps, double temperature, double xt,
+                        int ntab, double dr, const double *xvv);
+int context_set_atoms(Context &c, const std::vector<int> &cnt, const double *sig,
+                      const double *eps, const double *q, const double *xyz);
+void context_release(Context &c);
 
 bool cuda_ok(Context &c, cudaError_t e, const char *what);
 // message returned by rism3d_last_error(NULL) (context-free entry points)

@@ -25,6 +25,7 @@
 // The AN2 history stores Y_i = tp_i + m rp_i and RP_i = rp_i: the reference
 // update u + m(v - u) (anderson_cuda.cu:16-22) is algebraically
 // y + s1 (Y_0 - y) + s2 (Y_1 - y) with y = t + m R.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -63,6 +64,28 @@ struct IterArgs {
   int nblocks;
   unsigned *count;          // blocks of pass R done (reset by the last one)
 };
+
+// Batched solves: blockIdx.y selects the solute; every per-solute array is
+// laid out solute-major ([B][...]) and this view offsets the pointers, so
+// the kernel bodies below are the single-solute code unchanged.
+template <typename T, int V>
+__device__ __forceinline__ IterArgs<T> solute_view(const IterArgs<T> &a) {
+  constexpr int P = (V + 1) / 2;
+  IterArgs<T> s = a;
+  const size_t b = blockIdx.y, n = (size_t)a.n;
+  if (b == 0) return s;
+  s.buf = a.buf + b * P * n;
+  s.t = a.t + b * V * n;
+  s.U = a.U + b * V * n;
+  s.Y = a.Y + b * 2 * V * n;
+  s.RP = a.RP + b * 2 * V * n;
+  if (a.hout) { s.hout = a.hout + b * V * n; s.gout = a.gout + b * V * n; }
+  s.fkh = a.fkh + b * (n / 2);
+  s.st = a.st + b;
+  s.part = a.part + b * 6 * (size_t)a.nblocks;
+  s.count = a.count + b;
+  return s;
+}
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -306,7 +329,8 @@ __device__ void pass_a_final(const IterArgs<T> &a, int mode, int done, int slot,
 }
 
 template <typename T, int V, int CLOS>
-__global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a) {
+__global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a0) {
+  const IterArgs<T> a = solute_view<T, V>(a0);
   const DevState *st = a.st;
   const int done = st->done;
   const int mode = st->mode;
@@ -324,7 +348,8 @@ __global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a) {
 
 // ---------------------------------------------------------------- pass K
 template <typename T, int V>
-__global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a) {
+__global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a0) {
+  const IterArgs<T> a = solute_view<T, V>(a0);
   typedef typename Cx<T>::t C;
   constexpr int P = (V + 1) / 2;
   if (a.st->done) return;
@@ -418,7 +443,8 @@ __device__ void finalize_block(DevState *st, const double *part, int nblocks,
                                double nv_points);
 
 template <typename T, int V, int CLOS>
-__global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a) {
+__global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a0) {
+  const IterArgs<T> a = solute_view<T, V>(a0);
   typedef typename Cx<T>::t C;
   constexpr int P = (V + 1) / 2;
   constexpr int PTS = sizeof(T) == 4 ? 2 : 1;
@@ -566,44 +592,50 @@ __device__ void finalize_block(DevState *st, const double *part, int nblocks,
   if (st->iter >= st->maxstep) st->done = 3;   // iterate.cu:51 loop bound
 }
 
-// U_SR = u_v + q_v cf esr for a charge-up stage (FP64 and FP32 copies).
-__global__ void k_stage_u(long long n, int nv, const double *u,
+// U_SR = u_v + q_v cf esr for a charge-up stage (FP64 and FP32 copies);
+// arrays [B][V][N], esr [B][N].
+__global__ void k_stage_u(long long n, int nv, long long total, const double *u,
                           const double *esr, const StageParams *sp, double *U,
                           float *Uf) {
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
-       j += (long long)gridDim.x * blockDim.x) {
-    const double e = esr[j];
-    for (int v = 0; v < nv; ++v) {
-      double x = u[(size_t)v * n + j] + sp->qcf[v] * e;
-      U[(size_t)v * n + j] = x;
-      if (Uf) Uf[(size_t)v * n + j] = (float)x;
-    }
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < total;
+       f += (long long)gridDim.x * blockDim.x) {
+    const long long b = f / (nv * n), r = f - b * nv * n;
+    const int v = (int)(r / n);
+    const long long j = r - (long long)v * n;
+    const double x = u[f] + sp->qcf[v] * esr[b * n + j];
+    U[f] = x;
+    if (Uf) Uf[f] = (float)x;
   }
 }
 
 // t_SR from an absolute restart t (read_tuv.cu) or zero (initialize_tuv.cu:
 // t = q fr  <=>  t_SR = 0; charge-up start t = 0 with cf = 0 <=> t_SR = 0).
-__global__ void k_init_t(long long n, int nv, const double *tabs,
+__global__ void k_init_t(long long n, int nv, long long total, const double *tabs,
                          const double *fr, const StageParams *sp, double *t) {
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
-       j += (long long)gridDim.x * blockDim.x)
-    for (int v = 0; v < nv; ++v)
-      t[(size_t)v * n + j] = tabs ? tabs[(size_t)v * n + j] - sp->qcf[v] * fr[j] : 0.0;
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < total;
+       f += (long long)gridDim.x * blockDim.x) {
+    if (!tabs) { t[f] = 0.0; continue; }
+    const long long b = f / (nv * n), r = f - b * nv * n;
+    const int v = (int)(r / n);
+    const long long j = r - (long long)v * n;
+    t[f] = tabs[f] - sp->qcf[v] * fr[b * n + j];
+  }
 }
 
 // Charge-up step (add_tuv.cu): the absolute t gains q cuf fr, so t_SR is
 // unchanged while the stored history tp_i (absolute in the reference) must
 // be re-expressed in the new stage's short-range frame: Y_i -= q cuf fr.
+// Y is [B][2][V][N].
 template <typename T>
-__global__ void k_shift_history(long long n, int nv, const double *fr,
+__global__ void k_shift_history(long long n, int nv, long long total, const double *fr,
                                 const StageParams *sp_step, T *Y) {
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
-       j += (long long)gridDim.x * blockDim.x)
-    for (int s = 0; s < 2; ++s)
-      for (int v = 0; v < nv; ++v) {
-        size_t i = ((size_t)s * nv + v) * n + j;
-        Y[i] = (T)((double)Y[i] - sp_step->qcf[v] * fr[j]);
-      }
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < total;
+       f += (long long)gridDim.x * blockDim.x) {
+    const long long b = f / (2 * nv * n), r = f - b * 2 * nv * n;
+    const int v = (int)((r / n) % nv);
+    const long long j = r % n;
+    Y[f] = (T)((double)Y[f] - sp_step->qcf[v] * fr[b * n + j]);
+  }
 }
 
 template <typename A, typename B>
@@ -621,7 +653,7 @@ int grid_blocks(long long work) {
 
 template <typename T, int V, int CLOS>
 void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
-  int ba = grid_blocks(a.n), bk = grid_blocks(a.n / 2);
+  const dim3 ba(grid_blocks(a.n), c.nb), bk(grid_blocks(a.n / 2), c.nb), br(a.nblocks, c.nb);
   k_pass_a<T, V, CLOS><<<ba, kThreads, 0, c.stream>>>(a);
   typedef typename Cx<T>::t C;
   if (sizeof(T) == 8) {
@@ -635,7 +667,7 @@ void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   } else {
     cufftExecC2C(plan, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
   }
-  k_pass_r<T, V, CLOS><<<a.nblocks, kThreads, 0, c.stream>>>(a);
+  k_pass_r<T, V, CLOS><<<br, kThreads, 0, c.stream>>>(a);
   (void)sizeof(C);
 }
 
@@ -690,13 +722,17 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
   a.gout = snapshot ? c.d_g : nullptr;
   a.tw = (const typename Cx<T>::t *)(sizeof(T) == 8 ? (void *)c.d_tw : (void *)c.d_twf);
   // reset the per-run control words; AN2 count/binary persist
-  DevState hs;
-  if (!cuda_ok(c, cudaMemcpyAsync(&hs, c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream), "state read") ||
+  const int nb = c.nb;
+  std::vector<DevState> hs(nb);
+  if (!cuda_ok(c, cudaMemcpyAsync(hs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream), "state read") ||
       !cuda_ok(c, cudaStreamSynchronize(c.stream), "sync"))
     return RISM3D_CUDA_ERROR;
-  hs.done = 0; hs.after_done = 0; hs.iter = 0; hs.mode = 0;
-  hs.conv = conv; hs.maxstep = max_iter;
-  if (!cuda_ok(c, cudaMemcpyAsync(c.d_state, &hs, sizeof(DevState), cudaMemcpyHostToDevice, c.stream), "state write"))
+  for (DevState &h : hs) {
+    h.done = 0; h.after_done = 0; h.iter = 0; h.mode = 0;
+    h.conv = conv; h.maxstep = max_iter;
+  }
+  if (!cuda_ok(c, cudaMemcpyAsync(c.d_state, hs.data(), sizeof(DevState) * nb, cudaMemcpyHostToDevice, c.stream), "state write") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "sync"))
     return RISM3D_CUDA_ERROR;
   if (!cufft_ok(c, cufftSetStream(plan, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
   cudaGraphExec_t &gx = (sizeof(T) == 8) ? c.graph64 : c.graph32;
@@ -704,30 +740,39 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
   const int kRing = 4, kLag = 2;
   cudaEvent_t ev[kRing];
   for (int i = 0; i < kRing; ++i) cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
-  double best = 1e300;
-  int since_best = 0, launched = 0, status = RISM3D_OK, printed = 0;
+  // per solute: best rms seen and observations since it last improved
+  std::vector<double> best(nb, 1e300);
+  std::vector<int> since_best(nb, 0);
+  int launched = 0, status = RISM3D_OK, printed = 0;
   bool stop = false;
   while (!stop) {
     if (gx) cudaGraphLaunch(gx, c.stream);
     else launch_iteration<T, V, CLOS>(c, a, plan);
     c.launches += 3;
-    cudaMemcpyAsync(&c.h_state[launched % kRing], c.d_state, sizeof(DevState),
+    cudaMemcpyAsync(&c.h_state[(size_t)(launched % kRing) * nb], c.d_state, sizeof(DevState) * nb,
                     cudaMemcpyDeviceToHost, c.stream);
     cudaEventRecord(ev[launched % kRing], c.stream);
     ++launched;
     if (launched > kLag) {
       int k = (launched - 1 - kLag) % kRing;
       if (!cuda_ok(c, cudaEventSynchronize(ev[k]), "iteration")) { status = RISM3D_CUDA_ERROR; break; }
-      const DevState &s = c.h_state[k];
-      if (c.prm.verbose && s.iter > printed) {       // iterate.cu:63
-        printf(" Step = %d Reside = %g\n", s.iter, s.rms);
-        printed = s.iter;
+      const DevState *ss = &c.h_state[(size_t)k * nb];
+      if (nb == 1 && c.prm.verbose && ss[0].iter > printed) {   // iterate.cu:63
+        printf(" Step = %d Reside = %g\n", ss[0].iter, ss[0].rms);
+        printed = ss[0].iter;
       }
-      if (s.done) stop = true;
-      if (watch_stagnation && !stop) {
-        if (s.rms < 0.9 * best) { best = s.rms; since_best = 0; }
-        else if (++since_best > 30) stop = true;
+      bool all_done = true, all_idle = true;
+      for (int b = 0; b < nb; ++b) {
+        const DevState &s = ss[b];
+        if (!s.done) all_done = false;
+        if (watch_stagnation && !s.done) {
+          if (s.rms < 0.9 * best[b]) { best[b] = s.rms; since_best[b] = 0; }
+          else ++since_best[b];
+          if (since_best[b] <= 30) all_idle = false;
+        }
       }
+      if (all_done) stop = true;
+      if (watch_stagnation && all_idle) stop = true;
     }
     if (launched > max_iter + kLag + 2) stop = true;   // hard bound
   }
@@ -736,17 +781,20 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
     if (gx) cudaGraphLaunch(gx, c.stream);
     else launch_iteration<T, V, CLOS>(c, a, plan);
     c.launches += 3;
-    cudaMemcpyAsync(&c.h_state[0], c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream);
+    cudaMemcpyAsync(c.h_state, c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream);
     if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "iteration drain")) status = RISM3D_CUDA_ERROR;
   }
   for (int i = 0; i < kRing; ++i) cudaEventDestroy(ev[i]);
-  iters_out = c.h_state[0].iter;
+  iters_out = 0;
+  for (int b = 0; b < nb; ++b) iters_out = std::max(iters_out, c.h_state[b].iter);
   return status;
 }
 
 template <int V, int CLOS>
 int solve_v(Context &c, int chargeup) {
   const long long n = c.n;
+  const int nb = c.nb;
+  const long long vnb = (long long)V * n * nb;     // elements of a [B][V][N] grid
   const bool mixed = c.prm.precision == RISM3D_MIXED;
   const int gb = grid_blocks(n);
   StageParams sp{};
@@ -754,21 +802,24 @@ int solve_v(Context &c, int chargeup) {
   // stage schedule (iterate.cu:30-47)
   int cu = chargeup;
   double cf, cuf = 0.0;
-  const bool restart = !c.t_init.empty();
+  const bool restart = !c.t_init.empty() && nb == 1;
   if (restart) { cu = 0; cf = 1.0; }
   else if (cu == 0) cf = 1.0;
   else { cuf = 1.0 / cu; cf = 0.0; }
 
   // AN2 state (anderson.cu:13-32)
-  DevState hs{};
-  hs.count = c.prm.an2_count; hs.binary = 0; hs.m = c.prm.an2_m; hs.mp = c.prm.an2_mp;
-  hs.maxstep = c.prm.maxstep; hs.conv = c.prm.convergence;
-  cudaMemcpyAsync(c.d_state, &hs, sizeof(DevState), cudaMemcpyHostToDevice, c.stream);
-  cudaMemsetAsync(c.d_Y, 0, sizeof(double) * 2 * V * n, c.stream);
-  cudaMemsetAsync(c.d_RP, 0, sizeof(double) * 2 * V * n, c.stream);
+  std::vector<DevState> hs0(nb);
+  for (DevState &hs : hs0) {
+    hs = DevState{};
+    hs.count = c.prm.an2_count; hs.binary = 0; hs.m = c.prm.an2_m; hs.mp = c.prm.an2_mp;
+    hs.maxstep = c.prm.maxstep; hs.conv = c.prm.convergence;
+  }
+  cudaMemcpyAsync(c.d_state, hs0.data(), sizeof(DevState) * nb, cudaMemcpyHostToDevice, c.stream);
+  cudaMemsetAsync(c.d_Y, 0, sizeof(double) * 2 * vnb, c.stream);
+  cudaMemsetAsync(c.d_RP, 0, sizeof(double) * 2 * vnb, c.stream);
   if (mixed) {
-    cudaMemsetAsync(c.f_Y, 0, sizeof(float) * 2 * V * n, c.stream);
-    cudaMemsetAsync(c.f_RP, 0, sizeof(float) * 2 * V * n, c.stream);
+    cudaMemsetAsync(c.f_Y, 0, sizeof(float) * 2 * vnb, c.stream);
+    cudaMemsetAsync(c.f_RP, 0, sizeof(float) * 2 * vnb, c.stream);
   }
   // initial t_SR
   for (int v = 0; v < V; ++v) sp.qcf[v] = c.qv[v] * cf;
@@ -779,7 +830,7 @@ int solve_v(Context &c, int chargeup) {
         !cuda_ok(c, cudaMemcpyAsync(d_tinit, c.t_init.data(), sizeof(double) * V * n, cudaMemcpyHostToDevice, c.stream), "copy"))
       return RISM3D_CUDA_ERROR;
   }
-  k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, d_tinit, c.d_fr, c.d_stage, c.d_t);
+  k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, vnb, d_tinit, c.d_fr, c.d_stage, c.d_t);
   c.launches += 1;
   if (d_tinit) cudaFreeAsync(d_tinit, c.stream);
 
@@ -793,24 +844,24 @@ int solve_v(Context &c, int chargeup) {
       StageParams step{};
       for (int v = 0; v < V; ++v) step.qcf[v] = c.qv[v] * (cfn - cf);
       cudaMemcpyAsync(d_step, &step, sizeof(step), cudaMemcpyHostToDevice, c.stream);
-      k_shift_history<double><<<gb, kThreads, 0, c.stream>>>(n, V, c.d_fr, d_step, c.d_Y);
+      k_shift_history<double><<<gb, kThreads, 0, c.stream>>>(n, V, 2 * vnb, c.d_fr, d_step, c.d_Y);
       c.launches += 1;
       if (mixed) {
-        k_shift_history<float><<<gb, kThreads, 0, c.stream>>>(n, V, c.d_fr, d_step, c.f_Y);
+        k_shift_history<float><<<gb, kThreads, 0, c.stream>>>(n, V, 2 * vnb, c.d_fr, d_step, c.f_Y);
         c.launches += 1;
       }
       cf = cfn;
     }
     for (int v = 0; v < V; ++v) sp.qcf[v] = c.qv[v] * cf;
     cudaMemcpyAsync(c.d_stage, &sp, sizeof(sp), cudaMemcpyHostToDevice, c.stream);
-    k_stage_u<<<gb, kThreads, 0, c.stream>>>(n, V, c.d_u, c.d_e, c.d_stage, c.d_U, mixed ? c.f_U : nullptr);
+    k_stage_u<<<gb, kThreads, 0, c.stream>>>(n, V, vnb, c.d_u, c.d_e, c.d_stage, c.d_U, mixed ? c.f_U : nullptr);
     c.launches += 1;
     if (c.prm.verbose) printf("relaxing 3D UV RISM: Charge Up Factor = %g\n", cf);
     int left = c.prm.maxstep;
     if (mixed) {
       // FP32 bulk: t/history to FP32, iterate to the switch point or until
       // progress stalls, then promote back to FP64 for the polish.
-      const long long vn = (long long)V * n;
+      const long long vn = vnb;
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(vn, c.d_t, c.f_t);
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.d_Y, c.f_Y);
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.d_RP, c.f_RP);
@@ -821,14 +872,16 @@ int solve_v(Context &c, int chargeup) {
       int st = iterate_phase<float, V, CLOS>(c, c.plan32, c.f_t, c.f_U, c.f_Y, c.f_RP,
                                             c.f_buf, false, sw, left, true, it32);
       if (st != RISM3D_OK) { status = st; break; }
-      DevState s32;
-      cudaMemcpy(&s32, c.d_state, sizeof(s32), cudaMemcpyDeviceToHost);
+      std::vector<DevState> s32(nb);
+      cudaMemcpy(s32.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost);
+      bool any_div = false;
+      for (const DevState &x : s32) any_div = any_div || x.done == 2;
       total32 += it32;
       total += it32;
       left -= it32;
-      if (s32.done == 2) {
+      if (any_div) {
         // FP32 diverged: restart this stage in FP64 from the stage start
-        k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, nullptr, c.d_fr, c.d_stage, c.d_t);
+        k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, vnb, nullptr, c.d_fr, c.d_stage, c.d_t);
         c.launches += 1;
       } else {
         k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(vn, c.f_t, c.d_t);
@@ -843,13 +896,24 @@ int solve_v(Context &c, int chargeup) {
                                            c.d_buf, true, c.prm.convergence, left, false, it);
     if (st != RISM3D_OK) { status = st; break; }
     total += it;
-    DevState fs;
-    cudaMemcpy(&fs, c.d_state, sizeof(fs), cudaMemcpyDeviceToHost);
-    c.res.rms = fs.rms;
-    if (fs.done == 2) {                    // iterate.cu:74-75: report, go on
+    std::vector<DevState> fs(nb);
+    cudaMemcpy(fs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost);
+    c.res.rms = fs[0].rms;
+    if (nb > 1) {
+      c.bres.assign(nb, rism3d_result{});
+      for (int b = 0; b < nb; ++b) {
+        c.bres[b].rms = fs[b].rms;
+        c.bres[b].iterations = fs[b].iter;
+        c.bres[b].status = fs[b].done == 1 ? RISM3D_OK
+                         : fs[b].done == 2 ? RISM3D_DIVERGED : RISM3D_NOT_CONVERGED;
+      }
+    }
+    bool div = false, lim = false;
+    for (const DevState &x : fs) { div = div || x.done == 2; lim = lim || (x.done != 1 && x.done != 2); }
+    if (div) {                             // iterate.cu:74-75: report, go on
       if (c.prm.verbose) printf("Calculation diverged.\n");
       status = RISM3D_DIVERGED;
-    } else if (fs.done != 1) {             // iterate.cu:76-79: stop charging
+    } else if (lim) {                      // iterate.cu:76-79: stop charging
       if (c.prm.verbose) printf("3D UV RISM: reached limit # of relaxation steps: %d\n", c.prm.maxstep);
       status = RISM3D_NOT_CONVERGED;
       break;

@@ -187,6 +187,24 @@ class Solver:
         self._check(lib().rism3d_grad(self.h, _dp(dq), _dp(ds), _dp(de), _dp(dR)))
         return dq, ds, de, dR
 
+    def solve_batch(self, mols):
+        """mols: list of (sig, eps, q, xyz, grid, box), cubic cells; returns a
+        list of result dicts (rism3d_solve_batch)."""
+        natoms = np.array([len(m[2]) for m in mols], dtype=np.int32)
+        grids = np.array([int(m[4]) for m in mols], dtype=np.int32)
+        boxes = _f64([float(m[5]) for m in mols])
+        sig = _f64(np.concatenate([np.asarray(m[0], float) for m in mols]))
+        eps = _f64(np.concatenate([np.asarray(m[1], float) for m in mols]))
+        q = _f64(np.concatenate([np.asarray(m[2], float) for m in mols]))
+        xyz = _f64(np.concatenate([np.asarray(m[3], float).reshape(-1, 3) for m in mols]))
+        res = (Result * len(mols))()
+        ip = C.POINTER(C.c_int)
+        self._check(lib().rism3d_solve_batch(
+            self.h, len(mols), natoms.ctypes.data_as(ip), grids.ctypes.data_as(ip),
+            _dp(boxes), _dp(sig), _dp(eps), _dp(q), _dp(xyz), res),
+            (OK, DIVERGED, NOT_CONVERGED))
+        return [r.as_dict() for r in res]
+
     def refresh_potentials(self):
         self._check(lib().rism3d_refresh_potentials(self.h))
 

@@ -1,0 +1,63 @@
+"""Batched solves of many small solutes (rism3d_solve_batch): every solute
+of a mixed-size batch gets the result of its own single solve, and the
+single solves agree with the oracle."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from helpers import MU_TOL
+from oracle import formats as F
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _mols():
+    import rism3d_b200.synth as S
+    out = []
+    for k, (g, L) in enumerate([(32, 16.0), (48, 24.0), (32, 16.0), (64, 32.0), (48, 24.0),
+                                (64, 32.0), (32, 16.0)]):
+        m = S.small_chain(seed=100 + k, natom=8 + 4 * k, grid=(g, g, g), box=(L, L, L))
+        F.centre(m.xyz)
+        out.append((m.sig, m.eps, m.q, m.xyz, g, L))
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_matches_single_solves(precision):
+    import rism3d_b200 as R
+    sv = F.read_xvk(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    mols = _mols()
+    parent = R.Solver((32, 32, 32), (16.0, 16.0, 16.0), precision=precision)
+    parent.set_solvent_obj(sv)
+    res = parent.solve_batch(mols)
+    res2 = parent.solve_batch(mols)               # cached children, same answers
+    for i, (sig, eps, q, xyz, g, L) in enumerate(mols):
+        s = R.Solver((g, g, g), (L, L, L), precision=precision)
+        s.set_solvent_obj(sv)
+        s.set_solute(sig, eps, q, xyz)
+        r = s.solve()
+        s.close()
+        assert res[i]["status"] == 0
+        assert abs(res[i]["sfe_sc"] - r["sfe_sc"]) < MU_TOL, i
+        assert abs(res[i]["sfe_gf"] - r["sfe_gf"]) < MU_TOL, i
+        assert abs(res[i]["pmv"] - r["pmv"]) < 1e-4, i
+        assert abs(res[i]["se"] - r["se"]) < 1e-4 * abs(r["se"]) + 1e-3, i
+        assert res2[i]["sfe_sc"] == res[i]["sfe_sc"]
+    parent.close()
+
+
+def test_batch_member_matches_oracle():
+    import rism3d_b200 as R
+    sv = F.read_xvk(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    mols = _mols()
+    parent = R.Solver((32, 32, 32), (16.0, 16.0, 16.0))
+    parent.set_solvent_obj(sv)
+    res = parent.solve_batch(mols)
+    parent.close()
+    sig, eps, q, xyz, g, L = mols[1]
+    o = O.solve(O.Case((g, g, g), (L, L, L), sv, sig, eps, q, xyz))
+    assert abs(res[1]["sfe_sc"] - o["sfe_sc"]) < MU_TOL
+    assert abs(res[1]["pmv"] - o["pmv"] * 1000) < 1e-4
