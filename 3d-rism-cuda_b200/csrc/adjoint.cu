@@ -1,20 +1,41 @@
 // Adjoint gradients of the solvation free energy SFE_SC with respect to the
-// solute parameters (charges, LJ sigma and epsilon, positions).
+// solute parameters (charges, LJ sigma and epsilon, positions): the exact
+// derivative of the reference's discrete mu_ex (cal_exchem.cu:55-122) at
+// the converged solution.
 //
-// For the KH and HNC closures the reference's free-energy expression
-// (cal_exchem.cu:55-122) is stationary with respect to the correlation
-// functions at the solution, so the derivative with respect to any solute
-// parameter p only sees the explicit potential:
+// With t the state, x = -beta u - q e + t the closure argument, g = C(x),
+// h the OZ result and c = h - t, the discrete equations of the reference
+// (calculate_cuda.cu, fft3d.cu) are h = L(c + delta), where L is the OZ
+// operator (L v)_a = F^-1[sum_b X_ab F[v_b]] -- symmetric in the inner
+// product weighted by rho, since rho_a X_ab = rho_b X_ba -- and
+// delta_a = q_a (fr - F^-1[fk]) is the mismatch between the real-space
+// long-range grid and its analytic transform (cal_Coulomb.cu:109-140: fk is
+// not the discrete transform of fr).  Differentiating the KH/HNC functional
+// at the solution and eliminating dc/dp with one adjoint solve gives
 //
-//   dSFE/dp = N_A kB T sum_v rho_v dv sum_r g_v(r) d(beta u_v(r))/dp
+//   dSFE/dp / (N_A kB T) = <rho (g - zeta/2), d(beta u)/dp>
+//                          + 1/2 <sum_a rho_a q_a (zeta_a - h_a), d(fr - F^-1 fk)/dp>
 //
-// with beta u_v = beta u_LJ,v + q_v beta e (cal_LJ.cu:57-71,
-// cal_Coulomb.cu:109-121).  The kernel back-propagates w_v(r) = rho_v g_v(r)
-// through the potential-grid computation: one atom per thread, grid points
-// streamed through shared memory, and every pair term recomputed from the
-// atom parameters instead of being stored.  Per pair it uses the same
-// rules as the forward kernel: r^2 clamped at 1e-4 for LJ (no positional
-// derivative inside the clamp) and no Coulomb term below r = 1e-5.
+// with zeta = L xi + w, w = L delta and xi the solution of the linear system
+//   G xi - (G - 1) L xi = (G - 1) w,      G = C'(x)
+// (the transpose of the solve's own Jacobian; no division by g, which is 0
+// in the solute core).  Without the mismatch (delta = 0) zeta vanishes and
+// the first term is the familiar <rho g d(beta u)/dp>.
+//
+// Inside the solute core G underflows and the system pins zeta to
+// G xi / (G - 1), i.e. to zero with g.  The iterative solve leaves a residual
+// of order its tolerance in L xi + w there, which the steep repulsive
+// potential (d(beta u)/dp ~ r^-14 near an atom) would amplify; zeta is
+// therefore taken from the pointwise form wherever G < 1/2, where both forms
+// agree at the solution.
+//
+// Kernels: the linear solve reuses the k-space OZ pass of the iteration
+// around cuFFT and is accelerated by Anderson mixing (depth 6); the gradient
+// back-propagates the weights through the potential-grid computation, one
+// atom per thread with grid points streamed through shared memory and every
+// pair term recomputed (cal_LJ.cu:57-71, cal_Coulomb.cu:109-121), and through
+// the k-space fk kernel with per-axis phase rows.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -23,21 +44,198 @@
 namespace rism3d {
 namespace {
 
+constexpr int kThreads = 256;
 constexpr int kAtomsPerBlock = 128;
 constexpr int kPtsTile = 128;
 constexpr int NOUT = 6;   // dq, dsigma, deps, dRx, dRy, dRz
+constexpr int kDepth = 6; // Anderson history of the adjoint solve
+constexpr int kDotBlocks = 2368;
 
 struct SiteW {
   double sig[kMaxSites], eps[kMaxSites], q[kMaxSites], rho[kMaxSites];
 };
 
+__device__ __forceinline__ void point_dir_dkf(long long j, int nx, int ny, const double2 *tw,
+                                              int &dir, double2 &dkf) {
+  const long long r = j / nx;
+  const int ix = (int)(j - r * nx), iy = (int)(r % ny), iz = (int)(r / ny);
+  dir = ((ix + iy + iz) & 1) ? -1 : 1;
+  const double2 a = tw[ix], b = tw[nx + iy], c = tw[nx + ny + iz];
+  const double2 ab = make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  dkf = make_double2(ab.x * c.x - ab.y * c.y, ab.x * c.y + ab.y * c.x);
+}
+
+// real grids v[V][N] -> packed pairs buf[P][N] with the forward pre-twiddle
+// dir dkf (timekf, fft3d.cu:41-49)
+__global__ void k_pack(long long n, int nv, int nx, int ny, const double2 *tw,
+                       const double *v, double2 *buf) {
+  const int P = (nv + 1) / 2;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    int dir;
+    double2 w;
+    point_dir_dkf(j, nx, ny, tw, dir, w);
+    for (int p = 0; p < P; ++p) {
+      const double a = v[(size_t)(2 * p) * n + j];
+      const double b = (2 * p + 1 < nv) ? v[(size_t)(2 * p + 1) * n + j] : 0.0;
+      buf[(size_t)p * n + j] = make_double2(dir * (a * w.x - b * w.y), dir * (a * w.y + b * w.x));
+    }
+  }
+}
+
+// packed pairs after the inverse FFT -> real grids, post-twiddle
+// (1/V) dir conj(dkf) (timekb, fft3d.cu:52-60)
+__global__ void k_unpack(long long n, int nv, int nx, int ny, const double2 *tw, double invvol,
+                         const double2 *buf, double *out) {
+  const int P = (nv + 1) / 2;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    int dir;
+    double2 w;
+    point_dir_dkf(j, nx, ny, tw, dir, w);
+    const double s = invvol * dir;
+    for (int p = 0; p < P; ++p) {
+      const double2 z = buf[(size_t)p * n + j];
+      const double re = s * (z.x * w.x + z.y * w.y), im = s * (z.y * w.x - z.x * w.y);
+      out[(size_t)(2 * p) * n + j] = re;
+      if (2 * p + 1 < nv) out[(size_t)(2 * p + 1) * n + j] = im;
+    }
+  }
+}
+
+// inverse-transform input for the real function with transform fk (owner
+// half stored): dir fk at k and -dir conj(fk) at the mirror -k
+__global__ void k_fk_to_buf(long long n, int nx, int ny, const double2 *fkh, double2 *buf) {
+  const long long nh = n / 2;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nh;
+       j += (long long)gridDim.x * blockDim.x) {
+    const long long r = j / nx;
+    const int ix = (int)(j - r * nx), iy = (int)(r % ny), iz = (int)(r / ny);
+    const int dir = ((ix + iy + iz) & 1) ? -1 : 1;
+    const double2 f = fkh[j];
+    buf[j] = make_double2(dir * f.x, dir * f.y);
+    buf[n - 1 - j] = make_double2(-dir * f.x, dir * f.y);
+  }
+}
+
+// delta_a = q_a (fr - F^-1 fk)
+__global__ void k_delta(long long n, int nv, const double *fr, const double *finv,
+                        const StageParams *sp, double *delta) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const double d = fr[j] - finv[j];
+    for (int v = 0; v < nv; ++v) delta[(size_t)v * n + j] = sp->qcf[v] * d;
+  }
+}
+
+// closure derivative G = C'(x), x = t_SR - U_SR (KH: 1 for x >= 0, else e^x)
+__global__ void k_gprime(long long tot, int closure, const double *t, const double *U, double *G) {
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
+       f += (long long)gridDim.x * blockDim.x) {
+    const double x = t[f] - U[f];
+    G[f] = (closure == 0 && x >= 0.0) ? 1.0 : exp(x);
+  }
+}
+
+// r = (G - 1)(w + L xi) - G xi
+__global__ void k_residual(long long tot, const double *G, const double *w, const double *Lxi,
+                           const double *xi, double *r) {
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
+       f += (long long)gridDim.x * blockDim.x)
+    r[f] = (G[f] - 1.0) * (w[f] + Lxi[f]) - G[f] * xi[f];
+}
+
+// partial dot products of r with the first ns history residuals and with
+// itself (last row); summed in a fixed order by k_sum_rows
+__global__ void k_dots(long long tot, const double *r, const double *const *hist, int ns,
+                       double *part) {
+  __shared__ double red[kThreads / 32][kDepth + 1];
+  double acc[kDepth + 1];
+  for (int i = 0; i <= kDepth; ++i) acc[i] = 0.0;
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
+       f += (long long)gridDim.x * blockDim.x) {
+    const double x = r[f];
+    acc[kDepth] += x * x;
+    for (int i = 0; i < ns; ++i) acc[i] += x * hist[i][f];
+  }
+  for (int i = 0; i <= kDepth; ++i) {
+    double v = acc[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[i] = v;
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int i = 0; i <= kDepth; ++i) red[wid][i] = acc[i];
+  __syncthreads();
+  if (threadIdx.x <= kDepth) {
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) s += red[w][threadIdx.x];
+    part[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+__global__ void k_sum_rows(const double *part, int ncols, double *out) {
+  __shared__ double red[kThreads];
+  const int k = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < ncols; b += blockDim.x) s += part[(size_t)k * ncols + b];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[k] = red[0];
+}
+
+struct Mix {
+  const double *xs[kDepth];
+  const double *rs[kDepth];
+  double c[kDepth];
+  int ns;
+  double eta;
+};
+
+// xi = sum_i c_i (xi_i + eta r_i)
+__global__ void k_combine(long long tot, Mix mx, double *xi) {
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
+       f += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int i = 0; i < mx.ns; ++i) s += mx.c[i] * (mx.xs[i][f] + mx.eta * mx.rs[i][f]);
+    xi[f] = s;
+  }
+}
+
+// zeta (L xi + w, or G xi / (G - 1) where G < 1/2), then the weights
+//   W_a = rho_a (g_a - zeta_a / 2),  Omega = sum_a rho_a q_a (zeta_a - h_a)
+__global__ void k_weights(long long n, int nv, const double *g, const double *h,
+                          const double *G, const double *xi, const double *Lxi,
+                          const double *w, SiteW sv, double *W, double *Om) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    double om = 0.0;
+    for (int v = 0; v < nv; ++v) {
+      const size_t i = (size_t)v * n + j;
+      const double gp = G[i];
+      const double zeta = gp < 0.5 ? gp * xi[i] / (gp - 1.0) : Lxi[i] + w[i];
+      W[i] = sv.rho[v] * (g[i] - 0.5 * zeta);
+      om += sv.rho[v] * sv.q[v] * (zeta - h[i]);
+    }
+    Om[j] = om;
+  }
+}
+
+// Real-space back-propagation, one atom per thread:
+//   W-weighted derivatives of beta u_LJ (N_A kB T units cancel) and of
+//   q_v e (x cc), plus the Omega-weighted derivative of fr (x cc / 2).
 template <int V>
 __global__ void __launch_bounds__(kAtomsPerBlock)
-k_adjoint(int nx, int ny, int nz, double drx, double dry, double drz,
-          const double *__restrict__ g, const double *__restrict__ atoms, int natom,
-          SiteW sv, double cc, long long chunk, double *part) {
-  __shared__ double4 pp[kPtsTile];
-  __shared__ double pw[V][kPtsTile];       // rho_v g_v at the point
+k_adjoint_r(int nx, int ny, int nz, double drx, double dry, double drz,
+            const double *__restrict__ W, const double *__restrict__ Om,
+            const double *__restrict__ atoms, int natom, SiteW sv, double cc,
+            long long chunk, double *part) {
+  __shared__ double4 pp[kPtsTile];          // x y z Omega
+  __shared__ double pw[V][kPtsTile];
   const long long n = (long long)nx * ny * nz;
   const int ia = blockIdx.x * kAtomsPerBlock + threadIdx.x;
   const bool live = ia < natom;
@@ -52,7 +250,7 @@ k_adjoint(int nx, int ny, int nz, double drx, double dry, double drz,
     sg[v] = (su + sv.sig[v]) * 0.5;               // cal_LJ.cu:28
     sg2[v] = sg[v] * sg[v];
     euv[v] = sqrt(eu * sv.eps[v]);               // cal_LJ.cu:29
-    deps_fac[v] = eu > 0.0 ? 0.5 * euv[v] / eu : 0.0;   // d eps_uv / d eps_u
+    deps_fac[v] = eu > 0.0 ? 0.5 * euv[v] / eu : 0.0;
     qc[v] = sv.q[v] * cc;
   }
   double acc[NOUT] = {0, 0, 0, 0, 0, 0};
@@ -65,9 +263,9 @@ k_adjoint(int nx, int ny, int nz, double drx, double dry, double drz,
       if (j < j1) {
         const long long r = j / nx;
         const int ix = (int)(j - r * nx), iy = (int)(r % ny), iz = (int)(r / ny);
-        pp[i] = make_double4((ix - nx / 2) * drx, (iy - ny / 2) * dry, (iz - nz / 2) * drz, 0.0);
+        pp[i] = make_double4((ix - nx / 2) * drx, (iy - ny / 2) * dry, (iz - nz / 2) * drz, Om[j]);
 #pragma unroll
-        for (int v = 0; v < V; ++v) pw[v][i] = sv.rho[v] * g[(size_t)v * n + j];
+        for (int v = 0; v < V; ++v) pw[v][i] = W[(size_t)v * n + j];
       } else {
         pp[i] = make_double4(1.0e30, 1.0e30, 1.0e30, 0.0);
 #pragma unroll
@@ -81,27 +279,37 @@ k_adjoint(int nx, int ny, int nz, double drx, double dry, double drz,
       const double4 p = pp[i];
       const double dx = p.x - X, dy = p.y - Y, dz = p.z - Z;
       const double r2 = dx * dx + dy * dy + dz * dz;
-      const bool clamped = r2 < 1.0e-4;
+      const bool clamped = r2 < 1.0e-4;            // cal_LJ.cu:64
       const double ir2 = clamped ? 1.0e4 : 1.0 / r2;
       const double ri = r2 > 0.0 ? rsqrt(r2) : 0.0;
-      const bool coul = r2 * ri >= 1.0e-5;
-      double wsum_q = 0.0, fr = 0.0;
+      const double ra = r2 * ri;
+      const bool coul = ra >= 1.0e-5;              // cal_Coulomb.cu:114
+      double wq = 0.0, fr = 0.0;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         const double w = pw[v][i];
         const double s2 = sg2[v] * ir2;
         const double s6 = s2 * s2 * s2, s12 = s6 * s6;
-        // d/d sigma_u of 4 eps (s^12 - s^6): (24 eps/sigma_uv)(2 s^12 - s^6) / 2
-        acc[1] += w * 12.0 * euv[v] / sg[v] * (2.0 * s12 - s6);
-        // d/d eps_u: 4 (s^12 - s^6) d eps_uv / d eps_u
-        acc[2] += w * 4.0 * (s12 - s6) * deps_fac[v];
-        // d/d R_u: 24 eps (2 s^12 - s^6) / r^2 (r - R_u)  (cal_grad.cu:73)
-        if (!clamped) fr += w * 24.0 * euv[v] * (2.0 * s12 - s6) * ir2;
-        if (coul) wsum_q += w * qc[v];
+        // w = 0 in the solute core, where g and zeta underflow
+        if (w != 0.0) {
+          acc[1] += w * 12.0 * euv[v] / sg[v] * (2.0 * s12 - s6);  // d/d sigma_u
+          acc[2] += w * 4.0 * (s12 - s6) * deps_fac[v];           // d/d eps_u
+          if (!clamped) fr += w * 24.0 * euv[v] * (2.0 * s12 - s6) * ir2;
+        }
+        if (coul) wq += w * qc[v];
       }
+      // half-weighted long-range term: phi(r) = (1 - e^-r)/r, phi = 1 below 1e-5
+      const double om = 0.5 * cc * p.w;
       if (coul) {
-        acc[0] += wsum_q * ri;                     // d/d q_u of q_u q_v cc / r
-        fr += wsum_q * qu * ri * ri * ri;          // q_u q_v cc (r - R_u) / r^3
+        acc[0] += wq * ri;
+        fr += wq * qu * ri * ri * ri;
+        const double em = exp(-ra);
+        const double phi = (1.0 - em) * ri;
+        const double dphi = (ra * em - (1.0 - em)) * ri * ri;      // d phi / d r
+        acc[0] += om * phi;
+        fr -= om * qu * dphi * ri;                 // d phi(|p - R|)/dR = -phi' (p - R)/r
+      } else {
+        acc[0] += om;                              // fr gets q below 1e-5
       }
       acc[3] += fr * dx;
       acc[4] += fr * dy;
@@ -115,51 +323,328 @@ k_adjoint(int nx, int ny, int nz, double drx, double dry, double drz,
   }
 }
 
-__global__ void k_adjoint_sum(const double *part, int nchunk, int natom, double *out) {
+// k-space back-propagation of the fk term: per atom
+//   scale * sum over the owner half of e^{-ik.R} 4 pi conj(Omega^) / (k^2 (k^2+1))
+// (the mirror half contributes the complex conjugate, folded into scale)
+__global__ void __launch_bounds__(kAtomsPerBlock)
+k_adjoint_k(int nx, int ny, int nz, double bx, double by, double bz, const double2 *omh,
+            const double2 *ph, const double *atoms, int natom, double scale, long long chunk,
+            double *part) {
+  __shared__ double2 sw[kPtsTile];            // 4 pi conj(Omega^) / (k^2 (k^2 + 1))
+  __shared__ double4 sk[kPtsTile];            // kx ky kz
+  __shared__ int4 si[kPtsTile];               // ix iy iz
+  const long long nh = (long long)nx * ny * nz / 2;
+  const int L = nx + ny + nz;
+  const int ia = blockIdx.x * kAtomsPerBlock + threadIdx.x;
+  const bool live = ia < natom;
+  const double qu = live ? atoms[8 * (size_t)ia + 3] : 0.0;
+  const double2 *row = ph + (size_t)(live ? ia : 0) * L;
+  double aq = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+  const long long j0 = (long long)blockIdx.y * chunk;
+  const long long j1 = min(nh, j0 + chunk);
+  for (long long base = j0; base < j1; base += kPtsTile) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < kPtsTile; i += blockDim.x) {
+      const long long j = base + i;
+      if (j < j1) {
+        const long long r = j / nx;
+        const int ix = (int)(j - r * nx), iy = (int)(r % ny), iz = (int)(r / ny);
+        const double kx = 2.0 * kPi * (ix - nx / 2.0 + 0.5) / bx;   // set_g
+        const double ky = 2.0 * kPi * (iy - ny / 2.0 + 0.5) / by;
+        const double kz = 2.0 * kPi * (iz - nz / 2.0 + 0.5) / bz;
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        const double f = 4.0 * kPi / (k2 * (k2 + 1.0));
+        const double2 o = omh[j];
+        sw[i] = make_double2(o.x * f, -o.y * f);
+        sk[i] = make_double4(kx, ky, kz, 0.0);
+        si[i] = make_int4(ix, iy, iz, 0);
+      } else {
+        sw[i] = make_double2(0.0, 0.0);
+        sk[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+        si[i] = make_int4(0, 0, 0, 0);
+      }
+    }
+    __syncthreads();
+    if (!live) continue;
+    const int m = (int)min((long long)kPtsTile, j1 - base);
+    for (int i = 0; i < m; ++i) {
+      const int4 id = si[i];
+      const double2 px = row[id.x], py = row[nx + id.y], pz = row[nx + ny + id.z];
+      const double yzr = py.x * pz.x - py.y * pz.y, yzi = py.x * pz.y + py.y * pz.x;
+      const double er = px.x * yzr - px.y * yzi, ei = px.x * yzi + px.y * yzr;  // e^{-ik.R}
+      const double2 w = sw[i];
+      const double pr = er * w.x - ei * w.y, pim = er * w.y + ei * w.x;
+      aq += pr;                                     // d/dq_u: Re(e^{-ik.R} w)
+      ax += sk[i].x * pim;                          // d/dR_u: Re(-i k q e^{-ik.R} w)
+      ay += sk[i].y * pim;
+      az += sk[i].z * pim;
+    }
+  }
+  if (live) {
+    double *o = part + ((size_t)blockIdx.y * natom + ia) * 4;
+    o[0] = scale * aq;
+    o[1] = scale * qu * ax;
+    o[2] = scale * qu * ay;
+    o[3] = scale * qu * az;
+  }
+}
+
+// Omega^ = F[Omega] on the owner half: dv dir Y (Y = FFT of dir dkf Omega;
+// the packed imaginary part is zero, so no unpacking is needed)
+__global__ void k_forward_post(long long n, int nx, int ny, double dv, const double2 *buf,
+                               double2 *out) {
+  const long long nh = n / 2;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nh;
+       j += (long long)gridDim.x * blockDim.x) {
+    const long long r = j / nx;
+    const int ix = (int)(j - r * nx), iy = (int)(r % ny), iz = (int)(r / ny);
+    const double s = dv * (((ix + iy + iz) & 1) ? -1.0 : 1.0);
+    const double2 y = buf[j];
+    out[j] = make_double2(s * y.x, s * y.y);
+  }
+}
+
+__global__ void k_sum_chunks(const double *part, int nchunk, int natom, int na, double *out) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= natom * NOUT) return;
+  if (idx >= natom * na) return;
   double s = 0.0;
-  for (int c = 0; c < nchunk; ++c) s += part[(size_t)c * natom * NOUT + idx];
+  for (int c = 0; c < nchunk; ++c) s += part[(size_t)c * natom * na + idx];
   out[idx] = s;
+}
+
+// per-atom phase rows e^{-i k_x X}, e^{-i k_y Y}, e^{-i k_z Z}
+__global__ void k_phase_rows_adj(int nx, int ny, int nz, double bx, double by, double bz,
+                                 const double *__restrict__ atoms, int natom,
+                                 double2 *__restrict__ ph) {
+  const int L = nx + ny + nz;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)natom * L) return;
+  const int u = (int)(idx / L), i = (int)(idx % L);
+  double k, R;
+  if (i < nx) { k = 2.0 * kPi * (i - nx / 2.0 + 0.5) / bx; R = atoms[8 * (size_t)u + 0]; }
+  else if (i < nx + ny) { k = 2.0 * kPi * (i - nx - ny / 2.0 + 0.5) / by; R = atoms[8 * (size_t)u + 1]; }
+  else { k = 2.0 * kPi * (i - nx - ny - nz / 2.0 + 0.5) / bz; R = atoms[8 * (size_t)u + 2]; }
+  double s, c;
+  sincos(k * R, &s, &c);
+  ph[idx] = make_double2(c, -s);
+}
+
+int blocks_for(long long work) {
+  long long b = (work + kThreads - 1) / kThreads;
+  return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+// Device scratch of one adjoint evaluation (stream-ordered, freed at the end).
+struct Scratch {
+  std::vector<void *> ptrs;
+  Context &c;
+  explicit Scratch(Context &cc) : c(cc) {}
+  template <typename T> T *get(size_t count) {
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, sizeof(T) * count, c.stream) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return (T *)p;
+  }
+  ~Scratch() {
+    for (void *p : ptrs) cudaFreeAsync(p, c.stream);
+    cudaStreamSynchronize(c.stream);
+  }
+};
+
+// Solve min |sum c_i r_i| subject to sum c_i = 1 over m stored residuals
+// (Gram matrix gram[a][b] = <r_a, r_b>) by the bordered normal equations.
+void anderson_coefficients(const std::vector<double> &gram, int m, std::vector<double> &c) {
+  const int dd = m + 1;
+  std::vector<double> M((size_t)dd * dd, 0.0), rhs(dd, 0.0), x(dd, 0.0);
+  double sc = 0.0;
+  for (int a = 0; a < m; ++a) sc = std::max(sc, gram[(size_t)a * kDepth + a]);
+  if (!(sc > 0)) sc = 1.0;
+  for (int a = 0; a < m; ++a) {
+    for (int b = 0; b < m; ++b) M[(size_t)a * dd + b] = gram[(size_t)a * kDepth + b] / sc;
+    M[(size_t)a * dd + m] = 1.0;
+    M[(size_t)m * dd + a] = 1.0;
+  }
+  rhs[m] = 1.0;
+  for (int col = 0; col < dd; ++col) {                 // partial pivoting
+    int pv = col;
+    for (int rr = col + 1; rr < dd; ++rr)
+      if (fabs(M[(size_t)rr * dd + col]) > fabs(M[(size_t)pv * dd + col])) pv = rr;
+    for (int k = 0; k < dd; ++k) std::swap(M[(size_t)col * dd + k], M[(size_t)pv * dd + k]);
+    std::swap(rhs[col], rhs[pv]);
+    const double piv = M[(size_t)col * dd + col];
+    if (fabs(piv) < 1e-300) continue;
+    for (int rr = col + 1; rr < dd; ++rr) {
+      const double f = M[(size_t)rr * dd + col] / piv;
+      for (int k = col; k < dd; ++k) M[(size_t)rr * dd + k] -= f * M[(size_t)col * dd + k];
+      rhs[rr] -= f * rhs[col];
+    }
+  }
+  for (int rr = dd - 1; rr >= 0; --rr) {
+    double s = rhs[rr];
+    for (int k = rr + 1; k < dd; ++k) s -= M[(size_t)rr * dd + k] * x[k];
+    const double piv = M[(size_t)rr * dd + rr];
+    x[rr] = fabs(piv) < 1e-300 ? 0.0 : s / piv;
+  }
+  c.assign(x.begin(), x.begin() + m);
 }
 
 template <int V>
 int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
+  const long long n = c.n, tot = (long long)V * n;
+  const int P = (V + 1) / 2, gb = blocks_for(n), gt = blocks_for(tot);
   const int A = c.natom;
-  const int tiles = (A + kAtomsPerBlock - 1) / kAtomsPerBlock;
-  int nchunk = (148 * 8 + tiles - 1) / tiles;
-  long long chunk = (c.n + nchunk - 1) / nchunk;
-  chunk = ((chunk + kPtsTile - 1) / kPtsTile) * kPtsTile;
-  nchunk = (int)((c.n + chunk - 1) / chunk);
-  double *part = nullptr;
-  const size_t need = (size_t)nchunk * A * NOUT + (size_t)A * NOUT;
-  if (!cuda_ok(c, cudaMallocAsync(&part, sizeof(double) * need, c.stream), "adjoint scratch"))
+  Scratch S(c);
+  double *G = S.get<double>(tot), *w = S.get<double>(tot), *xi = S.get<double>(tot);
+  double *Lxi = S.get<double>(tot), *tmp = S.get<double>(tot), *Om = S.get<double>(n);
+  double *xs = S.get<double>((size_t)kDepth * tot), *rs = S.get<double>((size_t)kDepth * tot);
+  double *dpart = S.get<double>((size_t)(kDepth + 1) * kDotBlocks);
+  double *dsum = S.get<double>(kDepth + 1);
+  double **hist = S.get<double *>(kDepth);
+  StageParams *sp0 = S.get<StageParams>(1), *spq = S.get<StageParams>(1);
+  DevState *st0 = S.get<DevState>(1);
+  double2 *buf = c.d_buf;                       // the solve is finished: reuse
+  if (!G || !w || !xi || !Lxi || !tmp || !Om || !xs || !rs || !dpart || !dsum || !hist ||
+      !sp0 || !spq || !st0) {
+    c.err = "adjoint: out of device memory";
     return RISM3D_CUDA_ERROR;
+  }
+  StageParams zero{}, q{};
+  for (int v = 0; v < V; ++v) q.qcf[v] = c.qv[v] * c.cf_final;
+  DevState run{};
+  std::vector<const double *> hp(kDepth);
+  for (int i = 0; i < kDepth; ++i) hp[i] = rs + (size_t)i * tot;
+  if (!cuda_ok(c, cudaMemcpyAsync(sp0, &zero, sizeof(zero), cudaMemcpyHostToDevice, c.stream), "adjoint") ||
+      !cuda_ok(c, cudaMemcpyAsync(spq, &q, sizeof(q), cudaMemcpyHostToDevice, c.stream), "adjoint") ||
+      !cuda_ok(c, cudaMemcpyAsync(st0, &run, sizeof(run), cudaMemcpyHostToDevice, c.stream), "adjoint") ||
+      !cuda_ok(c, cudaMemcpyAsync(hist, hp.data(), sizeof(double *) * kDepth,
+                                  cudaMemcpyHostToDevice, c.stream), "adjoint") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "adjoint"))
+    return RISM3D_CUDA_ERROR;
+  if (!cufft_ok(c, cufftSetStream(c.plan64, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
+  auto fft = [&](int dir) {
+    return cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)buf, (cufftDoubleComplex *)buf, dir);
+  };
+  // (L v)_a = F^-1[sum_b X_ab F[v_b]]
+  auto applyL = [&](const double *v, double *out) -> int {
+    k_pack<<<gb, kThreads, 0, c.stream>>>(n, V, c.nx, c.ny, c.d_tw, v, buf);
+    if (fft(CUFFT_FORWARD) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
+    int rc = launch_oz_kspace(c, buf, sp0, st0);
+    if (rc != RISM3D_OK) return rc;
+    if (fft(CUFFT_INVERSE) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
+    k_unpack<<<gb, kThreads, 0, c.stream>>>(n, V, c.nx, c.ny, c.d_tw, 1.0 / c.vol, buf, out);
+    c.launches += 2;
+    return RISM3D_OK;
+  };
+  // delta = q (fr - F^-1 fk) (into tmp), w = L delta
+  cudaMemsetAsync(buf, 0, sizeof(double2) * P * n, c.stream);
+  k_fk_to_buf<<<gb, kThreads, 0, c.stream>>>(n, c.nx, c.ny, c.d_fkh, buf);
+  if (fft(CUFFT_INVERSE) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
+  k_unpack<<<gb, kThreads, 0, c.stream>>>(n, 1, c.nx, c.ny, c.d_tw, 1.0 / c.vol, buf, Om);
+  k_delta<<<gb, kThreads, 0, c.stream>>>(n, V, c.d_fr, Om, spq, tmp);
+  c.launches += 3;
+  int rc = applyL(tmp, w);
+  if (rc != RISM3D_OK) return rc;
+  k_gprime<<<gt, kThreads, 0, c.stream>>>(tot, c.prm.closure, c.d_t, c.d_U, G);
+  c.launches += 1;
+  // Anderson-accelerated solve of G xi - (G - 1) L xi = (G - 1) w from xi = 0
+  cudaMemsetAsync(xi, 0, sizeof(double) * tot, c.stream);
+  cudaMemsetAsync(xs, 0, sizeof(double) * kDepth * tot, c.stream);
+  cudaMemsetAsync(rs, 0, sizeof(double) * kDepth * tot, c.stream);
+  std::vector<double> gram((size_t)kDepth * kDepth, 0.0), coef;
+  double bnorm = -1.0;
+  int ns = 0, slot = 0, it = 0;
+  const double eta = 0.5, tol = 1.0e-10;
+  const int maxit = 3000;
+  for (; it < maxit; ++it) {
+    rc = applyL(xi, Lxi);
+    if (rc != RISM3D_OK) return rc;
+    double *r = rs + (size_t)slot * tot;
+    k_residual<<<gt, kThreads, 0, c.stream>>>(tot, G, w, Lxi, xi, r);
+    cudaMemcpyAsync(xs + (size_t)slot * tot, xi, sizeof(double) * tot, cudaMemcpyDeviceToDevice,
+                    c.stream);
+    const int nd = ns < kDepth ? ns + 1 : kDepth;      // filled slots incl. this one
+    k_dots<<<kDotBlocks, kThreads, 0, c.stream>>>(tot, r, hist, nd, dpart);
+    k_sum_rows<<<kDepth + 1, kThreads, 0, c.stream>>>(dpart, kDotBlocks, dsum);
+    c.launches += 3;
+    double d[kDepth + 1];
+    if (!cuda_ok(c, cudaMemcpyAsync(d, dsum, sizeof(d), cudaMemcpyDeviceToHost, c.stream), "adjoint") ||
+        !cuda_ok(c, cudaStreamSynchronize(c.stream), "adjoint"))
+      return RISM3D_CUDA_ERROR;
+    if (!std::isfinite(d[kDepth])) { c.err = "adjoint solve diverged"; return RISM3D_DIVERGED; }
+    if (bnorm < 0) bnorm = sqrt(d[kDepth]);            // xi = 0: r = (G - 1) w
+    if (sqrt(d[kDepth]) <= tol * bnorm) break;
+    for (int i = 0; i < kDepth; ++i)
+      gram[(size_t)slot * kDepth + i] = gram[(size_t)i * kDepth + slot] = d[i];
+    gram[(size_t)slot * kDepth + slot] = d[kDepth];
+    ns = nd;
+    anderson_coefficients(gram, ns, coef);
+    Mix mx{};
+    mx.ns = ns;
+    mx.eta = eta;
+    for (int a = 0; a < ns; ++a) {
+      mx.xs[a] = xs + (size_t)a * tot;
+      mx.rs[a] = rs + (size_t)a * tot;
+      mx.c[a] = coef[a];
+    }
+    k_combine<<<gt, kThreads, 0, c.stream>>>(tot, mx, xi);
+    c.launches += 1;
+    slot = (slot + 1) % kDepth;
+  }
+  if (it == maxit) { c.err = "adjoint solve did not converge"; return RISM3D_NOT_CONVERGED; }
+  // weights from zeta; L xi is current (the loop leaves right after applyL)
+  double *W = xs;                               // history no longer needed
   SiteW sv{};
   for (int v = 0; v < V; ++v) {
-    sv.sig[v] = c.sigv[v]; sv.eps[v] = c.epsv[v]; sv.q[v] = c.qv[v]; sv.rho[v] = c.rho[v];
+    sv.sig[v] = c.sigv[v]; sv.eps[v] = c.epsv[v]; sv.q[v] = c.qv[v] * c.cf_final; sv.rho[v] = c.rho[v];
   }
-  const double cc = kHartree * kBohr * kAvogadro;      // N_A kB T * ubeta
-  k_adjoint<V><<<dim3(tiles, nchunk), kAtomsPerBlock, 0, c.stream>>>(
-      c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, A, sv, cc, chunk, part);
-  double *sum = part + (size_t)nchunk * A * NOUT;
-  k_adjoint_sum<<<(A * NOUT + 255) / 256, 256, 0, c.stream>>>(part, nchunk, A, sum);
-  c.launches += 2;
-  std::vector<double> h((size_t)A * NOUT);
-  bool ok = cuda_ok(c, cudaGetLastError(), "adjoint") &&
-            cuda_ok(c, cudaMemcpyAsync(h.data(), sum, sizeof(double) * h.size(),
-                                       cudaMemcpyDeviceToHost, c.stream), "adjoint") &&
-            cuda_ok(c, cudaFreeAsync(part, c.stream), "adjoint") &&
-            cuda_ok(c, cudaStreamSynchronize(c.stream), "adjoint");
-  if (!ok) return RISM3D_CUDA_ERROR;
-  // charges enter the closure as q cf; gradients are for the final stage
+  k_weights<<<gb, kThreads, 0, c.stream>>>(n, V, c.d_g, c.d_h, G, xi, Lxi, w, sv, W, Om);
+  c.launches += 1;
+  const double cc = kHartree * kBohr * kAvogadro;      // N_A kB T x ubeta
+  // real-space part: atoms in tiles of 128, grid points split in chunks
+  const int tiles = (A + kAtomsPerBlock - 1) / kAtomsPerBlock;
+  const int want = std::max(1, 148 * 8 / tiles);
+  long long chunk = (n + want - 1) / want;
+  chunk = ((chunk + kPtsTile - 1) / kPtsTile) * kPtsTile;
+  const int nchunk = (int)((n + chunk - 1) / chunk);
+  long long chunk_k = (n / 2 + want - 1) / want;
+  chunk_k = ((chunk_k + kPtsTile - 1) / kPtsTile) * kPtsTile;
+  const int nchunk_k = (int)((n / 2 + chunk_k - 1) / chunk_k);
+  double *part_r = S.get<double>((size_t)(nchunk + 1) * A * NOUT);
+  double *part_k = S.get<double>((size_t)(nchunk_k + 1) * A * 4);
+  double2 *ph = S.get<double2>((size_t)A * (c.nx + c.ny + c.nz));
+  double2 *omh = S.get<double2>(n / 2);
+  if (!part_r || !part_k || !ph || !omh) { c.err = "adjoint: out of device memory"; return RISM3D_CUDA_ERROR; }
+  k_adjoint_r<V><<<dim3(tiles, nchunk), kAtomsPerBlock, 0, c.stream>>>(
+      c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], W, Om, c.d_atoms, A, sv, cc, chunk, part_r);
+  double *sum_r = part_r + (size_t)nchunk * A * NOUT;
+  k_sum_chunks<<<(A * NOUT + 255) / 256, 256, 0, c.stream>>>(part_r, nchunk, A, NOUT, sum_r);
+  // k-space part: Omega^ = F[Omega]; -cc/2 (1/V) sum over all k = -cc/V Re over the owner half
+  k_pack<<<gb, kThreads, 0, c.stream>>>(n, 1, c.nx, c.ny, c.d_tw, Om, buf);
+  if (fft(CUFFT_FORWARD) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
+  k_forward_post<<<gb, kThreads, 0, c.stream>>>(n, c.nx, c.ny, c.dv, buf, omh);
+  const long long L3 = (long long)A * (c.nx + c.ny + c.nz);
+  k_phase_rows_adj<<<(unsigned)((L3 + 255) / 256), 256, 0, c.stream>>>(
+      c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], c.d_atoms, A, ph);
+  k_adjoint_k<<<dim3(tiles, nchunk_k), kAtomsPerBlock, 0, c.stream>>>(
+      c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], omh, ph, c.d_atoms, A,
+      -cc / c.vol, chunk_k, part_k);
+  double *sum_k = part_k + (size_t)nchunk_k * A * 4;
+  k_sum_chunks<<<(A * 4 + 255) / 256, 256, 0, c.stream>>>(part_k, nchunk_k, A, 4, sum_k);
+  c.launches += 7;
+  std::vector<double> hr((size_t)A * NOUT), hk((size_t)A * 4);
+  if (!cuda_ok(c, cudaGetLastError(), "adjoint") ||
+      !cuda_ok(c, cudaMemcpyAsync(hr.data(), sum_r, sizeof(double) * hr.size(), cudaMemcpyDeviceToHost, c.stream), "adjoint") ||
+      !cuda_ok(c, cudaMemcpyAsync(hk.data(), sum_k, sizeof(double) * hk.size(), cudaMemcpyDeviceToHost, c.stream), "adjoint") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "adjoint"))
+    return RISM3D_CUDA_ERROR;
+  // the charge-up factor of the last stage is already in the site charges
   for (int u = 0; u < A; ++u) {
-    const double *o = &h[(size_t)u * NOUT];
-    if (dq) dq[u] = o[0] * c.dv * c.cf_final;
+    const double *o = &hr[(size_t)u * NOUT], *kk = &hk[(size_t)u * 4];
+    if (dq) dq[u] = o[0] * c.dv + kk[0];
     if (dsig) dsig[u] = o[1] * c.dv;
     if (deps) deps[u] = o[2] * c.dv;
     if (dR)
-      for (int k = 0; k < 3; ++k) dR[3 * u + k] = o[3 + k] * c.dv;
+      for (int k = 0; k < 3; ++k) dR[3 * u + k] = o[3 + k] * c.dv + kk[1 + k];
   }
   return RISM3D_OK;
 }
@@ -167,6 +652,7 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
 }  // namespace
 
 int compute_adjoint(Context &c, double *dq, double *dsig, double *deps, double *dR) {
+  if (c.nb != 1) { c.err = "gradients are for single-solute contexts"; return RISM3D_BAD_STATE; }
   switch (c.natv) {
     case 1: return adjoint_v<1>(c, dq, dsig, deps, dR);
     case 2: return adjoint_v<2>(c, dq, dsig, deps, dR);

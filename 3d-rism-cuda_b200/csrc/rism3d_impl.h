@@ -194,6 +194,8 @@ int compute_observables(Context &c);              // observe.cu
 int compute_atom_integrals(Context &c, bool forces);  // observe.cu
 int compute_adjoint(Context &c, double *dq, double *dsig, double *deps,
                     double *dR);                  // adjoint.cu
+// FP64 OZ k-space pass on a packed buffer (adjoint solve)
+int launch_oz_kspace(Context &c, double2 *buf, const StageParams *sp, DevState *st);
 int fetch_grid(Context &c, int which, double *host);
 int time_kernel(Context &c, int which, int reps, double *ms);   // solver.cu
 void free_device(Context &c);

@@ -1136,6 +1136,32 @@ int time_kernel(Context &c, int which, int reps, double *ms) {
   return RISM3D_UNSUPPORTED_SHAPE;
 }
 
+// The FP64 k-space pass alone on a caller-packed buffer (one solute): the
+// OZ product h(k) = chi(k) (c(k) - q cf fk) between the two transforms, used
+// by the adjoint solve to apply the same discrete operator as the iteration.
+template <int V>
+int oz_kspace_v(Context &c, double2 *buf, const StageParams *sp, DevState *st) {
+  IterArgs<double> a = make_args<double>(c, true);
+  a.buf = buf; a.sp = sp; a.st = st;
+  k_kspace<double, V><<<dim3(grid_blocks(c.n / 2), 1), kThreads, 0, c.stream>>>(a);
+  c.launches += 1;
+  return cuda_ok(c, cudaGetLastError(), "oz k-space") ? RISM3D_OK : RISM3D_CUDA_ERROR;
+}
+
+int launch_oz_kspace(Context &c, double2 *buf, const StageParams *sp, DevState *st) {
+  switch (c.natv) {
+    case 1: return oz_kspace_v<1>(c, buf, sp, st);
+    case 2: return oz_kspace_v<2>(c, buf, sp, st);
+    case 3: return oz_kspace_v<3>(c, buf, sp, st);
+    case 4: return oz_kspace_v<4>(c, buf, sp, st);
+    case 5: return oz_kspace_v<5>(c, buf, sp, st);
+    case 6: return oz_kspace_v<6>(c, buf, sp, st);
+    case 7: return oz_kspace_v<7>(c, buf, sp, st);
+    case 8: return oz_kspace_v<8>(c, buf, sp, st);
+  }
+  return RISM3D_UNSUPPORTED_SHAPE;
+}
+
 int run_solve(Context &c, int chargeup) {
   switch (c.natv) {
     case 1: return solve_c<1>(c, chargeup);

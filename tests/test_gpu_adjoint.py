@@ -81,13 +81,16 @@ def test_lj_parameter_gradients_match_central_differences(tight):
 
 def test_position_gradient_agrees_with_cal_grad_forces(tight):
     """cal_grad (cal_grad.cu:51-145) integrates rho g grad_R u outside
-    r < sigma/2; the adjoint has no cutoff, and g is ~0 inside it."""
+    r < sigma/2.  That is the derivative of mu_ex only when the analytic
+    long-range transform fk equals the discrete transform of fr; the exact
+    gradient adds the mismatch term (about 0.5% here, and the finite-difference
+    tests above show it belongs to the derivative), so the two agree to 1%."""
     case, s, (_, _, _, dR) = tight
     s.set_solute(case.sig, case.eps, case.q, case.xyz)
     s.solve()
     dulj, due = s.forces()
     tot = dulj + due
-    assert np.abs(tot - dR).max() <= 1e-3 * np.abs(dR).max()
+    assert np.abs(tot - dR).max() <= 1e-2 * np.abs(dR).max()
 
 
 def test_autograd_function_routes_backward_through_the_adjoint(tight):
