@@ -3,6 +3,7 @@
 // points.  No compute happens on the host: every grid operation is a CUDA
 // kernel or cuFFT, and a missing or failing device is an error, never a
 // fallback.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -59,16 +60,17 @@ bool cufft_ok(Context &c, cufftResult r, const char *what) {
 void free_device(Context &c) {
   void *ptrs[] = {c.d_u, c.d_e, c.d_fr, c.d_fkh, c.d_atoms, c.d_tw, c.d_twf,
                   c.d_U, c.d_t, c.d_Y, c.d_RP, c.d_buf, c.d_h, c.d_g,
-                  c.f_U, c.f_t, c.f_Y, c.f_RP, c.f_buf, c.d_part, c.d_state,
-                  c.d_stage, c.d_obs, c.d_atom_part, c.chi.d_coef, c.d_xs,
+                  c.f_U, c.f_t, c.f_Y, c.f_RP, c.f_buf, c.f_R0, c.f_x0, c.d_part, c.d_state,
+                  c.d_stage, c.d_stage_ref, c.d_obs, c.d_atom_part, c.chi.d_coef, c.d_xs,
                   c.d_atom_off, c.d_atom_cnt};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   c.d_u = c.d_e = c.d_fr = nullptr; c.d_fkh = nullptr; c.d_atoms = nullptr;
   c.d_tw = nullptr; c.d_twf = nullptr; c.d_U = c.d_t = c.d_Y = c.d_RP = nullptr;
   c.d_buf = nullptr; c.d_h = c.d_g = nullptr;
-  c.f_U = c.f_t = c.f_Y = c.f_RP = nullptr; c.f_buf = nullptr;
-  c.d_part = nullptr; c.d_state = nullptr; c.d_stage = nullptr; c.d_obs = nullptr;
+  c.f_U = c.f_t = c.f_Y = c.f_RP = nullptr; c.f_buf = nullptr; c.f_R0 = c.f_x0 = nullptr;
+  c.d_part = nullptr; c.d_state = nullptr; c.d_stage = nullptr; c.d_stage_ref = nullptr;
+  c.d_obs = nullptr;
   c.d_atom_part = nullptr; c.chi.d_coef = nullptr; c.natom_part_cap = 0;
   c.d_xs = nullptr; c.nxs = 0;
   c.d_atom_off = c.d_atom_cnt = nullptr;
@@ -76,7 +78,15 @@ void free_device(Context &c) {
   c.h_state = nullptr;
   if (c.graph64) cudaGraphExecDestroy(c.graph64);
   if (c.graph32) cudaGraphExecDestroy(c.graph32);
-  c.graph64 = c.graph32 = nullptr;
+  if (c.graph32r) cudaGraphExecDestroy(c.graph32r);
+  c.graph64 = c.graph32 = c.graph32r = nullptr;
+  for (cudaGraphExec_t *g : {&c.loop64, &c.loop32, &c.loop32r}) {
+    if (*g) cudaGraphExecDestroy(*g);
+    *g = nullptr;
+  }
+  if (c.d_hist) cudaFree(c.d_hist);
+  c.d_hist = nullptr;
+  c.hist_cap = 0;
   if (c.d_count) cudaFree(c.d_count);
   c.d_count = nullptr;
   if (c.plan64) cufftDestroy(c.plan64);
@@ -156,7 +166,9 @@ static int alloc_state(Context &c) {
          A((void **)&c.f_t, sizeof(float) * V * n, "alloc t32") &&
          A((void **)&c.f_Y, sizeof(float) * 2 * V * n, "alloc Y32") &&
          A((void **)&c.f_RP, sizeof(float) * 2 * V * n, "alloc RP32") &&
-         A((void **)&c.f_buf, sizeof(float2) * P * n, "alloc buf32");
+         A((void **)&c.f_buf, sizeof(float2) * P * n, "alloc buf32") &&
+         A((void **)&c.f_R0, sizeof(float) * V * n, "alloc R0 32") &&
+         A((void **)&c.f_x0, sizeof(float) * V * n, "alloc x0 32");
   if (!ok) return RISM3D_CUDA_ERROR;
   // batched 3D plans over the site pairs; x is the fastest axis
   // one batched plan over all site pairs of all solutes
@@ -234,7 +246,12 @@ int context_init(Context &c, const rism3d_params *p, int nb, std::string &err) {
             cuda_ok(c, cudaMalloc(&c.d_twf, sizeof(float2) * (c.nx + c.ny + c.nz)), "alloc tw") &&
             cuda_ok(c, cudaMalloc(&c.d_state, sizeof(DevState) * nb), "alloc state") &&
             cuda_ok(c, cudaMalloc(&c.d_stage, sizeof(StageParams)), "alloc stage") &&
+            cuda_ok(c, cudaMalloc(&c.d_stage_ref, sizeof(StageParams)), "alloc stage") &&
+            (!(p->verbose && nb == 1) ||
+             cuda_ok(c, cudaMalloc(&c.d_hist, sizeof(double) * ((size_t)std::max(p->maxstep, 1) + 8)),
+                     "alloc history")) &&
             cuda_ok(c, cudaHostAlloc(&c.h_state, sizeof(DevState) * 4 * nb, cudaHostAllocDefault), "alloc pinned");
+  if (c.d_hist) c.hist_cap = std::max(p->maxstep, 1) + 8;
   long long nbk = (c.n + 255) / 256;
   c.nred_blocks = (int)(nbk < 148 * 8 ? nbk : 148 * 8);
   ok = ok && cuda_ok(c, cudaMalloc(&c.d_part, sizeof(double) * 64 * c.nred_blocks * nb), "alloc partials") &&

@@ -25,7 +25,8 @@ constexpr double kPi = 3.14159265358979323846;
 // no host round trip.  Mirrors the host-side state of AN2
 // (anderson.h:16-37) and RISM3D::iterate (iterate.cu:49-73).
 struct DevState {
-  int done;        // 0 running, 1 converged, 2 diverged, 3 maxstep reached
+  int done;        // 0 running, 1 converged, 2 diverged, 3 maxstep reached,
+                   // 4 stalled (no 10% rms gain in 30 steps while watched)
   int after_done;  // finalize calls since `done` was set
   int iter;        // iterations completed in this run
   int mode;        // update the next pass A applies: 0 none, 1 Picard, 2 AN2
@@ -34,6 +35,10 @@ struct DevState {
   int count;       // Picard warm-up steps left
   int maxstep;
   int measure;     // 1: the finalize only records the sums (kernel timing)
+  int watch;       // 1: stop as stalled (done = 4) when progress stops
+  int since;       // steps since the best rms last improved by 10 %
+  int loops;       // device-side loop: bodies run in this launch (solute 0)
+  double best;     // best rms of this run (stagnation watch)
   double conv;
   double m, mp;    // AN2 mixing factor and bias
   double s1, s2;   // AN2 coefficients for the next update
@@ -137,12 +142,15 @@ struct Context {
   // FP32 iteration state (MIXED)
   float *f_U = nullptr, *f_t = nullptr, *f_Y = nullptr, *f_RP = nullptr;
   float2 *f_buf = nullptr;
+  // FP32 refinement: base residual R0 and closure argument x0 = t0 - U_SR
+  float *f_R0 = nullptr, *f_x0 = nullptr;
 
   double *d_part = nullptr;  // reduction partials
   int nred_blocks = 0;
   DevState *d_state = nullptr;
   DevState *h_state = nullptr;  // pinned mirror
   StageParams *d_stage = nullptr;
+  StageParams *d_stage_ref = nullptr;  // refinement passes: qcf = 0
   double *d_obs = nullptr;      // observables scratch
   double *d_atom_part = nullptr;
   int natom_part_cap = 0;
@@ -150,7 +158,13 @@ struct Context {
   cufftHandle plan64 = 0, plan32 = 0;
   bool plans_ok = false;
   // one captured iteration per precision, reused by every solve
-  cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
+  cudaGraphExec_t graph64 = nullptr, graph32 = nullptr, graph32r = nullptr;
+  // the same iterations inside a device-side while loop (conditional graph
+  // node): one launch runs a whole phase; null when the driver refuses it
+  cudaGraphExec_t loop64 = nullptr, loop32 = nullptr, loop32r = nullptr;
+  bool no_device_loop = false;
+  double *d_hist = nullptr;     // per-iteration rms (verbose single solves)
+  int hist_cap = 0;
   unsigned *d_count = nullptr;  // pass-R block counter (last block finalizes)
 
   // restart guess

@@ -25,6 +25,17 @@
 // The AN2 history stores Y_i = tp_i + m rp_i and RP_i = rp_i: the reference
 // update u + m(v - u) (anderson_cuda.cu:16-22) is algebraically
 // y + s1 (Y_0 - y) + s2 (Y_1 - y) with y = t + m R.
+//
+// Mixed precision iterates in FP32 in two forms.  The plain form carries t
+// itself; its rounding floor (eps32 times the size of g and h near the
+// solute, ~1e-5 in rms) ends it.  The refinement form (REF) carries the
+// correction d = t - t0 to a fixed FP64 base t0 whose residual R0 = R(t0)
+// was computed once in FP64.  Because the OZ operator L is linear,
+//   R(t0 + d) = R0 + L[dc] - dg,   dg = C(x0 + d) - C(x0),  dc = dg - d,
+// with x0 = t0 - U_SR, and the long-range fk term cancels.  Every FP32
+// quantity is then of the size of the correction, so the residual is exact
+// to eps32 |d| and AN2 (which is affine, so it acts on d unchanged)
+// converges to the FP64 tolerance in FP32 passes.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -50,6 +61,7 @@ struct IterArgs {
   const double *xs;         // chi table per odd-square sum (cubic cells) or null
   typename Cx<T>::t *buf;   // [P][N]
   T *t, *U, *Y, *RP;        // t, U: [V][N]; Y, RP: [2][V][N]
+  const T *R0;              // refinement: base residual [V][N] (t = d, U = x0)
   double *hout, *gout;      // final snapshot, [V][N] (may be null)
   const typename Cx<T>::t *tw;  // px[nx] py[ny] pz[nz]
   double invvol, dv;
@@ -63,6 +75,8 @@ struct IterArgs {
   double *part;
   int nblocks;
   unsigned *count;          // blocks of pass R done (reset by the last one)
+  double *hist;             // per-iteration rms (single solves, verbose) or null
+  int hist_cap;
 };
 
 // Batched solves: blockIdx.y selects the solute; every per-solute array is
@@ -80,6 +94,7 @@ __device__ __forceinline__ IterArgs<T> solute_view(const IterArgs<T> &a) {
   s.Y = a.Y + b * 2 * V * n;
   s.RP = a.RP + b * 2 * V * n;
   if (a.hout) { s.hout = a.hout + b * V * n; s.gout = a.gout + b * V * n; }
+  if (a.R0) s.R0 = a.R0 + b * V * n;
   s.fkh = a.fkh + b * (n / 2);
   s.st = a.st + b;
   s.part = a.part + b * 6 * (size_t)a.nblocks;
@@ -160,6 +175,36 @@ __device__ __forceinline__ T closure(T x) {
   return fexp(x);
 }
 
+__device__ __forceinline__ double fexpm1(double x) { return expm1(x); }
+__device__ __forceinline__ float fexpm1(float x) { return expm1f(x); }
+
+// C(x0 + d) - C(x0) to the relative precision of the difference itself
+// (refinement form): e^x0 expm1(d) on the exponential branch, d on the
+// linear KH branch, and the two mixed cases where x0 and x0 + d straddle 0
+// (there |x0| <= |d|, so nothing large cancels).
+template <int CLOS, typename T>
+__device__ __forceinline__ T closure_diff(T x0, T d) {
+  if (CLOS == 1) return fexp(x0) * fexpm1(d);
+  const T x = x0 + d;
+  if (x0 < T(0)) return x < T(0) ? fexp(x0) * fexpm1(d) : x - fexpm1(x0);
+  return x >= T(0) ? d : fexpm1(x) - x0;
+}
+
+// Residual of the cycle at the current state: plain h + 1 - C(t - U);
+// refinement R0 + h - [C(x0 + d) - C(x0)] (t = d, U = x0, h = L[dc]).
+template <int CLOS, bool REF, typename T>
+__device__ __forceinline__ T residual(T h, T t, T U, T r0) {
+  if (REF) return r0 + h - closure_diff<CLOS>(U, t);
+  return h + T(1) - closure<CLOS>(t - U);
+}
+
+// Packed FFT input: plain c_SR = C(t - U) - 1 - t; refinement dc = dg - d.
+template <int CLOS, bool REF, typename T>
+__device__ __forceinline__ T cfun(T t, T U) {
+  if (REF) return closure_diff<CLOS>(U, t) - t;
+  return closure<CLOS>(t - U) - T(1) - t;
+}
+
 // Point index -> (ix, iy, iz), +-1 checkerboard dir = (-1)^(ix+iy+iz)
 // (set_ir, fft3d.cu:86-94) and dkf = exp(-i pi sum x_d/n_d)
 // (set_kf, fft3d.cu:71-83) as a product of three per-axis phases.
@@ -189,7 +234,7 @@ __device__ __forceinline__ void point_phase(long long j, const FastDiv &fdx,
 // once per thread): every load of a point is issued before any store.  Each
 // thread handles PTS adjacent points (2 for FP32, so each thread keeps as
 // many bytes in flight as the FP64 version).
-template <typename T, int V, int CLOS, int MODE, int PTS>
+template <typename T, int V, int CLOS, int MODE, int PTS, bool REF>
 __device__ __forceinline__ void pass_a_body(const IterArgs<T> &a, int slot, T s1, T s2, T m) {
   typedef typename Cx<T>::t C;
   constexpr int P = (V + 1) / 2;
@@ -203,7 +248,7 @@ __device__ __forceinline__ void pass_a_body(const IterArgs<T> &a, int slot, T s1
   for (long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * PTS; j < n;
        j += (long long)gridDim.x * blockDim.x * PTS) {
     C zb[P][PTS];
-    T tv[V][PTS], Uv[V][PTS], y0[V][PTS], y1[V][PTS];
+    T tv[V][PTS], Uv[V][PTS], y0[V][PTS], y1[V][PTS], r0[V][PTS];
     if (MODE != 0) {
 #pragma unroll
       for (int p = 0; p < P; ++p) ldc<PTS>(buf + (size_t)p * n + j, zb[p]);
@@ -212,6 +257,11 @@ __device__ __forceinline__ void pass_a_body(const IterArgs<T> &a, int slot, T s1
     for (int v = 0; v < V; ++v) {
       ldr<PTS>(tt + (size_t)v * n + j, tv[v]);
       ldr<PTS>(UU + (size_t)v * n + j, Uv[v]);
+      if (REF && MODE != 0) ldr<PTS>(a.R0 + (size_t)v * n + j, r0[v]);
+      else {
+#pragma unroll
+        for (int k = 0; k < PTS; ++k) r0[v][k] = T(0);
+      }
       if (MODE == 2) {
         ldr<PTS>(Y + (size_t)v * n + j, y0[v]);
         ldr<PTS>(Y + (size_t)(V + v) * n + j, y1[v]);
@@ -239,7 +289,7 @@ __device__ __forceinline__ void pass_a_body(const IterArgs<T> &a, int slot, T s1
         }
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-          const T R = h[v] + T(1) - closure<CLOS>(tv[v][k] - Uv[v][k]);   // tr
+          const T R = residual<CLOS, REF>(h[v], tv[v][k], Uv[v][k], r0[v][k]);   // tr
           rw[v][k] = R;
           if (MODE == 1) {                       // newdt0 (Picard)
             yw[v][k] = tv[v][k] + m * R;
@@ -274,10 +324,8 @@ __device__ __forceinline__ void pass_a_body(const IterArgs<T> &a, int slot, T s1
         const int dir = (k & 1) ? -dir0 : dir0;
         const C wf = mk<C>(dkf[k].x * dir, dkf[k].y * dir);
         C z;
-        z.x = closure<CLOS>(tn[2 * p][k] - Uv[2 * p][k]) - T(1) - tn[2 * p][k];
-        z.y = (2 * p + 1 < V)
-                  ? closure<CLOS>(tn[2 * p + 1][k] - Uv[2 * p + 1][k]) - T(1) - tn[2 * p + 1][k]
-                  : T(0);
+        z.x = cfun<CLOS, REF>(tn[2 * p][k], Uv[2 * p][k]);
+        z.y = (2 * p + 1 < V) ? cfun<CLOS, REF>(tn[2 * p + 1][k], Uv[2 * p + 1][k]) : T(0);
         out[k] = cmul(z, wf);
       }
       stc<PTS>(buf + (size_t)p * n + j, out);
@@ -289,7 +337,7 @@ __device__ __forceinline__ void pass_a_body(const IterArgs<T> &a, int slot, T s1
 // (closure of the t used in that cycle), and when maxstep ended the loop
 // apply the pending update as the reference does (iterate.cu:61 runs
 // ma->calculate before the step bound is tested).
-template <typename T, int V, int CLOS>
+template <typename T, int V, int CLOS, bool REF>
 __device__ void pass_a_final(const IterArgs<T> &a, int mode, int done, int slot, T s1,
                              T s2, T m) {
   typedef typename Cx<T>::t C;
@@ -313,10 +361,12 @@ __device__ void pass_a_final(const IterArgs<T> &a, int mode, int done, int slot,
     for (int v = 0; v < V; ++v) {
       const size_t iv = (size_t)v * n + j;
       const T t = a.t[iv];
-      const T gold = closure<CLOS>(t - a.U[iv]);
-      if (a.hout) { a.hout[iv] = (double)h[v]; a.gout[iv] = (double)gold; }
+      if (!REF && a.hout) {
+        a.hout[iv] = (double)h[v];
+        a.gout[iv] = (double)closure<CLOS>(t - a.U[iv]);
+      }
       if (done == 3 && mode != 0) {
-        const T R = h[v] + T(1) - gold;
+        const T R = residual<CLOS, REF>(h[v], t, a.U[iv], REF ? a.R0[iv] : T(0));
         const T y = t + m * R;
         T tn = t + R;
         if (mode == 2) tn = y + s1 * (a.Y[iv] - y) + s2 * (a.Y[(size_t)V * n + iv] - y);
@@ -328,7 +378,7 @@ __device__ void pass_a_final(const IterArgs<T> &a, int mode, int done, int slot,
   }
 }
 
-template <typename T, int V, int CLOS>
+template <typename T, int V, int CLOS, bool REF>
 __global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a0) {
   const IterArgs<T> a = solute_view<T, V>(a0);
   const DevState *st = a.st;
@@ -337,13 +387,13 @@ __global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a0) {
   const int slot = st->upd_slot;
   const T s1 = (T)st->s1, s2 = (T)st->s2, m = (T)st->m;
   if (done) {
-    if (st->after_done == 0) pass_a_final<T, V, CLOS>(a, mode, done, slot, s1, s2, m);
+    if (st->after_done == 0) pass_a_final<T, V, CLOS, REF>(a, mode, done, slot, s1, s2, m);
     return;                                     // past the snapshot: idle
   }
   constexpr int PTS = sizeof(T) == 4 ? 2 : 1;
-  if (mode == 2) pass_a_body<T, V, CLOS, 2, PTS>(a, slot, s1, s2, m);
-  else if (mode == 1) pass_a_body<T, V, CLOS, 1, PTS>(a, slot, s1, s2, m);
-  else pass_a_body<T, V, CLOS, 0, PTS>(a, slot, s1, s2, m);
+  if (mode == 2) pass_a_body<T, V, CLOS, 2, PTS, REF>(a, slot, s1, s2, m);
+  else if (mode == 1) pass_a_body<T, V, CLOS, 1, PTS, REF>(a, slot, s1, s2, m);
+  else pass_a_body<T, V, CLOS, 0, PTS, REF>(a, slot, s1, s2, m);
 }
 
 // ---------------------------------------------------------------- pass K
@@ -440,9 +490,9 @@ __global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a0) {
 
 // ---------------------------------------------------------------- pass R
 __device__ void finalize_block(DevState *st, const double *part, int nblocks,
-                               double nv_points);
+                               double nv_points, double *hist, int hist_cap);
 
-template <typename T, int V, int CLOS>
+template <typename T, int V, int CLOS, bool REF>
 __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a0) {
   const IterArgs<T> a = solute_view<T, V>(a0);
   typedef typename Cx<T>::t C;
@@ -470,13 +520,18 @@ __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a0) {
   for (long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * PTS; j < n;
        j += (long long)gridDim.x * blockDim.x * PTS) {
     C zb[P][PTS];
-    T tv[V][PTS], Uv[V][PTS], r0[V][PTS], r1[V][PTS];
+    T tv[V][PTS], Uv[V][PTS], r0[V][PTS], r1[V][PTS], rb[V][PTS];
 #pragma unroll
     for (int p = 0; p < P; ++p) ldc<PTS>(buf + (size_t)p * n + j, zb[p]);
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       ldr<PTS>(tt + (size_t)v * n + j, tv[v]);
       ldr<PTS>(UU + (size_t)v * n + j, Uv[v]);
+      if (REF) ldr<PTS>(a.R0 + (size_t)v * n + j, rb[v]);
+      else {
+#pragma unroll
+        for (int k = 0; k < PTS; ++k) rb[v][k] = T(0);
+      }
       if (gram) {
         ldr<PTS>(RP + (size_t)v * n + j, r0[v]);
         ldr<PTS>(RP + (size_t)(V + v) * n + j, r1[v]);
@@ -500,8 +555,7 @@ __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a0) {
       }
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const T g = closure<CLOS>(tv[v][k] - Uv[v][k]);
-        const double R = (double)(h[v] + T(1) - g);
+        const double R = (double)residual<CLOS, REF>(h[v], tv[v][k], Uv[v][k], rb[v][k]);
         acc[0] += R * R;                          // cal_rms.cu:18
         if (gram) {                               // theta30, anderson_cuda.cu:33-39
           const double d0 = R - (double)r0[v][k];
@@ -537,7 +591,7 @@ __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a0) {
   __syncthreads();
   if (!last) return;
   __threadfence();
-  finalize_block(st, a.part, a.nblocks, (double)n * V);
+  finalize_block(st, a.part, a.nblocks, (double)n * V, a.hist, a.hist_cap);
   if (threadIdx.x == 0) *a.count = 0u;
 }
 
@@ -546,7 +600,7 @@ __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a0) {
 // block sums, then the host logic of iterate.cu:52-62 and AN2::calculate
 // (anderson.cu:35-63) on one thread -- no separate launch, no host sync.
 __device__ void finalize_block(DevState *st, const double *part, int nblocks,
-                               double nv_points) {
+                               double nv_points, double *hist, int hist_cap) {
   __shared__ double red[6][kThreads];
   double s[6] = {0, 0, 0, 0, 0, 0};
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
@@ -567,8 +621,13 @@ __device__ void finalize_block(DevState *st, const double *part, int nblocks,
   st->rms = rms;
   if (st->measure) return;
   st->iter += 1;
+  if (hist && st->iter <= hist_cap) hist[st->iter - 1] = rms;  // iterate.cu:63 output
   if (!isfinite(rms)) { st->done = 2; st->mode = 0; return; }  // iterate.cu:54-57
   if (rms <= st->conv) { st->done = 1; st->mode = 0; return; } // :58-59
+  if (st->watch) {                       // a phase that may hand over early
+    if (rms < 0.9 * st->best) { st->best = rms; st->since = 0; }
+    else if (++st->since > 30) { st->done = 4; st->mode = 0; return; }
+  }
   if (st->count > 0) {                                         // anderson.cu:43-49
     st->count -= 1;
     st->mode = 1;
@@ -638,6 +697,62 @@ __global__ void k_shift_history(long long n, int nv, long long total, const doub
   }
 }
 
+// Refinement base, after one FP64 cycle at t0 (buf holds its inverse
+// transform): R0 = h + 1 - C(t0 - U), x0 = t0 - U, d = 0, and the FP32 AN2
+// history re-expressed as corrections to t0 (Y_i - t0; RP_i unchanged).
+template <int V, int CLOS>
+__global__ void __launch_bounds__(kThreads)
+k_refine_base(IterArgs<double> a0, float *R0, float *x0, float *d, float *Yf) {
+  const IterArgs<double> a = solute_view<double, V>(a0);
+  constexpr int P = (V + 1) / 2;
+  const long long n = a.n;
+  const size_t b = blockIdx.y;
+  R0 += b * V * n; x0 += b * V * n; d += b * V * n; Yf += b * 2 * V * n;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    int ix, iy, iz, dir;
+    double2 dkf;
+    point_phase(j, a.fdx, a.fdy, a.tw, ix, iy, iz, dir, dkf);
+    const double sc = a.invvol * dir;
+    const double2 w = make_double2(dkf.x * sc, -dkf.y * sc);
+    double h[V];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const double2 z = cmul(a.buf[(size_t)p * n + j], w);
+      h[2 * p] = z.x;
+      if (2 * p + 1 < V) h[2 * p + 1] = z.y;
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const size_t iv = (size_t)v * n + j;
+      const double t0 = a.t[iv], x = t0 - a.U[iv];
+      R0[iv] = (float)(h[v] + 1.0 - closure<CLOS>(x));
+      x0[iv] = (float)x;
+      d[iv] = 0.0f;
+      Yf[iv] = (float)((double)Yf[iv] - t0);
+      Yf[(size_t)V * n + iv] = (float)((double)Yf[(size_t)V * n + iv] - t0);
+    }
+  }
+}
+
+// Refinement end: t = t0 + d and the AN2 history back to absolute FP64
+// values; arrays [B][V][N] (t, d) and [B][2][V][N] (history).
+__global__ void k_refine_finish(long long n, int nv, long long total, const float *d,
+                                const float *Yf, const float *RPf, double *t, double *Y,
+                                double *RP) {
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < total;
+       f += (long long)gridDim.x * blockDim.x) {
+    const long long b = f / (nv * n), r = f - b * nv * n;
+    const size_t h0 = (size_t)b * 2 * nv * n + r, h1 = h0 + (size_t)nv * n;
+    const double t0 = t[f];
+    Y[h0] = (double)Yf[h0] + t0;
+    Y[h1] = (double)Yf[h1] + t0;
+    RP[h0] = (double)RPf[h0];
+    RP[h1] = (double)RPf[h1];
+    t[f] = t0 + (double)d[f];
+  }
+}
+
 template <typename A, typename B>
 __global__ void k_convert(long long n, const A *src, B *dst) {
   for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
@@ -651,10 +766,10 @@ int grid_blocks(long long work) {
   return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
 
-template <typename T, int V, int CLOS>
+template <typename T, int V, int CLOS, bool REF>
 void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   const dim3 ba(grid_blocks(a.n), c.nb), bk(grid_blocks(a.n / 2), c.nb), br(a.nblocks, c.nb);
-  k_pass_a<T, V, CLOS><<<ba, kThreads, 0, c.stream>>>(a);
+  k_pass_a<T, V, CLOS, REF><<<ba, kThreads, 0, c.stream>>>(a);
   typedef typename Cx<T>::t C;
   if (sizeof(T) == 8) {
     cufftExecZ2Z(plan, (cufftDoubleComplex *)a.buf, (cufftDoubleComplex *)a.buf, CUFFT_FORWARD);
@@ -667,7 +782,7 @@ void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   } else {
     cufftExecC2C(plan, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
   }
-  k_pass_r<T, V, CLOS><<<br, kThreads, 0, c.stream>>>(a);
+  k_pass_r<T, V, CLOS, REF><<<br, kThreads, 0, c.stream>>>(a);
   (void)sizeof(C);
 }
 
@@ -682,6 +797,8 @@ IterArgs<T> make_args(Context &c, bool fp64) {
   a.bx = c.prm.box[0]; a.by = c.prm.box[1]; a.bz = c.prm.box[2];
   a.st = c.d_state; a.sp = c.d_stage; a.part = c.d_part; a.nblocks = c.nred_blocks;
   a.count = c.d_count;
+  a.hist = c.nb == 1 ? c.d_hist : nullptr;
+  a.hist_cap = c.hist_cap;
   (void)fp64;
   return a;
 }
@@ -689,7 +806,7 @@ IterArgs<T> make_args(Context &c, bool fp64) {
 // Capture one iteration (passes, cuFFT, and the fused finalize) as a CUDA
 // graph, once per context and precision; every later solve relaunches it.
 // If capture of the cuFFT calls is refused, the loop launches directly.
-template <typename T, int V, int CLOS>
+template <typename T, int V, int CLOS, bool REF>
 cudaGraphExec_t capture(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   cudaGraph_t g = nullptr;
   cudaGraphExec_t x = nullptr;
@@ -697,7 +814,7 @@ cudaGraphExec_t capture(Context &c, const IterArgs<T> &a, cufftHandle plan) {
     cudaGetLastError();
     return nullptr;
   }
-  launch_iteration<T, V, CLOS>(c, a, plan);
+  launch_iteration<T, V, CLOS, REF>(c, a, plan);
   cudaError_t e = cudaStreamEndCapture(c.stream, &g);
   if (e != cudaSuccess || !g) {
     cudaGetLastError();
@@ -712,16 +829,74 @@ cudaGraphExec_t capture(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   return x;
 }
 
-template <typename T, int V, int CLOS>
+// End of one device-side loop body: keep looping while any solute is still
+// running or has not yet had the idle pass after its stop (the snapshot);
+// the body count is bounded by the phase's step limit plus a margin.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, DevState *st, int nb) {
+  if (threadIdx.x != 0) return;
+  bool more = false;
+  for (int b = 0; b < nb; ++b)
+    if (!(st[b].done && st[b].after_done >= 1)) more = true;
+  const int loops = ++st[0].loops;
+  const int cap = st[0].maxstep < 1000000 ? st[0].maxstep : 1000000;
+  if (loops >= cap + 4) more = false;
+  cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+// One whole phase as a single graph: a while node whose body is one
+// iteration (passes, cuFFT, finalize) plus k_loop_cond.  Returns null when
+// the driver or cuFFT cannot be captured this way; the caller then drives
+// the iterations from the host.
+template <typename T, int V, int CLOS, bool REF>
+cudaGraphExec_t capture_loop(Context &c, const IterArgs<T> &a, cufftHandle plan) {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  cudaGraphConditionalHandle h;
+  bool ok = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+  // the parameter union has no default constructor: zeroed storage
+  alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)] = {};
+  cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(raw);
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  ok = ok && cudaGraphAddNode(&node, g, nullptr, 0, &np) == cudaSuccess;
+  if (ok) {
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    ok = cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      launch_iteration<T, V, CLOS, REF>(c, a, plan);
+      k_loop_cond<<<1, 32, 0, c.stream>>>(h, a.st, c.nb);
+      cudaGraph_t out = nullptr;
+      ok = cudaStreamEndCapture(c.stream, &out) == cudaSuccess;
+    }
+  }
+  if (ok) ok = cudaGraphInstantiate(&x, g, 0) == cudaSuccess;
+  cudaGraphDestroy(g);
+  if (!ok) {
+    cudaGetLastError();
+    if (x) cudaGraphExecDestroy(x);
+    return nullptr;
+  }
+  return x;
+}
+
+template <typename T, int V, int CLOS, bool REF>
 int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
                   typename Cx<T>::t *buf, bool snapshot, double conv,
-                  int max_iter, bool watch_stagnation, int &iters_out) {
+                  int max_iter, bool watch_stagnation, int &iters_out,
+                  const T *R0 = nullptr, bool restart_an2 = false) {
   IterArgs<T> a = make_args<T>(c, sizeof(T) == 8);
   a.buf = buf; a.t = t; a.U = U; a.Y = Y; a.RP = RP;
+  if (REF) { a.R0 = R0; a.sp = c.d_stage_ref; }
   a.hout = snapshot ? c.d_h : nullptr;
   a.gout = snapshot ? c.d_g : nullptr;
   a.tw = (const typename Cx<T>::t *)(sizeof(T) == 8 ? (void *)c.d_tw : (void *)c.d_twf);
-  // reset the per-run control words; AN2 count/binary persist
+  // reset the per-run control words; AN2 count/binary persist unless the
+  // history was discarded
   const int nb = c.nb;
   std::vector<DevState> hs(nb);
   if (!cuda_ok(c, cudaMemcpyAsync(hs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream), "state read") ||
@@ -730,64 +905,105 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
   for (DevState &h : hs) {
     h.done = 0; h.after_done = 0; h.iter = 0; h.mode = 0;
     h.conv = conv; h.maxstep = max_iter;
+    h.watch = watch_stagnation ? 1 : 0; h.since = 0; h.best = 1e300; h.loops = 0;
+    if (restart_an2) { h.count = c.prm.an2_count; h.binary = 0; }
   }
   if (!cuda_ok(c, cudaMemcpyAsync(c.d_state, hs.data(), sizeof(DevState) * nb, cudaMemcpyHostToDevice, c.stream), "state write") ||
       !cuda_ok(c, cudaStreamSynchronize(c.stream), "sync"))
     return RISM3D_CUDA_ERROR;
   if (!cufft_ok(c, cufftSetStream(plan, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
-  cudaGraphExec_t &gx = (sizeof(T) == 8) ? c.graph64 : c.graph32;
-  if (!gx) gx = capture<T, V, CLOS>(c, a, plan);
-  const int kRing = 4, kLag = 2;
-  cudaEvent_t ev[kRing];
-  for (int i = 0; i < kRing; ++i) cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
-  // per solute: best rms seen and observations since it last improved
-  std::vector<double> best(nb, 1e300);
-  std::vector<int> since_best(nb, 0);
-  int launched = 0, status = RISM3D_OK, printed = 0;
-  bool stop = false;
-  while (!stop) {
-    if (gx) cudaGraphLaunch(gx, c.stream);
-    else launch_iteration<T, V, CLOS>(c, a, plan);
-    c.launches += 3;
-    cudaMemcpyAsync(&c.h_state[(size_t)(launched % kRing) * nb], c.d_state, sizeof(DevState) * nb,
-                    cudaMemcpyDeviceToHost, c.stream);
-    cudaEventRecord(ev[launched % kRing], c.stream);
-    ++launched;
-    if (launched > kLag) {
-      int k = (launched - 1 - kLag) % kRing;
-      if (!cuda_ok(c, cudaEventSynchronize(ev[k]), "iteration")) { status = RISM3D_CUDA_ERROR; break; }
-      const DevState *ss = &c.h_state[(size_t)k * nb];
-      if (nb == 1 && c.prm.verbose && ss[0].iter > printed) {   // iterate.cu:63
-        printf(" Step = %d Reside = %g\n", ss[0].iter, ss[0].rms);
-        printed = ss[0].iter;
+  int status = RISM3D_OK;
+  // preferred: the whole phase as one launch with a device-side loop
+  cudaGraphExec_t &lx = REF ? c.loop32r : (sizeof(T) == 8) ? c.loop64 : c.loop32;
+  if (!lx && !c.no_device_loop) {
+    lx = capture_loop<T, V, CLOS, REF>(c, a, plan);
+    if (!lx) c.no_device_loop = true;
+  }
+  if (lx) {
+    if (!cuda_ok(c, cudaGraphLaunch(lx, c.stream), "phase launch") ||
+        !cuda_ok(c, cudaMemcpyAsync(c.h_state, c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream), "state read") ||
+        !cuda_ok(c, cudaStreamSynchronize(c.stream), "phase"))
+      return RISM3D_CUDA_ERROR;
+    c.launches += 4LL * c.h_state[0].loops;
+  } else {
+    // host-driven: one captured iteration per launch, the state read two
+    // iterations late from pinned memory
+    cudaGraphExec_t &gx = REF ? c.graph32r : (sizeof(T) == 8) ? c.graph64 : c.graph32;
+    if (!gx) gx = capture<T, V, CLOS, REF>(c, a, plan);
+    const int kRing = 4, kLag = 2;
+    cudaEvent_t ev[kRing];
+    for (int i = 0; i < kRing; ++i) cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+    int launched = 0;
+    bool stop = false;
+    while (!stop) {
+      if (gx) cudaGraphLaunch(gx, c.stream);
+      else launch_iteration<T, V, CLOS, REF>(c, a, plan);
+      c.launches += 3;
+      cudaMemcpyAsync(&c.h_state[(size_t)(launched % kRing) * nb], c.d_state, sizeof(DevState) * nb,
+                      cudaMemcpyDeviceToHost, c.stream);
+      cudaEventRecord(ev[launched % kRing], c.stream);
+      ++launched;
+      if (launched > kLag) {
+        int k = (launched - 1 - kLag) % kRing;
+        if (!cuda_ok(c, cudaEventSynchronize(ev[k]), "iteration")) { status = RISM3D_CUDA_ERROR; break; }
+        const DevState *ss = &c.h_state[(size_t)k * nb];
+        bool all_done = true;
+        for (int b = 0; b < nb; ++b)
+          if (!ss[b].done) all_done = false;
+        if (all_done) stop = true;
       }
-      bool all_done = true, all_idle = true;
-      for (int b = 0; b < nb; ++b) {
-        const DevState &s = ss[b];
-        if (!s.done) all_done = false;
-        if (watch_stagnation && !s.done) {
-          if (s.rms < 0.9 * best[b]) { best[b] = s.rms; since_best[b] = 0; }
-          else ++since_best[b];
-          if (since_best[b] <= 30) all_idle = false;
-        }
-      }
-      if (all_done) stop = true;
-      if (watch_stagnation && all_idle) stop = true;
+      if (launched > max_iter + kLag + 2) stop = true;   // hard bound
     }
-    if (launched > max_iter + kLag + 2) stop = true;   // hard bound
+    // drain: one more iteration guarantees the snapshot pass ran
+    if (status == RISM3D_OK) {
+      if (gx) cudaGraphLaunch(gx, c.stream);
+      else launch_iteration<T, V, CLOS, REF>(c, a, plan);
+      c.launches += 3;
+      cudaMemcpyAsync(c.h_state, c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream);
+      if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "iteration drain")) status = RISM3D_CUDA_ERROR;
+    }
+    for (int i = 0; i < kRing; ++i) cudaEventDestroy(ev[i]);
   }
-  // drain: one more iteration guarantees the snapshot pass ran
-  if (status == RISM3D_OK) {
-    if (gx) cudaGraphLaunch(gx, c.stream);
-    else launch_iteration<T, V, CLOS>(c, a, plan);
-    c.launches += 3;
-    cudaMemcpyAsync(c.h_state, c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream);
-    if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "iteration drain")) status = RISM3D_CUDA_ERROR;
-  }
-  for (int i = 0; i < kRing; ++i) cudaEventDestroy(ev[i]);
   iters_out = 0;
   for (int b = 0; b < nb; ++b) iters_out = std::max(iters_out, c.h_state[b].iter);
+  // progress lines of the reference (iterate.cu:63), from the device record
+  if (status == RISM3D_OK && c.prm.verbose && nb == 1 && c.d_hist && iters_out > 0) {
+    std::vector<double> hr(std::min(iters_out, c.hist_cap));
+    if (cuda_ok(c, cudaMemcpy(hr.data(), c.d_hist, sizeof(double) * hr.size(), cudaMemcpyDeviceToHost), "history"))
+      for (size_t i = 0; i < hr.size(); ++i) printf(" Step = %d Reside = %g\n", (int)i + 1, hr[i]);
+  }
   return status;
+}
+
+// One FP64 cycle at the base t0 = d_t without an update (pass A in mode 0,
+// both transforms, the k-space pass with the stage's fk), then the
+// refinement base: R0, x0, d = 0 and the FP32 history relative to t0.
+template <int V, int CLOS>
+int refine_base(Context &c) {
+  const int nb = c.nb;
+  std::vector<DevState> hs(nb);
+  if (!cuda_ok(c, cudaMemcpyAsync(hs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream), "state read") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "sync"))
+    return RISM3D_CUDA_ERROR;
+  for (DevState &h : hs) { h.done = 0; h.after_done = 0; h.mode = 0; }
+  if (!cuda_ok(c, cudaMemcpyAsync(c.d_state, hs.data(), sizeof(DevState) * nb, cudaMemcpyHostToDevice, c.stream), "state write"))
+    return RISM3D_CUDA_ERROR;
+  IterArgs<double> a = make_args<double>(c, true);
+  a.buf = c.d_buf; a.t = c.d_t; a.U = c.d_U; a.Y = c.d_Y; a.RP = c.d_RP;
+  a.tw = c.d_tw;
+  const dim3 ba(grid_blocks(c.n), nb), bk(grid_blocks(c.n / 2), nb);
+  if (!cufft_ok(c, cufftSetStream(c.plan64, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
+  k_pass_a<double, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a);
+  if (!cufft_ok(c, cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)a.buf, (cufftDoubleComplex *)a.buf,
+                                CUFFT_FORWARD), "refine base FFT"))
+    return RISM3D_CUFFT_ERROR;
+  k_kspace<double, V><<<bk, kThreads, 0, c.stream>>>(a);
+  if (!cufft_ok(c, cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)a.buf, (cufftDoubleComplex *)a.buf,
+                                CUFFT_INVERSE), "refine base FFT"))
+    return RISM3D_CUFFT_ERROR;
+  k_refine_base<V, CLOS><<<ba, kThreads, 0, c.stream>>>(a, c.f_R0, c.f_x0, c.f_t, c.f_Y);
+  c.launches += 5;
+  return cuda_ok(c, cudaGetLastError(), "refine base") ? RISM3D_OK : RISM3D_CUDA_ERROR;
 }
 
 template <int V, int CLOS>
@@ -835,6 +1051,8 @@ int solve_v(Context &c, int chargeup) {
   if (d_tinit) cudaFreeAsync(d_tinit, c.stream);
 
   int total = 0, total32 = 0, status = RISM3D_OK;
+  std::vector<int> per_it(nb, 0), per_it32(nb, 0);   // per solute, all phases and stages
+  bool fresh_an2 = false;
   StageParams *d_step = nullptr;
   if (!cuda_ok(c, cudaMallocAsync(&d_step, sizeof(StageParams), c.stream), "alloc")) return RISM3D_CUDA_ERROR;
   for (int s = 0; s <= cu; ++s) {
@@ -859,19 +1077,22 @@ int solve_v(Context &c, int chargeup) {
     if (c.prm.verbose) printf("relaxing 3D UV RISM: Charge Up Factor = %g\n", cf);
     int left = c.prm.maxstep;
     if (mixed) {
-      // FP32 bulk: t/history to FP32, iterate to the switch point or until
-      // progress stalls, then promote back to FP64 for the polish.
+      // FP32 bulk (plain form) down to the switch residual, then one FP64
+      // cycle fixes the base t0 and FP32 refinement passes carry the
+      // correction to the FP64 tolerance; the FP64 phase below then only
+      // confirms convergence and snapshots h and g.
       const long long vn = vnb;
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(vn, c.d_t, c.f_t);
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.d_Y, c.f_Y);
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.d_RP, c.f_RP);
       c.launches += 3;
-      double sw = c.prm.mixed_switch > 0 ? c.prm.mixed_switch : 5.0 * c.prm.convergence;
+      double sw = c.prm.mixed_switch > 0 ? c.prm.mixed_switch : 100.0 * c.prm.convergence;
       if (sw < c.prm.convergence) sw = c.prm.convergence;
       int it32 = 0;
-      int st = iterate_phase<float, V, CLOS>(c, c.plan32, c.f_t, c.f_U, c.f_Y, c.f_RP,
-                                            c.f_buf, false, sw, left, true, it32);
+      int st = iterate_phase<float, V, CLOS, false>(c, c.plan32, c.f_t, c.f_U, c.f_Y, c.f_RP,
+                                                   c.f_buf, false, sw, left, true, it32);
       if (st != RISM3D_OK) { status = st; break; }
+      for (int b = 0; b < nb; ++b) { per_it[b] += c.h_state[b].iter; per_it32[b] += c.h_state[b].iter; }
       std::vector<DevState> s32(nb);
       cudaMemcpy(s32.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost);
       bool any_div = false;
@@ -884,18 +1105,55 @@ int solve_v(Context &c, int chargeup) {
         k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, vnb, nullptr, c.d_fr, c.d_stage, c.d_t);
         c.launches += 1;
       } else {
+        // base t0 = the FP32 state (exact in FP64), its residual in FP64
         k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(vn, c.f_t, c.d_t);
-        k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.f_Y, c.d_Y);
-        k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.f_RP, c.d_RP);
-        c.launches += 3;
+        c.launches += 1;
+        st = refine_base<V, CLOS>(c);
+        if (st != RISM3D_OK) { status = st; break; }
+        total += 1;
+        left -= 1;
+        for (int b = 0; b < nb; ++b) per_it[b] += 1;
+        int itr = 0;
+        if (left > 0) {
+          StageParams spr{};
+          for (int v = 0; v < V; ++v) spr.irho[v] = sp.irho[v];   // qcf = 0: fk cancels
+          cudaMemcpyAsync(c.d_stage_ref, &spr, sizeof(spr), cudaMemcpyHostToDevice, c.stream);
+          st = iterate_phase<float, V, CLOS, true>(c, c.plan32, c.f_t, c.f_x0, c.f_Y, c.f_RP,
+                                                  c.f_buf, false, c.prm.convergence, left,
+                                                  true, itr, c.f_R0);
+          if (st != RISM3D_OK) { status = st; break; }
+          bool rdiv = false;
+          for (int b = 0; b < nb; ++b) {
+            per_it[b] += c.h_state[b].iter;
+            per_it32[b] += c.h_state[b].iter;
+            rdiv = rdiv || c.h_state[b].done == 2;
+          }
+          if (rdiv) {
+            // a refinement that blew up: keep the base t0 and let FP64
+            // continue from it with a fresh AN2 history
+            cudaMemsetAsync(c.f_t, 0, sizeof(float) * vn, c.stream);
+            cudaMemsetAsync(c.f_Y, 0, sizeof(float) * 2 * vn, c.stream);
+            cudaMemsetAsync(c.f_RP, 0, sizeof(float) * 2 * vn, c.stream);
+            fresh_an2 = true;
+          }
+        }
+        total32 += itr;
+        total += itr;
+        left -= itr;
+        k_refine_finish<<<gb, kThreads, 0, c.stream>>>(n, V, vnb, c.f_t, c.f_Y, c.f_RP, c.d_t,
+                                                      c.d_Y, c.d_RP);
+        c.launches += 1;
       }
       if (left < 1) left = 1;
     }
     int it = 0;
-    int st = iterate_phase<double, V, CLOS>(c, c.plan64, c.d_t, c.d_U, c.d_Y, c.d_RP,
-                                           c.d_buf, true, c.prm.convergence, left, false, it);
+    int st = iterate_phase<double, V, CLOS, false>(c, c.plan64, c.d_t, c.d_U, c.d_Y, c.d_RP,
+                                                  c.d_buf, true, c.prm.convergence, left, false,
+                                                  it, nullptr, fresh_an2);
     if (st != RISM3D_OK) { status = st; break; }
+    fresh_an2 = false;
     total += it;
+    for (int b = 0; b < nb; ++b) per_it[b] += c.h_state[b].iter;
     std::vector<DevState> fs(nb);
     cudaMemcpy(fs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost);
     c.res.rms = fs[0].rms;
@@ -903,7 +1161,8 @@ int solve_v(Context &c, int chargeup) {
       c.bres.assign(nb, rism3d_result{});
       for (int b = 0; b < nb; ++b) {
         c.bres[b].rms = fs[b].rms;
-        c.bres[b].iterations = fs[b].iter;
+        c.bres[b].iterations = per_it[b];
+        c.bres[b].iterations_fp32 = per_it32[b];
         c.bres[b].status = fs[b].done == 1 ? RISM3D_OK
                          : fs[b].done == 2 ? RISM3D_DIVERGED : RISM3D_NOT_CONVERGED;
       }
@@ -939,6 +1198,7 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
     if (!c.f_buf) { c.err = "FP32 kernels need a MIXED context"; return RISM3D_BAD_STATE; }
     a.buf = (typename Cx<T>::t *)c.f_buf; a.t = (T *)c.f_t; a.U = (T *)c.f_U;
     a.Y = (T *)c.f_Y; a.RP = (T *)c.f_RP;
+    if (which == 13 || which == 15) { a.U = (T *)c.f_x0; a.R0 = (const T *)c.f_R0; }
   }
   a.tw = (const typename Cx<T>::t *)(fp64 ? (void *)c.d_tw : (void *)c.d_twf);
   DevState saved, run;
@@ -955,10 +1215,12 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
   const int ba = grid_blocks(a.n), bk = grid_blocks(a.n / 2);
   cudaEventRecord(e0, c.stream);
   for (int r = 0; r < reps; ++r) {
-    switch (which % 10) {
-      case 0: k_pass_a<T, V, CLOS><<<ba, kThreads, 0, c.stream>>>(a); break;
-      case 1: k_kspace<T, V><<<bk, kThreads, 0, c.stream>>>(a); break;
-      default: k_pass_r<T, V, CLOS><<<a.nblocks, kThreads, 0, c.stream>>>(a); break;
+    switch (which) {
+      case 0: case 10: k_pass_a<T, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a); break;
+      case 13: k_pass_a<T, V, CLOS, true><<<ba, kThreads, 0, c.stream>>>(a); break;
+      case 1: case 11: k_kspace<T, V><<<bk, kThreads, 0, c.stream>>>(a); break;
+      case 15: k_pass_r<T, V, CLOS, true><<<a.nblocks, kThreads, 0, c.stream>>>(a); break;
+      default: k_pass_r<T, V, CLOS, false><<<a.nblocks, kThreads, 0, c.stream>>>(a); break;
     }
   }
   cudaEventRecord(e1, c.stream);
@@ -1068,6 +1330,11 @@ int upload_chi(Context &c) {
   // the captured iteration graphs embed the table pointers
   if (c.graph64) { cudaGraphExecDestroy(c.graph64); c.graph64 = nullptr; }
   if (c.graph32) { cudaGraphExecDestroy(c.graph32); c.graph32 = nullptr; }
+  if (c.graph32r) { cudaGraphExecDestroy(c.graph32r); c.graph32r = nullptr; }
+  for (cudaGraphExec_t *g : {&c.loop64, &c.loop32, &c.loop32r}) {
+    if (*g) cudaGraphExecDestroy(*g);
+    *g = nullptr;
+  }
   // Cubic cells: evaluate the spline once per distinct |k|^2 (the sorted
   // unique-|k| table of initialize_g.cu:31-43, indexed directly).
   if (c.d_xs) { cudaFree(c.d_xs); c.d_xs = nullptr; c.nxs = 0; }
@@ -1119,7 +1386,7 @@ int time_kernel(Context &c, int which, int reps, double *ms) {
     *ms = t / reps;
     return RISM3D_OK;
   }
-  if (!(which >= 0 && which <= 2) && !(which >= 10 && which <= 12)) {
+  if (!(which >= 0 && which <= 2) && !(which >= 10 && which <= 13) && which != 15) {
     c.err = "unknown kernel id";
     return RISM3D_BAD_INPUT;
   }

@@ -66,7 +66,7 @@ typedef struct {
   double an2_m;           /* AN2 mixing factor */
   double an2_mp;          /* AN2 bias on the newer slot */
   int precision;          /* RISM3D_FP64 or RISM3D_MIXED */
-  double mixed_switch;    /* MIXED: leave FP32 once rms <= this (0 = auto) */
+  double mixed_switch;    /* MIXED: plain FP32 -> FP32 refinement once rms <= this (0 = 100 x convergence) */
   int device;             /* CUDA ordinal (main.cu:57) */
   int verbose;            /* 1: print " Step = n Reside = r" like iterate.cu:63 */
   void *stream;           /* caller-owned cudaStream_t for all work; NULL: the
@@ -157,7 +157,8 @@ long long rism3d_kernel_launches(const rism3d_ctx *ctx);
 /* Measurement hook: launch one kernel `reps` times back to back on the
  * context stream and report the mean device time per launch (CUDA events).
  * which: 0/1/2 = FP64 pass A / pass K / pass R, 10/11/12 = the FP32
- * versions (MIXED contexts), 20 = real-space potential kernel.  The
+ * versions (MIXED contexts), 13/15 = FP32 pass A / pass R of the
+ * refinement form (MIXED, after a solve), 20 = real-space potential kernel.  The
  * iteration kernels run on the current state with an AN2 update armed, so
  * the stored solution is invalid afterwards (solve again to restore it). */
 int rism3d_time_kernel(rism3d_ctx *ctx, int which, int reps, double *ms_per_launch);

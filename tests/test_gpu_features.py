@@ -229,6 +229,9 @@ def test_large_cases_match_reference_executable(name, prec):
     r = s.solve()
     ref = ref_xmu(name)
     summary = json.load(open(os.path.join(GOLDEN, "ref_b200", "summary.json")))
+    if prec == 1:
+        # FP32 refinement reaches the FP64 tolerance: two FP64 cycles
+        assert r["iterations"] - r["iterations_fp32"] <= 3
     if prec == 0:
         # same AN2 trajectory; rounding of the packed-pair FFT can move the
         # step at which the 1e-6 threshold is crossed by a few iterations
