@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <new>
@@ -252,6 +253,9 @@ int context_init(Context &c, const rism3d_params *p, int nb, std::string &err) {
                      "alloc history")) &&
             cuda_ok(c, cudaHostAlloc(&c.h_state, sizeof(DevState) * 4 * nb, cudaHostAllocDefault), "alloc pinned");
   if (c.d_hist) c.hist_cap = std::max(p->maxstep, 1) + 8;
+  // RISM3D_HOST_LOOP=1: drive iterations from the host (one graph launch per
+  // iteration) instead of the device-side loop, e.g. for per-launch profiling
+  if (const char *e = getenv("RISM3D_HOST_LOOP")) c.no_device_loop = e[0] == '1';
   long long nbk = (c.n + 255) / 256;
   c.nred_blocks = (int)(nbk < 148 * 8 ? nbk : 148 * 8);
   ok = ok && cuda_ok(c, cudaMalloc(&c.d_part, sizeof(double) * 64 * c.nred_blocks * nb), "alloc partials") &&

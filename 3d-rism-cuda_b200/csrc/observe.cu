@@ -10,6 +10,8 @@
 // cal_grad gradients (cal_grad.cu:51-145) for ALL atoms in one launch: one
 // atom per thread, grid points streamed through shared memory (the
 // reference launches one full-grid kernel + Thrust reductions per pair).
+// Mixed-precision contexts evaluate the SE pair terms in FP32 (coordinates
+// as FP32 hi/lo pairs) and add each tile's FP32 sums into FP64.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -159,7 +161,7 @@ k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
       const double4 p = pp[i];
       const double dx = p.x - X, dy = p.y - Y, dz = p.z - Z;
       const double r2 = dx * dx + dy * dy + dz * dz;
-      const double ri = rsqrt(r2);
+      const double ri = rsqrt_nr<2>(r2);
       const double r1 = r2 * ri;
       const double ir2 = ri * ri;
       const double ir6 = ir2 * ir2 * ir2;
@@ -190,6 +192,142 @@ k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
     }
 #pragma unroll
     for (int k = 2 * V; k < NA; ++k) o[k] = acc[k];
+  }
+}
+
+// SE only, pair terms in FP32 (mixed-precision contexts); same partial
+// layout as k_atom_integrals with GRAD = 0.  Coordinates are carried as FP32
+// (hi, lo) pairs, so dx = (x_hi - X_hi) + (x_lo - X_lo) is accurate to FP32
+// relative precision of dx itself without any FP64 work in the pair loop.
+// The cutoff r < sigma/2 is tested on r^2; points within 2e-5 of a cutoff
+// re-test in FP64.  Each thread carries NA_T atoms (block: NA_T x 128
+// atoms) for independent work per shared-memory point.
+template <int V, int NA_T>
+__global__ void __launch_bounds__(kAtomsPerBlock, 4)
+k_atom_se32(int nx, int ny, int nz, double drx, double dry, double drz,
+            const double *__restrict__ g, const double *__restrict__ atoms_all,
+            const int *__restrict__ aoff, const int *__restrict__ acnt, int natom_tot,
+            SiteAll sv, double cc, long long chunk, double *part) {
+  constexpr int NA = 2 * V + 6;
+  const int sb = blockIdx.z;
+  const double *__restrict__ atoms = atoms_all + 8 * (size_t)aoff[sb];
+  const int natom = acnt[sb];
+  g += (size_t)sb * V * (size_t)nx * ny * nz;
+  __shared__ float4 ph[kPtsTile];           // x_hi y_hi z_hi
+  __shared__ float4 pl[kPtsTile];           // x_lo y_lo z_lo
+  __shared__ float pg[V][kPtsTile];
+  const long long n = (long long)nx * ny * nz;
+  int ia[NA_T];
+  bool live[NA_T], any = false;
+  float Xh[NA_T], Yh[NA_T], Zh[NA_T], Xl[NA_T], Yl[NA_T], Zl[NA_T];
+  float s6v[NA_T][V], e4[NA_T][V], qq[NA_T][V], hs2[NA_T][V];
+#pragma unroll
+  for (int a = 0; a < NA_T; ++a) {
+    ia[a] = blockIdx.x * kAtomsPerBlock * NA_T + a * kAtomsPerBlock + threadIdx.x;
+    live[a] = ia[a] < natom;
+    any = any || live[a];
+    double X = 0, Y = 0, Z = 0, qu = 0, su = 0, eu = 0;
+    if (live[a]) {
+      const double *p = atoms + 8 * (size_t)ia[a];
+      X = p[0]; Y = p[1]; Z = p[2]; qu = p[3]; su = p[4]; eu = p[5];
+    }
+    Xh[a] = (float)X; Yh[a] = (float)Y; Zh[a] = (float)Z;
+    Xl[a] = (float)(X - Xh[a]); Yl[a] = (float)(Y - Yh[a]); Zl[a] = (float)(Z - Zh[a]);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const double sg = (su + sv.sig[v]) * 0.5;  // cal_LJ.cu:28
+      const double sg2 = sg * sg;
+      s6v[a][v] = (float)(sg2 * sg2 * sg2);
+      e4[a][v] = (float)(4.0 * sqrt(eu * sv.eps[v]));
+      qq[a][v] = (float)(qu * sv.q[v] * cc);
+      hs2[a][v] = (float)(0.25 * sg2);
+    }
+  }
+  double acc[NA_T][2 * V];
+#pragma unroll
+  for (int a = 0; a < NA_T; ++a)
+#pragma unroll
+    for (int k = 0; k < 2 * V; ++k) acc[a][k] = 0.0;
+  const long long j0 = (long long)blockIdx.y * chunk;
+  const long long j1 = min(n, j0 + chunk);
+  for (long long base = j0; base < j1; base += kPtsTile) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < kPtsTile; i += blockDim.x) {
+      const long long j = base + i;
+      if (j < j1) {
+        const long long r = j / nx;
+        const int ix = (int)(j - r * nx), iy = (int)(r % ny), iz = (int)(r / ny);
+        const double px = (ix - nx / 2) * drx, py = (iy - ny / 2) * dry,   // cal_euv.cu:45-47
+                     pz = (iz - nz / 2) * drz;
+        const float hx = (float)px, hy = (float)py, hz = (float)pz;
+        ph[i] = make_float4(hx, hy, hz, 0.0f);
+        pl[i] = make_float4((float)(px - hx), (float)(py - hy), (float)(pz - hz), 0.0f);
+#pragma unroll
+        for (int v = 0; v < V; ++v) pg[v][i] = (float)g[(size_t)v * n + j];
+      } else {
+        ph[i] = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.0f);
+        pl[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+        for (int v = 0; v < V; ++v) pg[v][i] = 0.0f;
+      }
+    }
+    __syncthreads();
+    if (!any) continue;
+    const int m = (int)min((long long)kPtsTile, j1 - base);
+    float tl[NA_T][2 * V];
+#pragma unroll
+    for (int a = 0; a < NA_T; ++a)
+#pragma unroll
+      for (int k = 0; k < 2 * V; ++k) tl[a][k] = 0.0f;
+    for (int i = 0; i < m; ++i) {
+      const float4 h = ph[i], l = pl[i];
+      float gv[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) gv[v] = pg[v][i];
+#pragma unroll
+      for (int a = 0; a < NA_T; ++a) {
+        const float dx = (h.x - Xh[a]) + (l.x - Xl[a]);
+        const float dy = (h.y - Yh[a]) + (l.y - Yl[a]);
+        const float dz = (h.z - Zh[a]) + (l.z - Zl[a]);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float ri = rsqrtf(r2);
+        const float ir2 = ri * ri;
+        const float ir6 = ir2 * ir2 * ir2;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          bool inside = r2 < hs2[a][v];
+          if (fabsf(r2 - hs2[a][v]) < 2.0e-5f * hs2[a][v]) {   // rare: exact test
+            const double *p = atoms + 8 * (size_t)ia[a];
+            const double ex = ((double)h.x + l.x) - p[0], ey = ((double)h.y + l.y) - p[1],
+                         ez = ((double)h.z + l.z) - p[2];
+            inside = sqrt(ex * ex + ey * ey + ez * ez) < (p[4] + sv.sig[v]) * 0.25;
+          }
+          const float rs6i = s6v[a][v] * ir6;
+          const float lj = e4[a][v] * rs6i * (rs6i - 1.0f) * gv[v];
+          const float es = qq[a][v] * ri * gv[v];
+          // cutoff r < sigma/2 (selects, so r = 0 with its infinite terms
+          // inside the cutoff contributes exactly 0)
+          tl[a][v] += inside ? 0.0f : lj;
+          tl[a][V + v] += inside ? 0.0f : es;
+        }
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < NA_T; ++a)
+#pragma unroll
+      for (int k = 0; k < 2 * V; ++k) acc[a][k] += (double)tl[a][k];
+  }
+#pragma unroll
+  for (int a = 0; a < NA_T; ++a) {
+    if (!live[a]) continue;
+    double *o = part + ((size_t)blockIdx.y * natom_tot + aoff[sb] + ia[a]) * NA;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      o[v] = acc[a][v] * sv.rho[v];
+      o[V + v] = acc[a][V + v] * sv.rho[v];
+    }
+#pragma unroll
+    for (int k = 2 * V; k < NA; ++k) o[k] = 0.0;
   }
 }
 
@@ -255,7 +393,11 @@ int atoms_v(Context &c, bool forces) {
   const int A = c.natom;            // all solutes
   int amax = 0;
   for (int x : c.atom_cnt) amax = std::max(amax, x);
-  const int tiles = (amax + kAtomsPerBlock - 1) / kAtomsPerBlock;
+  // FP32 SE (mixed contexts, no forces): kSeAtoms atoms per thread
+  constexpr int kSeAtoms = V <= 4 ? 2 : 1;
+  const bool se32 = !forces && c.prm.precision == RISM3D_MIXED;
+  const int per_block = kAtomsPerBlock * (se32 ? kSeAtoms : 1);
+  const int tiles = (amax + per_block - 1) / per_block;
   // enough chunks to fill the GPU a few times over
   int nchunk = (148 * 8 + tiles * c.nb - 1) / (tiles * c.nb);
   if (nchunk < 1) nchunk = 1;
@@ -277,6 +419,10 @@ int atoms_v(Context &c, bool forces) {
   dim3 grid(tiles, nchunk, c.nb);
   if (forces)
     k_atom_integrals<V, 1><<<grid, kAtomsPerBlock, 0, c.stream>>>(
+        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, c.d_atom_off,
+        c.d_atom_cnt, A, sv, cc, chunk, c.d_atom_part);
+  else if (se32)
+    k_atom_se32<V, kSeAtoms><<<grid, kAtomsPerBlock, 0, c.stream>>>(
         c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g, c.d_atoms, c.d_atom_off,
         c.d_atom_cnt, A, sv, cc, chunk, c.d_atom_part);
   else

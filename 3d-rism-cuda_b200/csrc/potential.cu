@@ -15,6 +15,11 @@
 //
 // Atoms are staged through shared memory in tiles (every thread of a block
 // reads the same atom: broadcast); all sites are produced in one pass.
+//
+// Mixed-precision contexts (MIX) evaluate the LJ pair terms in FP32 with
+// per-tile FP64 accumulation and the e^-r factor beyond 20 A in FP32 (there
+// it is below 2e-9, so fr keeps FP64 accuracy); fr itself, 1/r and the
+// sums stay FP64.
 #include "rism3d_impl.h"
 
 namespace rism3d {
@@ -29,12 +34,13 @@ struct SiteLJ {
 };
 
 // Real-space grids.  Each thread owns two neighbouring points along x (one
-// row, the atom tile read once for both); per (point, atom) one FP64 rsqrt
-// gives 1/r, r and 1/r^2.  Beyond 40 A the factor e^-r (< 4.3e-18) is
-// dropped: there the reference's q (1 - e^-r) / r already rounds to q / r.
+// row, the atom tile read once for both); per (point, atom) one refined
+// reciprocal square root gives 1/r, r and 1/r^2.  Beyond 40 A the factor
+// e^-r (< 4.3e-18) is dropped: there the reference's q (1 - e^-r) / r
+// already rounds to q / r.
 constexpr int kPts = 2;
 
-template <int V>
+template <int V, bool MIX>
 __global__ void __launch_bounds__(kThreads)
 k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
               const double *__restrict__ atoms_all, const int *__restrict__ aoff,
@@ -42,6 +48,7 @@ k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
               double *__restrict__ u, double *__restrict__ esr, double *__restrict__ fr) {
   __shared__ double4 sa[kTile];           // x y z q
   __shared__ double2 sl[V][kTile];        // sigma_uv^2, 4 eps_uv / kBT
+  __shared__ float2 slf[V][kTile];        // the same in FP32 (MIX)
   const long long n = (long long)nx * ny * nz;
   // solute blockIdx.y: its atoms and its [V][N] / [N] grids
   const int sb = blockIdx.y;
@@ -80,11 +87,17 @@ k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
         for (int v = 0; v < V; ++v) {
           const double sg = (a[4] + sites.sig[v]) * 0.5;                 // cal_LJ.cu:28
           sl[v][i] = make_double2(sg * sg, 4.0 * sqrt(a[5] * sites.eps[v]) * ikbt);  // :29, :38
+          slf[v][i] = make_float2((float)sl[v][i].x, (float)sl[v][i].y);
         }
       }
     }
     __syncthreads();
     const int m = min(kTile, natom - t0);
+    float accf[kPts][V];
+#pragma unroll
+    for (int k = 0; k < kPts; ++k)
+#pragma unroll
+      for (int v = 0; v < V; ++v) accf[k][v] = 0.0f;
     for (int i = 0; i < m; ++i) {
       const double4 at = sa[i];
       const double dy = ry - at.y, dz = rz - at.z;
@@ -93,22 +106,37 @@ k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
       for (int k = 0; k < kPts; ++k) {
         const double dx = rx[k] - at.x;
         const double r2 = dx * dx + dyz;
-        const double ri = rsqrt(r2);
-        const double ir2 = r2 < cut2 ? 1.0 / cut2 : ri * ri;
+        const double ri = rsqrt_nr<MIX ? 1 : 2>(r2);
+        if (MIX) {
+          const float ir2 = r2 < cut2 ? (float)(1.0 / cut2) : (float)(ri * ri);
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const double2 p = sl[v][i];
-          const double s2 = p.x * ir2;
-          const double s6 = s2 * s2 * s2;
-          acc[k][v] += p.y * s6 * (s6 - 1.0);
+          for (int v = 0; v < V; ++v) {
+            const float2 p = slf[v][i];
+            const float s2 = p.x * ir2;
+            const float s6 = s2 * s2 * s2;
+            accf[k][v] += p.y * s6 * (s6 - 1.0f);
+          }
+        } else {
+          const double ir2 = r2 < cut2 ? 1.0 / cut2 : ri * ri;
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const double2 p = sl[v][i];
+            const double s2 = p.x * ir2;
+            const double s6 = s2 * s2 * s2;
+            acc[k][v] += p.y * s6 * (s6 - 1.0);
+          }
         }
         const double ra = r2 > 0.0 ? r2 * ri : 0.0;
         if (ra >= 1.0e-5) {                 // cal_Coulomb.cu:114-120
           const double qr = at.w * ri;
-          if (ra < 40.0) {
+          if (ra < (MIX ? 20.0 : 40.0)) {
             const double em1 = expm1(-ra);  // e^-r - 1
             afr[k] -= qr * em1;             // q (1 - e^-r) / r
             aes[k] += qr * (em1 + 1.0);     // q e^-r / r
+          } else if (MIX && ra < 40.0) {
+            const double es = qr * (double)expf(-(float)ra);
+            afr[k] += qr - es;
+            aes[k] += es;
           } else {
             afr[k] += qr;
           }
@@ -117,6 +145,12 @@ k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
           aes[k] -= at.w;
         }
       }
+    }
+    if (MIX) {
+#pragma unroll
+      for (int k = 0; k < kPts; ++k)
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[k][v] += (double)accf[k][v];
     }
   }
 #pragma unroll
@@ -196,9 +230,15 @@ k_potential_k(int nx, int ny, int nz, double bx, double by, double bz,
 template <int V>
 void launch_r(Context &c, const SiteLJ &sl, double ikbt, double ubeta) {
   long long blocks = (c.n / kPts + kThreads - 1) / kThreads;
-  k_potential_r<V><<<dim3((unsigned)blocks, c.nb), kThreads, 0, c.stream>>>(
-      c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.d_atom_off, c.d_atom_cnt, sl,
-      ikbt, ubeta, c.d_u, c.d_e, c.d_fr);
+  const dim3 grid((unsigned)blocks, c.nb);
+  if (c.prm.precision == RISM3D_MIXED)
+    k_potential_r<V, true><<<grid, kThreads, 0, c.stream>>>(
+        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.d_atom_off, c.d_atom_cnt, sl,
+        ikbt, ubeta, c.d_u, c.d_e, c.d_fr);
+  else
+    k_potential_r<V, false><<<grid, kThreads, 0, c.stream>>>(
+        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.d_atom_off, c.d_atom_cnt, sl,
+        ikbt, ubeta, c.d_u, c.d_e, c.d_fr);
 }
 
 }  // namespace

@@ -38,6 +38,12 @@ struct DevState {
   int watch;       // 1: stop as stalled (done = 4) when progress stops
   int since;       // steps since the best rms last improved by 10 %
   int loops;       // device-side loop: bodies run in this launch (solute 0)
+  int bodies;      // device-side loop bodies of the whole solve (solute 0)
+  int stage_iter;  // steps of this charge-up stage, all phases
+  int total_iter;  // steps of the solve, all stages and phases
+  int total32;     // of which FP32
+  int fallback;    // (solute 0) the FP32 bulk diverged: stage restarts in FP64
+  int restart_next;  // (solute 0) FP64 phase starts a fresh AN2 history
   double best;     // best rms of this run (stagnation watch)
   double conv;
   double m, mp;    // AN2 mixing factor and bias
@@ -45,6 +51,23 @@ struct DevState {
   double rms;
   double sums[6];  // sum R^2, c0, c1, a00, a01, a11 of the last pass R
 };
+
+// 1/sqrt(x) for x > 0: the FP64 hardware approximation (rsqrt.approx.f64,
+// ~2^-22 relative error e) refined by STEPS Newton-Raphson steps
+// y <- y (3 - x y^2) / 2, each of which squares the error (1.5 e^2 after
+// one step, ~1e-13; FP64 rounding after two).  x below 1e-300 is treated as
+// 1e-300 (callers handle r = 0 separately).
+#ifdef __CUDACC__
+template <int STEPS>
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  x = fmax(x, 1.0e-300);
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+#pragma unroll
+  for (int s = 0; s < STEPS; ++s) y = y * (1.5 - 0.5 * x * y * y);
+  return y;
+}
+#endif
 
 // Per charge-up stage constants, read by the kernels through a pointer so
 // that one captured iteration graph serves every stage.

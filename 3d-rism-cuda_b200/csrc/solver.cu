@@ -37,8 +37,10 @@
 // to eps32 |d| and AN2 (which is affine, so it acts on d unchanged)
 // converges to the FP64 tolerance in FP32 passes.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "rism3d_impl.h"
@@ -736,15 +738,20 @@ k_refine_base(IterArgs<double> a0, float *R0, float *x0, float *d, float *Yf) {
 }
 
 // Refinement end: t = t0 + d and the AN2 history back to absolute FP64
-// values; arrays [B][V][N] (t, d) and [B][2][V][N] (history).
+// values; arrays [B][V][N] (t, d) and [B][2][V][N] (history).  After a
+// bulk divergence (fallback) nothing changes; after a refinement that blew
+// up, t stays t0 and the FP64 phase rebuilds the history (restart_next).
 __global__ void k_refine_finish(long long n, int nv, long long total, const float *d,
-                                const float *Yf, const float *RPf, double *t, double *Y,
-                                double *RP) {
+                                const float *Yf, const float *RPf, const DevState *st,
+                                double *t, double *Y, double *RP) {
+  if (st[0].fallback) return;
+  const bool keep = st[0].restart_next != 0;
   for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < total;
        f += (long long)gridDim.x * blockDim.x) {
     const long long b = f / (nv * n), r = f - b * nv * n;
     const size_t h0 = (size_t)b * 2 * nv * n + r, h1 = h0 + (size_t)nv * n;
     const double t0 = t[f];
+    if (keep) continue;
     Y[h0] = (double)Yf[h0] + t0;
     Y[h1] = (double)Yf[h1] + t0;
     RP[h0] = (double)RPf[h0];
@@ -838,6 +845,7 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, DevState *st, int nb) 
   for (int b = 0; b < nb; ++b)
     if (!(st[b].done && st[b].after_done >= 1)) more = true;
   const int loops = ++st[0].loops;
+  st[0].bodies += 1;
   const int cap = st[0].maxstep < 1000000 ? st[0].maxstep : 1000000;
   if (loops >= cap + 4) more = false;
   cudaGraphSetConditional(h, more ? 1u : 0u);
@@ -884,47 +892,113 @@ cudaGraphExec_t capture_loop(Context &c, const IterArgs<T> &a, cufftHandle plan)
   return x;
 }
 
+// Phase control on the device, so that a solve needs no host round trip
+// between its phases.  Kinds: the plain FP32 bulk, the FP32 refinement,
+// the final FP64 phase, and the single FP64 base cycle of the refinement.
+enum PhaseKind { kPlain32 = 0, kRefine32 = 1, kFinal64 = 2, kBase64 = 3 };
+
+// Start of a phase: reset the per-run words of every solute; the step
+// budget is what the stage has left (iterate.cu:51).  A refinement after
+// an FP32 divergence (fallback) is skipped: one idle body.  The final FP64
+// phase restarts AN2 from Picard steps when the history was discarded.
+__global__ void k_phase_begin(DevState *st, int nb, int kind, double conv, int maxstep,
+                              int watch, int an2_count) {
+  const bool fallback = st[0].fallback != 0;
+  const bool fresh = fallback || st[0].restart_next != 0;
+  __syncthreads();
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    DevState &s = st[b];
+    s.done = 0; s.after_done = 0; s.iter = 0; s.mode = 0;
+    if (kind == kBase64) continue;
+    s.conv = conv;
+    s.maxstep = max(1, maxstep - s.stage_iter);
+    s.watch = watch; s.since = 0; s.best = 1e300; s.loops = 0;
+    if (kind == kRefine32 && fallback) { s.done = 4; s.after_done = 1; }
+    if (kind == kFinal64 && fresh) { s.count = an2_count; s.binary = 0; }
+  }
+}
+
+// End of a phase: step counters, and the flags the next phases read.
+__global__ void k_phase_end(DevState *st, int nb, int kind, int fp32) {
+  __shared__ int any_div;
+  if (threadIdx.x == 0) any_div = 0;
+  __syncthreads();
+  const bool fallback = st[0].fallback != 0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    DevState &s = st[b];
+    const int steps = kind == kBase64 ? (fallback ? 0 : 1) : s.iter;
+    s.stage_iter += steps;
+    s.total_iter += steps;
+    if (fp32) s.total32 += steps;
+    if (s.done == 2) atomicOr(&any_div, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (kind == kPlain32) st[0].fallback = any_div;
+    if (kind == kRefine32 && !fallback) st[0].restart_next = any_div;
+  }
+}
+
+__global__ void k_stage_begin(DevState *st, int nb) {
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) st[b].stage_iter = 0;
+  if (threadIdx.x == 0) { st[0].fallback = 0; st[0].restart_next = 0; }
+}
+
+// After the FP32 bulk: the refinement base t0 (exact FP32 -> FP64), or on a
+// divergence the stage start t_SR = 0 for the FP64 restart.
+__global__ void k_promote_base(long long total, const float *tf, const DevState *st,
+                               double *t) {
+  const bool fallback = st[0].fallback != 0;
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < total;
+       f += (long long)gridDim.x * blockDim.x)
+    t[f] = fallback ? 0.0 : (double)tf[f];
+}
+
+// One phase: the device-side loop graph when available (no host sync), else
+// iterations driven from the host.  Progress lines and the optional trace
+// need the host and synchronise.
 template <typename T, int V, int CLOS, bool REF>
-int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
-                  typename Cx<T>::t *buf, bool snapshot, double conv,
-                  int max_iter, bool watch_stagnation, int &iters_out,
-                  const T *R0 = nullptr, bool restart_an2 = false) {
+int run_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
+              typename Cx<T>::t *buf, bool snapshot, int kind, double conv, bool watch,
+              const T *R0 = nullptr) {
   IterArgs<T> a = make_args<T>(c, sizeof(T) == 8);
   a.buf = buf; a.t = t; a.U = U; a.Y = Y; a.RP = RP;
   if (REF) { a.R0 = R0; a.sp = c.d_stage_ref; }
   a.hout = snapshot ? c.d_h : nullptr;
   a.gout = snapshot ? c.d_g : nullptr;
   a.tw = (const typename Cx<T>::t *)(sizeof(T) == 8 ? (void *)c.d_tw : (void *)c.d_twf);
-  // reset the per-run control words; AN2 count/binary persist unless the
-  // history was discarded
   const int nb = c.nb;
-  std::vector<DevState> hs(nb);
-  if (!cuda_ok(c, cudaMemcpyAsync(hs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream), "state read") ||
-      !cuda_ok(c, cudaStreamSynchronize(c.stream), "sync"))
-    return RISM3D_CUDA_ERROR;
-  for (DevState &h : hs) {
-    h.done = 0; h.after_done = 0; h.iter = 0; h.mode = 0;
-    h.conv = conv; h.maxstep = max_iter;
-    h.watch = watch_stagnation ? 1 : 0; h.since = 0; h.best = 1e300; h.loops = 0;
-    if (restart_an2) { h.count = c.prm.an2_count; h.binary = 0; }
-  }
-  if (!cuda_ok(c, cudaMemcpyAsync(c.d_state, hs.data(), sizeof(DevState) * nb, cudaMemcpyHostToDevice, c.stream), "state write") ||
-      !cuda_ok(c, cudaStreamSynchronize(c.stream), "sync"))
-    return RISM3D_CUDA_ERROR;
+  k_phase_begin<<<1, 128, 0, c.stream>>>(c.d_state, nb, kind, conv, c.prm.maxstep,
+                                         watch ? 1 : 0, c.prm.an2_count);
+  c.launches += 1;
   if (!cufft_ok(c, cufftSetStream(plan, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
   int status = RISM3D_OK;
-  // preferred: the whole phase as one launch with a device-side loop
+  static const bool trace = getenv("RISM3D_TRACE") && getenv("RISM3D_TRACE")[0] == '1';
   cudaGraphExec_t &lx = REF ? c.loop32r : (sizeof(T) == 8) ? c.loop64 : c.loop32;
   if (!lx && !c.no_device_loop) {
     lx = capture_loop<T, V, CLOS, REF>(c, a, plan);
     if (!lx) c.no_device_loop = true;
   }
   if (lx) {
-    if (!cuda_ok(c, cudaGraphLaunch(lx, c.stream), "phase launch") ||
-        !cuda_ok(c, cudaMemcpyAsync(c.h_state, c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream), "state read") ||
-        !cuda_ok(c, cudaStreamSynchronize(c.stream), "phase"))
-      return RISM3D_CUDA_ERROR;
-    c.launches += 4LL * c.h_state[0].loops;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (trace) {
+      cudaEventCreate(&t0);
+      cudaEventCreate(&t1);
+      cudaEventRecord(t0, c.stream);
+    }
+    if (!cuda_ok(c, cudaGraphLaunch(lx, c.stream), "phase launch")) return RISM3D_CUDA_ERROR;
+    if (trace) {
+      cudaEventRecord(t1, c.stream);
+      DevState s0;
+      cudaMemcpyAsync(&s0, c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream);
+      cudaStreamSynchronize(c.stream);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, t0, t1);
+      fprintf(stderr, "[rism3d] phase %s%s: %d bodies, %d steps, device %.2f ms\n",
+              sizeof(T) == 8 ? "fp64" : "fp32", REF ? "-refine" : "", s0.loops, s0.iter, ms);
+      cudaEventDestroy(t0);
+      cudaEventDestroy(t1);
+    }
   } else {
     // host-driven: one captured iteration per launch, the state read two
     // iterations late from pinned memory
@@ -951,26 +1025,31 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
         for (int b = 0; b < nb; ++b)
           if (!ss[b].done) all_done = false;
         if (all_done) stop = true;
+        if (launched > ss[0].maxstep + kLag + 2) stop = true;   // hard bound
       }
-      if (launched > max_iter + kLag + 2) stop = true;   // hard bound
+      if (launched > c.prm.maxstep + kLag + 2) stop = true;
     }
     // drain: one more iteration guarantees the snapshot pass ran
     if (status == RISM3D_OK) {
       if (gx) cudaGraphLaunch(gx, c.stream);
       else launch_iteration<T, V, CLOS, REF>(c, a, plan);
       c.launches += 3;
-      cudaMemcpyAsync(c.h_state, c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream);
-      if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "iteration drain")) status = RISM3D_CUDA_ERROR;
     }
     for (int i = 0; i < kRing; ++i) cudaEventDestroy(ev[i]);
   }
-  iters_out = 0;
-  for (int b = 0; b < nb; ++b) iters_out = std::max(iters_out, c.h_state[b].iter);
+  // the loop's bodies (4 launches each: passes A, K, R and the loop test)
+  // are counted from the device record at the end of the solve
+  k_phase_end<<<1, 128, 0, c.stream>>>(c.d_state, nb, kind, sizeof(T) == 4 ? 1 : 0);
+  c.launches += 1;
   // progress lines of the reference (iterate.cu:63), from the device record
-  if (status == RISM3D_OK && c.prm.verbose && nb == 1 && c.d_hist && iters_out > 0) {
-    std::vector<double> hr(std::min(iters_out, c.hist_cap));
-    if (cuda_ok(c, cudaMemcpy(hr.data(), c.d_hist, sizeof(double) * hr.size(), cudaMemcpyDeviceToHost), "history"))
-      for (size_t i = 0; i < hr.size(); ++i) printf(" Step = %d Reside = %g\n", (int)i + 1, hr[i]);
+  if (status == RISM3D_OK && c.prm.verbose && nb == 1 && c.d_hist) {
+    DevState s0;
+    if (cuda_ok(c, cudaMemcpyAsync(&s0, c.d_state, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream), "state") &&
+        cuda_ok(c, cudaStreamSynchronize(c.stream), "state") && s0.iter > 0) {
+      std::vector<double> hr(std::min(s0.iter, c.hist_cap));
+      if (cuda_ok(c, cudaMemcpy(hr.data(), c.d_hist, sizeof(double) * hr.size(), cudaMemcpyDeviceToHost), "history"))
+        for (size_t i = 0; i < hr.size(); ++i) printf(" Step = %d Reside = %g\n", (int)i + 1, hr[i]);
+    }
   }
   return status;
 }
@@ -981,13 +1060,7 @@ int iterate_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
 template <int V, int CLOS>
 int refine_base(Context &c) {
   const int nb = c.nb;
-  std::vector<DevState> hs(nb);
-  if (!cuda_ok(c, cudaMemcpyAsync(hs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream), "state read") ||
-      !cuda_ok(c, cudaStreamSynchronize(c.stream), "sync"))
-    return RISM3D_CUDA_ERROR;
-  for (DevState &h : hs) { h.done = 0; h.after_done = 0; h.mode = 0; }
-  if (!cuda_ok(c, cudaMemcpyAsync(c.d_state, hs.data(), sizeof(DevState) * nb, cudaMemcpyHostToDevice, c.stream), "state write"))
-    return RISM3D_CUDA_ERROR;
+  k_phase_begin<<<1, 128, 0, c.stream>>>(c.d_state, nb, kBase64, 0.0, 0, 0, 0);
   IterArgs<double> a = make_args<double>(c, true);
   a.buf = c.d_buf; a.t = c.d_t; a.U = c.d_U; a.Y = c.d_Y; a.RP = c.d_RP;
   a.tw = c.d_tw;
@@ -1002,7 +1075,8 @@ int refine_base(Context &c) {
                                 CUFFT_INVERSE), "refine base FFT"))
     return RISM3D_CUFFT_ERROR;
   k_refine_base<V, CLOS><<<ba, kThreads, 0, c.stream>>>(a, c.f_R0, c.f_x0, c.f_t, c.f_Y);
-  c.launches += 5;
+  k_phase_end<<<1, 128, 0, c.stream>>>(c.d_state, nb, kBase64, 0);
+  c.launches += 6;
   return cuda_ok(c, cudaGetLastError(), "refine base") ? RISM3D_OK : RISM3D_CUDA_ERROR;
 }
 
@@ -1036,6 +1110,9 @@ int solve_v(Context &c, int chargeup) {
   if (mixed) {
     cudaMemsetAsync(c.f_Y, 0, sizeof(float) * 2 * vnb, c.stream);
     cudaMemsetAsync(c.f_RP, 0, sizeof(float) * 2 * vnb, c.stream);
+    StageParams spr{};
+    for (int v = 0; v < V; ++v) spr.irho[v] = sp.irho[v];   // qcf = 0: fk cancels
+    cudaMemcpyAsync(c.d_stage_ref, &spr, sizeof(spr), cudaMemcpyHostToDevice, c.stream);
   }
   // initial t_SR
   for (int v = 0; v < V; ++v) sp.qcf[v] = c.qv[v] * cf;
@@ -1050,11 +1127,11 @@ int solve_v(Context &c, int chargeup) {
   c.launches += 1;
   if (d_tinit) cudaFreeAsync(d_tinit, c.stream);
 
-  int total = 0, total32 = 0, status = RISM3D_OK;
-  std::vector<int> per_it(nb, 0), per_it32(nb, 0);   // per solute, all phases and stages
-  bool fresh_an2 = false;
+  int status = RISM3D_OK;
+  std::vector<DevState> fs(nb);
   StageParams *d_step = nullptr;
-  if (!cuda_ok(c, cudaMallocAsync(&d_step, sizeof(StageParams), c.stream), "alloc")) return RISM3D_CUDA_ERROR;
+  if (cu > 0 && !cuda_ok(c, cudaMallocAsync(&d_step, sizeof(StageParams), c.stream), "alloc"))
+    return RISM3D_CUDA_ERROR;
   for (int s = 0; s <= cu; ++s) {
     if (s > 0) {                                  // add_tuv (iterate.cu:43-47)
       double cfn = cf + cuf;
@@ -1073,14 +1150,16 @@ int solve_v(Context &c, int chargeup) {
     for (int v = 0; v < V; ++v) sp.qcf[v] = c.qv[v] * cf;
     cudaMemcpyAsync(c.d_stage, &sp, sizeof(sp), cudaMemcpyHostToDevice, c.stream);
     k_stage_u<<<gb, kThreads, 0, c.stream>>>(n, V, vnb, c.d_u, c.d_e, c.d_stage, c.d_U, mixed ? c.f_U : nullptr);
-    c.launches += 1;
+    k_stage_begin<<<1, 128, 0, c.stream>>>(c.d_state, nb);
+    c.launches += 2;
     if (c.prm.verbose) printf("relaxing 3D UV RISM: Charge Up Factor = %g\n", cf);
-    int left = c.prm.maxstep;
+    int st = RISM3D_OK;
     if (mixed) {
       // FP32 bulk (plain form) down to the switch residual, then one FP64
       // cycle fixes the base t0 and FP32 refinement passes carry the
       // correction to the FP64 tolerance; the FP64 phase below then only
-      // confirms convergence and snapshots h and g.
+      // confirms convergence and snapshots h and g.  A divergence of the
+      // bulk restarts the stage in FP64 (decided on the device).
       const long long vn = vnb;
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(vn, c.d_t, c.f_t);
       k_convert<double, float><<<gb, kThreads, 0, c.stream>>>(2 * vn, c.d_Y, c.f_Y);
@@ -1088,85 +1167,27 @@ int solve_v(Context &c, int chargeup) {
       c.launches += 3;
       double sw = c.prm.mixed_switch > 0 ? c.prm.mixed_switch : 100.0 * c.prm.convergence;
       if (sw < c.prm.convergence) sw = c.prm.convergence;
-      int it32 = 0;
-      int st = iterate_phase<float, V, CLOS, false>(c, c.plan32, c.f_t, c.f_U, c.f_Y, c.f_RP,
-                                                   c.f_buf, false, sw, left, true, it32);
+      st = run_phase<float, V, CLOS, false>(c, c.plan32, c.f_t, c.f_U, c.f_Y, c.f_RP, c.f_buf,
+                                           false, kPlain32, sw, true);
       if (st != RISM3D_OK) { status = st; break; }
-      for (int b = 0; b < nb; ++b) { per_it[b] += c.h_state[b].iter; per_it32[b] += c.h_state[b].iter; }
-      std::vector<DevState> s32(nb);
-      cudaMemcpy(s32.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost);
-      bool any_div = false;
-      for (const DevState &x : s32) any_div = any_div || x.done == 2;
-      total32 += it32;
-      total += it32;
-      left -= it32;
-      if (any_div) {
-        // FP32 diverged: restart this stage in FP64 from the stage start
-        k_init_t<<<gb, kThreads, 0, c.stream>>>(n, V, vnb, nullptr, c.d_fr, c.d_stage, c.d_t);
-        c.launches += 1;
-      } else {
-        // base t0 = the FP32 state (exact in FP64), its residual in FP64
-        k_convert<float, double><<<gb, kThreads, 0, c.stream>>>(vn, c.f_t, c.d_t);
-        c.launches += 1;
-        st = refine_base<V, CLOS>(c);
-        if (st != RISM3D_OK) { status = st; break; }
-        total += 1;
-        left -= 1;
-        for (int b = 0; b < nb; ++b) per_it[b] += 1;
-        int itr = 0;
-        if (left > 0) {
-          StageParams spr{};
-          for (int v = 0; v < V; ++v) spr.irho[v] = sp.irho[v];   // qcf = 0: fk cancels
-          cudaMemcpyAsync(c.d_stage_ref, &spr, sizeof(spr), cudaMemcpyHostToDevice, c.stream);
-          st = iterate_phase<float, V, CLOS, true>(c, c.plan32, c.f_t, c.f_x0, c.f_Y, c.f_RP,
-                                                  c.f_buf, false, c.prm.convergence, left,
-                                                  true, itr, c.f_R0);
-          if (st != RISM3D_OK) { status = st; break; }
-          bool rdiv = false;
-          for (int b = 0; b < nb; ++b) {
-            per_it[b] += c.h_state[b].iter;
-            per_it32[b] += c.h_state[b].iter;
-            rdiv = rdiv || c.h_state[b].done == 2;
-          }
-          if (rdiv) {
-            // a refinement that blew up: keep the base t0 and let FP64
-            // continue from it with a fresh AN2 history
-            cudaMemsetAsync(c.f_t, 0, sizeof(float) * vn, c.stream);
-            cudaMemsetAsync(c.f_Y, 0, sizeof(float) * 2 * vn, c.stream);
-            cudaMemsetAsync(c.f_RP, 0, sizeof(float) * 2 * vn, c.stream);
-            fresh_an2 = true;
-          }
-        }
-        total32 += itr;
-        total += itr;
-        left -= itr;
-        k_refine_finish<<<gb, kThreads, 0, c.stream>>>(n, V, vnb, c.f_t, c.f_Y, c.f_RP, c.d_t,
-                                                      c.d_Y, c.d_RP);
-        c.launches += 1;
-      }
-      if (left < 1) left = 1;
+      k_promote_base<<<gb, kThreads, 0, c.stream>>>(vn, c.f_t, c.d_state, c.d_t);
+      c.launches += 1;
+      st = refine_base<V, CLOS>(c);
+      if (st != RISM3D_OK) { status = st; break; }
+      st = run_phase<float, V, CLOS, true>(c, c.plan32, c.f_t, c.f_x0, c.f_Y, c.f_RP, c.f_buf,
+                                          false, kRefine32, c.prm.convergence, true, c.f_R0);
+      if (st != RISM3D_OK) { status = st; break; }
+      k_refine_finish<<<gb, kThreads, 0, c.stream>>>(n, V, vnb, c.f_t, c.f_Y, c.f_RP, c.d_state,
+                                                    c.d_t, c.d_Y, c.d_RP);
+      c.launches += 1;
     }
-    int it = 0;
-    int st = iterate_phase<double, V, CLOS, false>(c, c.plan64, c.d_t, c.d_U, c.d_Y, c.d_RP,
-                                                  c.d_buf, true, c.prm.convergence, left, false,
-                                                  it, nullptr, fresh_an2);
+    st = run_phase<double, V, CLOS, false>(c, c.plan64, c.d_t, c.d_U, c.d_Y, c.d_RP, c.d_buf,
+                                          true, kFinal64, c.prm.convergence, false);
     if (st != RISM3D_OK) { status = st; break; }
-    fresh_an2 = false;
-    total += it;
-    for (int b = 0; b < nb; ++b) per_it[b] += c.h_state[b].iter;
-    std::vector<DevState> fs(nb);
-    cudaMemcpy(fs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost);
-    c.res.rms = fs[0].rms;
-    if (nb > 1) {
-      c.bres.assign(nb, rism3d_result{});
-      for (int b = 0; b < nb; ++b) {
-        c.bres[b].rms = fs[b].rms;
-        c.bres[b].iterations = per_it[b];
-        c.bres[b].iterations_fp32 = per_it32[b];
-        c.bres[b].status = fs[b].done == 1 ? RISM3D_OK
-                         : fs[b].done == 2 ? RISM3D_DIVERGED : RISM3D_NOT_CONVERGED;
-      }
-    }
+    // the stage's outcome: one read of the device state
+    if (!cuda_ok(c, cudaMemcpyAsync(fs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream), "state read") ||
+        !cuda_ok(c, cudaStreamSynchronize(c.stream), "solve"))
+      return RISM3D_CUDA_ERROR;
     bool div = false, lim = false;
     for (const DevState &x : fs) { div = div || x.done == 2; lim = lim || (x.done != 1 && x.done != 2); }
     if (div) {                             // iterate.cu:74-75: report, go on
@@ -1178,12 +1199,33 @@ int solve_v(Context &c, int chargeup) {
       break;
     }
   }
-  cudaFreeAsync(d_step, c.stream);
+  if (d_step) cudaFreeAsync(d_step, c.stream);
+  if (!cuda_ok(c, cudaMemcpyAsync(fs.data(), c.d_state, sizeof(DevState) * nb, cudaMemcpyDeviceToHost, c.stream), "state read") ||
+      !cuda_ok(c, cudaStreamSynchronize(c.stream), "solve"))
+    return RISM3D_CUDA_ERROR;
+  int total = 0, total32 = 0;
+  long long bodies = 0;
+  for (const DevState &x : fs) {
+    total = std::max(total, x.total_iter);
+    total32 = std::max(total32, x.total32);
+  }
+  bodies = fs[0].bodies;
+  c.launches += 4 * bodies;
+  c.res.rms = fs[0].rms;
+  if (nb > 1) {
+    c.bres.assign(nb, rism3d_result{});
+    for (int b = 0; b < nb; ++b) {
+      c.bres[b].rms = fs[b].rms;
+      c.bres[b].iterations = fs[b].total_iter;
+      c.bres[b].iterations_fp32 = fs[b].total32;
+      c.bres[b].status = fs[b].done == 1 ? RISM3D_OK
+                       : fs[b].done == 2 ? RISM3D_DIVERGED : RISM3D_NOT_CONVERGED;
+    }
+  }
   c.cf_final = cf;
   c.res.iterations = total;
   c.res.iterations_fp32 = total32;
   c.res.status = status;
-  if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "solve")) return RISM3D_CUDA_ERROR;
   return (status == RISM3D_CUDA_ERROR || status == RISM3D_CUFFT_ERROR) ? status : RISM3D_OK;
 }
 

@@ -188,12 +188,14 @@ def run_ours(args, rank, world, dist):
     l0 = mixed.kernel_launches()
     clk.start()
     e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("mixed_solve")     # profiler filter (ncu --nvtx-include)
     e0.record(stream)
     res = []
     for _ in range(args.steps):
         mixed.refresh_potentials()
         res.append(mixed.solve())
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     clocks = clk.stop()
     barrier()
@@ -203,10 +205,12 @@ def run_ours(args, rank, world, dist):
 
     # ---- FP64 plain solve (the reference algorithm), same protocol
     barrier(); torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("fp64_solve")
     e0.record(stream)
     for _ in range(args.steps):
         fp64.refresh_potentials(); r64 = fp64.solve()
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     ms_fp64 = max_over_ranks(e0.elapsed_time(e1)) / args.steps
 

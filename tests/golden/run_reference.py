@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 BIN = os.path.join(ROOT, "oracle", "_ref", "3drism-cuda")
 
-CASES = ["test1", "test1_tight", "test2", "test2_tight", "test3", "test4",
+CASES = ["test1", "test1_tight", "test2", "test2_tight", "test3", "test4", "test4_tight",
          "cfg0_chain12", "cfg1_globule300", "cfg2_protein846_kh"]
 
 
