@@ -15,11 +15,12 @@ CSRC = os.path.join(TOP, "csrc")
 OBJ = os.path.join(CSRC, "_build")
 LIB = os.path.join(PKG, "librism3d_b200.so")
 CLI = os.path.join(TOP, "bin", "rism3d-b200")
+CLI1D = os.path.join(TOP, "bin", "rism1d-b200")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["potential.cu", "solver.cu", "observe.cu", "adjoint.cu", "batch.cu",
-           "noalloc.cu", "capi.cpp", "io.cpp"]
+           "noalloc.cu", "capi.cpp", "io.cpp", "xrism1d.cpp"]
 
 
 def _ccbin():
@@ -59,12 +60,13 @@ def build(verbose=False) -> str:
     if _newer(LIB, objs):
         subprocess.check_call([NVCC] + _ccbin() + ARCH + ["-shared", "-o", LIB] + objs +
                               ["-lcufft", "-lcudart"])
-    cli_src = os.path.join(CSRC, "cli.cpp")
-    if _newer(CLI, [cli_src, LIB]):
-        subprocess.check_call([NVCC] + _ccbin() + ["-O2", "-std=c++17",
-                               "-I" + os.path.join(ROOT, "include"), cli_src, "-o", CLI,
-                               "-L" + PKG, "-lrism3d_b200",
-                               "-Xlinker", "-rpath=$ORIGIN/../rism3d_b200"])
+    for exe, src in ((CLI, "cli.cpp"), (CLI1D, "cli1d.cpp")):
+        cli_src = os.path.join(CSRC, src)
+        if _newer(exe, [cli_src, LIB]):
+            subprocess.check_call([NVCC] + _ccbin() + ["-O2", "-std=c++17",
+                                   "-I" + os.path.join(ROOT, "include"), cli_src, "-o", exe,
+                                   "-L" + PKG, "-lrism3d_b200",
+                                   "-Xlinker", "-rpath=$ORIGIN/../rism3d_b200"])
     return LIB
 
 

@@ -3,7 +3,8 @@
 Workload: the protein-scale synthetic solute (846 atoms, compact random
 chain, Rg ~15 A, sigma 3.0-3.8 A, charges N(0, 0.3) shifted to net zero;
 seed 2) on a 256^3 grid in a 128 A cubic cell, KH closure, AN2 (2 0.6 0.2),
-convergence 1e-6, in the reference's TIP3P-like water (h2o_vv.xvk).  One
+convergence 1e-6, in the workloads' TIP3P water (298.15 K, 0.03334 /A^3;
+tip3p_cfg_vv.xvk from the library's own 1D XRISM-KH solve).  One
 step = one complete solve: potential grids, the iteration to convergence,
 and the .xmu observables (mu_ex SC/SC_HNC/GF, PMV, pressure, SE).
 
@@ -107,7 +108,7 @@ class Clocks:
 def workload():
     from oracle import formats as F
     ctrl, sol = F.read_control(os.path.join(GOLDEN, WORKLOAD + ".inp"))
-    sv = F.read_xvk(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    sv = F.read_xvk(os.path.join(GOLDEN, ctrl.fsolvent))
     return ctrl, sol, sv
 
 
@@ -253,10 +254,11 @@ def run_ours(args, rank, world, dist):
         "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": ("protein-like solute, 846 atoms, 256^3 grid, 128 A cell, KH, "
-                                "AN2 2/0.6/0.2, conv 1e-6, TIP3P-like water (h2o_vv.xvk)")
+                                "AN2 2/0.6/0.2, conv 1e-6, TIP3P water 298.15 K 0.03334/A^3 (tip3p_cfg_vv.xvk, "
+                                "1D XRISM-KH)")
                    if WORKLOAD == WORKLOADS["protein846"] else
                    ("globular solute, 300 atoms, 128^3 grid, 64 A cell, KH, AN2 2/0.6/0.2, "
-                    "conv 1e-6, TIP3P-like water (h2o_vv.xvk)"),
+                    "conv 1e-6, TIP3P water (tip3p_cfg_vv.xvk, 1D XRISM-KH)"),
                    "grid": list(ctrl.grid), "box": list(ctrl.box), "natom": len(sol.q),
                    "natv": V, "precision": "FP32 bulk + FP64 polish",
                    "l2": "state ~5 GB per solve >> 126 MB L2 (no flush needed)",
@@ -379,7 +381,8 @@ def run_reference(args):
                         "d2h_bytes_per_step": 0}}
     work = tempfile.mkdtemp(prefix="rism_ref_")
     shutil.copyfile(os.path.join(GOLDEN, WORKLOAD + ".inp"), os.path.join(work, WORKLOAD + ".inp"))
-    shutil.copyfile(os.path.join(GOLDEN, "h2o_vv.xvk"), os.path.join(work, "h2o_vv.xvk"))
+    ctrl, _, _ = workload()
+    shutil.copyfile(os.path.join(GOLDEN, ctrl.fsolvent), os.path.join(work, ctrl.fsolvent))
     times, iters, out = [], None, ""
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()

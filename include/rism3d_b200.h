@@ -224,6 +224,44 @@ int rism3d_iterate(rism3d_ctx *ctx, int chargeup);
  * .cuv, .euv, .qv according to the control file's outlist letters. */
 int rism3d_output(rism3d_ctx *ctx);
 
+/* ---- 1D XRISM solvent tables ------------------------------------------
+ * No counterpart in the reference: it reads X_ab(k) from .xvk files
+ * (solvent_read.cc:31-60) made by a separate program that it does not
+ * ship.  rism1d_solve computes them for a molecular solvent (any mixture of
+ * rigid molecules and ions) with the 1D extended RISM equations and the KH
+ * (or HNC) closure on the grid r_i = i dr, k_j = j pi / (ntab dr), and
+ * rism1d_write_xvk writes them in the .xvk layout the 3D solver reads. */
+typedef struct {
+  double temperature;   /* K */
+  int ntab;             /* radial / k points (power of two) */
+  double dr;            /* A */
+  int closure;          /* RISM3D_KH or RISM3D_HNC */
+  double convergence;   /* rms of the t update (0 = 1e-12) */
+  int maxstep;          /* 0 = 10000 */
+  double mixing;        /* DIIS mixing (0 = 0.3) */
+  int verbose;
+} rism1d_params;
+
+typedef struct {
+  char name[8];
+  int spc;              /* molecule (species) index, 1-based */
+  int sym;              /* site type, 1-based; negative: same type as |sym| */
+  double sigma;         /* A */
+  double epsilon;       /* J/mol */
+  double charge;        /* e */
+  double x, y, z;       /* A, in the molecule frame */
+  double density;       /* mol/L of the species */
+} rism1d_site;
+
+/* xvv (may be NULL): [ntype][ntype][ntab], X_ab(k_j) = sum over the sites
+ * of type b of (w_ab + rho_b h_ab), a the first site of its type (the
+ * layout of Solvent::xvv); xt: isothermal compressibility (1/Pa). */
+int rism1d_solve(const rism1d_params *p, int nsite, const rism1d_site *sites,
+                 double *xvv, double *xt, int *iterations);
+int rism1d_write_xvk(const char *path, const rism1d_params *p, int nsite,
+                     const rism1d_site *sites, const double *xvv, double xt);
+const char *rism1d_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,7 +27,8 @@ def run(case, outdir):
     d = os.path.join(outdir, case)
     os.makedirs(d, exist_ok=True)
     shutil.copyfile(os.path.join(HERE, case + ".inp"), os.path.join(d, case + ".inp"))
-    shutil.copyfile(os.path.join(HERE, "h2o_vv.xvk"), os.path.join(d, "h2o_vv.xvk"))
+    solvent = open(os.path.join(HERE, case + ".inp")).read().split()[4]   # read_input.cu:42
+    shutil.copyfile(os.path.join(HERE, solvent), os.path.join(d, solvent))
     t0 = time.perf_counter()
     p = subprocess.run(["timeout", "900", BIN, case + ".inp"], cwd=d,
                        capture_output=True, text=True)

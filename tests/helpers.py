@@ -14,8 +14,7 @@ MU_TOL = 0.01 * KCAL          # 0.01 kcal/mol in J/mol (the parity target)
 
 def load_case(name, **over):
     """Case from a control file in tests/golden (centred like the reference)."""
-    case, ctrl, sol = O.case_from_inp(os.path.join(GOLDEN, name + ".inp"),
-                                      xvk=os.path.join(GOLDEN, "h2o_vv.xvk"))
+    case, ctrl, sol = O.case_from_inp(os.path.join(GOLDEN, name + ".inp"))
     for k, v in over.items():
         setattr(case, k, v)
     return case, ctrl, sol

@@ -147,7 +147,8 @@ def _run_cli(tmp_path, inp_name, args=(), outlist=None):
     if outlist:
         txt = txt.replace(" m    0", " %s    0" % outlist, 1)
     (d / inp_name).write_text(txt)
-    shutil.copyfile(os.path.join(GOLDEN, "h2o_vv.xvk"), str(d / "h2o_vv.xvk"))
+    solvent = txt.split()[4]                       # read_input.cu:42
+    shutil.copyfile(os.path.join(GOLDEN, solvent), str(d / solvent))
     p = subprocess.run([CLI, *args, inp_name], cwd=str(d), capture_output=True, text=True,
                        timeout=300)
     assert p.returncode == 0, p.stdout + p.stderr

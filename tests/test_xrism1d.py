@@ -1,0 +1,52 @@
+"""1D XRISM solvent tables (rism1d_solve): the reference ships water
+susceptibility tables made by a program it does not include; the library's
+own 1D solver reproduces them from the model in their headers.  Runs on the
+CPU (host code of the library; no GPU involved)."""
+import os
+
+import numpy as np
+
+from conftest import GOLDEN
+from oracle import formats as F
+
+
+def _solve_shipped_water():
+    from rism3d_b200 import xrism1d as X
+    rows, T, ntab, dr = X.read_sites(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    return X, rows, T, ntab, dr, X.solve(rows, T, ntab, dr, convergence=1e-10)
+
+
+def test_water_table_matches_the_shipped_xvk():
+    """example/h2o_vv.xvk (TIP3P-like water, 298 K, 54 M, 4096 x 0.05 A):
+    X_ab(k) to 2e-5 absolute at every k, chi_T to 2e-5 relative."""
+    X, rows, T, ntab, dr, (xvv, xt, it) = _solve_shipped_water()
+    ref = F.read_xvk(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    assert xvv.shape == ref.xvv.shape
+    assert np.abs(xvv - ref.xvv).max() < 2e-5
+    assert abs(xt - ref.xt) < 2e-5 * ref.xt
+    # k -> pi/dr: the intramolecular terms alone (h vanishes on this grid)
+    assert xvv[0, 0, -1] == 1.0
+
+
+def test_written_table_reads_back(tmp_path):
+    X, rows, T, ntab, dr, (xvv, xt, it) = _solve_shipped_water()
+    path = str(tmp_path / "w.xvk")
+    X.write_xvk(path, rows, T, xvv, xt, ntab, dr)
+    back = F.read_xvk(path)
+    ref = F.read_xvk(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    assert back.natv == ref.natv and back.ntab == ref.ntab
+    assert np.allclose(back.rhov, ref.rhov) and np.allclose(back.qv, ref.qv)
+    assert np.allclose(back.sigv, ref.sigv) and np.allclose(back.epsv, ref.epsv)
+    assert abs(back.temper - T) < 1e-9 and abs(back.xt - xt) < 1e-9 * xt
+    assert np.abs(back.xvv - xvv).max() < 1e-14
+
+
+def test_bad_input_is_an_error():
+    import pytest
+    from rism3d_b200 import RismError
+    from rism3d_b200 import xrism1d as X
+    rows = [("O", 1, 1, 3.15, 636.0, 0.0, 0.0, 0.0, 0.0, 54.0)]
+    with pytest.raises(RismError):
+        X.solve(rows, 298.0, ntab=1000, dr=0.05)          # not a power of two
+    with pytest.raises(RismError):
+        X.solve([rows[0][:9] + (-1.0,)], 298.0, ntab=256)  # negative density
