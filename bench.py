@@ -168,13 +168,10 @@ def run_ours(args, rank, world, dist):
             import torch.distributed as D
             D.barrier()
 
+    from rism3d_b200 import replicas as RP
+
     def max_over_ranks(x):
-        if not dist:
-            return x
-        import torch.distributed as D
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        D.all_reduce(t, op=D.ReduceOp.MAX)
-        return float(t.item())
+        return RP.max_over_ranks(x, "cuda") if dist else x
 
     mixed = make(R.MIXED)
     fp64 = make(R.FP64)
@@ -242,8 +239,17 @@ def run_ours(args, rank, world, dist):
                            ("pass_r_fp64", 2, bpp64["pass_r"])):
         ms = fp64.time_kernel(kid, 20)
         kern[name] = {"ms": ms, "gbs": bpp * n / ms / 1e6}
+    # adjoint gradients of mu_ex (all charges, LJ parameters, positions) on
+    # the converged mixed solve: the exact discrete adjoint
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mixed.set_solute(sol.sig, sol.eps, sol.q, sol.xyz)
+    mixed.solve()
+    t1 = time.perf_counter()
+    mixed.grad()
+    adjoint_s = time.perf_counter() - t1
     mixed.close(); fp64.close()
-    batch = run_batch(args, dev, stream) if args.batch_mols > 0 else None
+    batch = run_batch(args, dev, stream, rank, world, dist) if args.batch_mols > 0 else None
     dom = "pass_a_fp32"
     achieved = kern[dom]["gbs"]
     traffic_pp = read_traffic("k_pass_a_fp32")
@@ -280,6 +286,8 @@ def run_ours(args, rank, world, dist):
                      "algorithmic_bytes_per_launch": bpp32["pass_a"] * n,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
         "batch": batch,
+        "adjoint": {"s_per_gradient": adjoint_s, "outputs": "d mu/d(q, sigma, eps, xyz) of all "
+                    "%d atoms" % len(sol.q)},
         "kernels": kern,
         "bytes_per_iteration": {"fp64": sum(bpp64.values()) * n, "fp32": sum(bpp32.values()) * n,
                                 "survey_formula_fp64": survey_bytes_per_iter(n, V, 8)},
@@ -289,22 +297,29 @@ def run_ours(args, rank, world, dist):
 
 
 # ------------------------------------------------------------ batch leg
-def run_batch(args, dev, stream):
+def run_batch(args, dev, stream, rank=0, world=1, dist=False):
     """Batched small solutes (BASELINE config 3 shapes): 256 molecules of
     8-40 atoms on 48^3 / 64^3 / 96^3 grids at 0.5 A, FP32 bulk + FP64 polish,
     in the reference's 3-site water + 0.1 M NaCl table (4 site types; the
     5-site water of the config needs the project's 1D XRISM tables).  Reports
     solves/s of one rism3d_solve_batch call and of a per-solute loop that
-    reuses one context per grid size (timed on a sample of the molecules)."""
+    reuses one context per grid size (timed on a sample of the molecules).
+    Under N ranks the molecules are split by estimated cost (grid points);
+    solves/s is all ranks' molecules over the slowest rank's time."""
     import torch
     import rism3d_b200 as R
     from oracle import formats as F
     from rism3d_b200 import synth
     sv = F.read_xvk(os.path.join(GOLDEN, "naclaq_sub4_vv.xvk"))
+    from rism3d_b200 import replicas as RP
     mols = []
     for m in synth.small_batch(seed=3, nmol=args.batch_mols):
         F.centre(m.xyz)
         mols.append((m.sig, m.eps, m.q, m.xyz, m.grid[0], m.box[0]))
+    n_total = len(mols)
+    if dist:
+        part = RP.partition_by_cost([RP.solve_cost(m[4] ** 3, len(m[2])) for m in mols], world)
+        mols = [mols[i] for i in part[rank]]
     parent = R.Solver((48, 48, 48), (24.0, 24.0, 24.0), precision=R.MIXED, device=dev,
                       stream=stream.cuda_stream)
     parent.set_solvent_obj(sv)
@@ -339,10 +354,15 @@ def run_batch(args, dev, stream):
     for c in ctxs.values():
         c.close()
     ok = sum(1 for r in res if r["status"] == 0)
-    return {"solves_per_s": len(mols) / s_batch, "n_mols": len(mols), "converged": ok,
-            "s_batch": s_batch, "loop_solves_per_s": len(sample) / s_loop,
+    dev_name = "cuda" if dist else None
+    rate = RP.job_rate(len(mols), s_batch, dev_name)
+    loop_rate = RP.job_rate(len(sample), s_loop, dev_name)
+    ok = int(RP.sum_over_ranks(ok, dev_name))
+    s_batch = RP.max_over_ranks(s_batch, dev_name)
+    return {"solves_per_s": rate, "n_mols": n_total, "converged": ok,
+            "s_batch": s_batch, "loop_solves_per_s": loop_rate,
             "loop_sample": len(sample),
-            "speedup_vs_loop": (len(mols) / s_batch) / (len(sample) / s_loop),
+            "speedup_vs_loop": rate / loop_rate,
             "solvent": "naclaq_vv.xvk (3-site water + 0.1 M NaCl), every 4th k row",
             "precision": "FP32 bulk + FP64 polish"}
 
