@@ -399,6 +399,90 @@ __global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a0) {
 }
 
 // ---------------------------------------------------------------- pass K
+// One mirror pair of k points: j (the owner, j < N/2, grid indices ix iy iz)
+// and jm = N-1-j with k(jm) = -k(j).  y/ym are the forward-transformed
+// packed site pairs at j and jm; out/outm receive the OZ result repacked
+// for the inverse transform.
+template <typename T, int V>
+__device__ __forceinline__ void kspace_pair(const IterArgs<T> &a, long long j, int ix, int iy,
+                                            int iz, const typename Cx<T>::t *y,
+                                            const typename Cx<T>::t *ym,
+                                            typename Cx<T>::t *out, typename Cx<T>::t *outm) {
+  typedef typename Cx<T>::t C;
+  constexpr int P = (V + 1) / 2;
+  const StageParams *sp = a.sp;
+  const int dir = ((ix + iy + iz) & 1) ? -1 : 1;
+  const double2 fk = a.fkh[j];
+  // unpack the site pairs and finish the forward transform
+  // (timeirvol * dv, fft3d.cu:32) and subtract q cf fk (mqvfk)
+  C F[V];
+  const T sc = (T)(a.dv * 0.5 * dir);
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const double qa = sp->qcf[2 * p];
+    F[2 * p] = mk<C>(sc * (y[p].x - ym[p].x) - qa * fk.x, sc * (y[p].y + ym[p].y) - qa * fk.y);
+    if (2 * p + 1 < V) {
+      const double qb = sp->qcf[2 * p + 1];
+      F[2 * p + 1] = mk<C>(sc * (y[p].y - ym[p].y) - qb * fk.x, -sc * (y[p].x + ym[p].x) - qb * fk.y);
+    }
+  }
+  // chi_ab(|k|) (solvent_spline.cu:36-47, applied per point by oz)
+  double X[V * V];
+  if (a.xs) {
+    // cubic cell: |k| = (pi/L) sqrt(s), s = sum of three odd squares
+    const int ox = 2 * ix - a.nx + 1, oy = 2 * iy - a.ny + 1, oz = 2 * iz - a.nz + 1;
+    const unsigned sq = (unsigned)(ox * ox + oy * oy + oz * oz);
+    const double2 *xr = reinterpret_cast<const double2 *>(a.xs + (size_t)((sq - 3u) >> 3) * V * V);
+#pragma unroll
+    for (int ab = 0; ab < V * V / 2; ++ab) {
+      const double2 q = xr[ab];
+      X[2 * ab] = q.x;
+      X[2 * ab + 1] = q.y;
+    }
+    if (V * V % 2) X[V * V - 1] = a.xs[(size_t)((sq - 3u) >> 3) * V * V + V * V - 1];
+  } else {
+    // general cell: natural spline on knots k_i = dk (i+1) with the
+    // bisection semantics of splint.cc:9-16 on uniform knots
+    const double kx = 2.0 * kPi * (ix - a.nx / 2.0 + 0.5) / a.bx;   // set_g
+    const double ky = 2.0 * kPi * (iy - a.ny / 2.0 + 0.5) / a.by;
+    const double kz = 2.0 * kPi * (iz - a.nz / 2.0 + 0.5) / a.bz;
+    const double kk = sqrt(kx * kx + ky * ky + kz * kz);
+    int k0 = (int)(kk / a.dk) - 1;
+    k0 = k0 < 0 ? 0 : (k0 > a.ntab - 2 ? a.ntab - 2 : k0);
+    while (k0 < a.ntab - 2 && a.dk * (k0 + 2) <= kk) ++k0;
+    while (k0 > 0 && a.dk * (k0 + 1) > kk) --k0;
+    const double tt = kk - a.dk * (k0 + 1);
+    const double2 *cf = reinterpret_cast<const double2 *>(a.chi + (size_t)k0 * V * V * 4);
+#pragma unroll
+    for (int ab = 0; ab < V * V; ++ab) {
+      const double2 lo = cf[2 * ab], hi2 = cf[2 * ab + 1];
+      X[ab] = ((hi2.y * tt + hi2.x) * tt + lo.y) * tt + lo.x;
+    }
+  }
+  C H[V];
+#pragma unroll
+  for (int va = 0; va < V; ++va) {
+    T hr = 0, hi = 0;
+#pragma unroll
+    for (int vb = 0; vb < V; ++vb) {
+      const T x = (T)X[va * V + vb];
+      hr += F[vb].x * x;                       // oz, calculate_cuda.cu:44-58
+      hi += F[vb].y * x;
+    }
+    H[va] = mk<C>(hr, hi);
+  }
+  // repack for the inverse: dir (h_a + i h_b) at k and its mirror
+  // (timeirvol before the inverse, fft3d.cu:34)
+  const T d = (T)dir;
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const C ha = H[2 * p];
+    const C hb = (2 * p + 1 < V) ? H[2 * p + 1] : mk<C>(0.0, 0.0);
+    out[p] = mk<C>(d * (ha.x - hb.y), d * (ha.y + hb.x));
+    outm[p] = mk<C>(-d * (ha.x + hb.y), -d * (hb.x - ha.y));
+  }
+}
+
 template <typename T, int V>
 __global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a0) {
   const IterArgs<T> a = solute_view<T, V>(a0);
@@ -406,89 +490,27 @@ __global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a0) {
   constexpr int P = (V + 1) / 2;
   if (a.st->done) return;
   const long long n = a.n, nh = n / 2;
-  const StageParams *sp = a.sp;
   C *__restrict__ buf = a.buf;
-  const double2 *__restrict__ fkh = a.fkh;
-  const double *__restrict__ chi = a.chi;
   for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nh;
        j += (long long)gridDim.x * blockDim.x) {
     const long long jm = n - 1 - j;             // k(jm) = -k(j)
     int ix, iy, iz;
     split_index(j, a.fdx, a.fdy, ix, iy, iz);
-    const int dir = ((ix + iy + iz) & 1) ? -1 : 1;
-    const double2 fk = fkh[j];
-    // unpack the site pairs and finish the forward transform
-    // (timeirvol * dv, fft3d.cu:32) and subtract q cf fk (mqvfk)
-    C F[V];
-    const T sc = (T)(a.dv * 0.5 * dir);
+    C y[P], ym[P], o[P], om[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-      const C y = buf[(size_t)p * n + j];
-      const C ym = buf[(size_t)p * n + jm];
-      const double qa = sp->qcf[2 * p];
-      F[2 * p] = mk<C>(sc * (y.x - ym.x) - qa * fk.x, sc * (y.y + ym.y) - qa * fk.y);
-      if (2 * p + 1 < V) {
-        const double qb = sp->qcf[2 * p + 1];
-        F[2 * p + 1] = mk<C>(sc * (y.y - ym.y) - qb * fk.x, -sc * (y.x + ym.x) - qb * fk.y);
-      }
+      y[p] = buf[(size_t)p * n + j];
+      ym[p] = buf[(size_t)p * n + jm];
     }
-    // chi_ab(|k|) (solvent_spline.cu:36-47, applied per point by oz)
-    double X[V * V];
-    if (a.xs) {
-      // cubic cell: |k| = (pi/L) sqrt(s), s = sum of three odd squares
-      const int ox = 2 * ix - a.nx + 1, oy = 2 * iy - a.ny + 1, oz = 2 * iz - a.nz + 1;
-      const unsigned sq = (unsigned)(ox * ox + oy * oy + oz * oz);
-      const double2 *xr = reinterpret_cast<const double2 *>(a.xs + (size_t)((sq - 3u) >> 3) * V * V);
-#pragma unroll
-      for (int ab = 0; ab < V * V / 2; ++ab) {
-        const double2 q = xr[ab];
-        X[2 * ab] = q.x;
-        X[2 * ab + 1] = q.y;
-      }
-      if (V * V % 2) X[V * V - 1] = a.xs[(size_t)((sq - 3u) >> 3) * V * V + V * V - 1];
-    } else {
-      // general cell: natural spline on knots k_i = dk (i+1) with the
-      // bisection semantics of splint.cc:9-16 on uniform knots
-      const double kx = 2.0 * kPi * (ix - a.nx / 2.0 + 0.5) / a.bx;   // set_g
-      const double ky = 2.0 * kPi * (iy - a.ny / 2.0 + 0.5) / a.by;
-      const double kz = 2.0 * kPi * (iz - a.nz / 2.0 + 0.5) / a.bz;
-      const double kk = sqrt(kx * kx + ky * ky + kz * kz);
-      int k0 = (int)(kk / a.dk) - 1;
-      k0 = k0 < 0 ? 0 : (k0 > a.ntab - 2 ? a.ntab - 2 : k0);
-      while (k0 < a.ntab - 2 && a.dk * (k0 + 2) <= kk) ++k0;
-      while (k0 > 0 && a.dk * (k0 + 1) > kk) --k0;
-      const double tt = kk - a.dk * (k0 + 1);
-      const double2 *cf = reinterpret_cast<const double2 *>(chi + (size_t)k0 * V * V * 4);
-#pragma unroll
-      for (int ab = 0; ab < V * V; ++ab) {
-        const double2 lo = cf[2 * ab], hi2 = cf[2 * ab + 1];
-        X[ab] = ((hi2.y * tt + hi2.x) * tt + lo.y) * tt + lo.x;
-      }
-    }
-    C H[V];
-#pragma unroll
-    for (int va = 0; va < V; ++va) {
-      T hr = 0, hi = 0;
-#pragma unroll
-      for (int vb = 0; vb < V; ++vb) {
-        const T x = (T)X[va * V + vb];
-        hr += F[vb].x * x;                       // oz, calculate_cuda.cu:44-58
-        hi += F[vb].y * x;
-      }
-      H[va] = mk<C>(hr, hi);
-    }
-    // repack for the inverse: dir (h_a + i h_b) at k and its mirror
-    // (timeirvol before the inverse, fft3d.cu:34)
-    const T d = (T)dir;
+    kspace_pair<T, V>(a, j, ix, iy, iz, y, ym, o, om);
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-      const C ha = H[2 * p];
-      const C hb = (2 * p + 1 < V) ? H[2 * p + 1] : mk<C>(0.0, 0.0);
-      buf[(size_t)p * n + j] = mk<C>(d * (ha.x - hb.y), d * (ha.y + hb.x));
-      buf[(size_t)p * n + jm] = mk<C>(-d * (ha.x + hb.y), -d * (hb.x - ha.y));
+      buf[(size_t)p * n + j] = o[p];
+      buf[(size_t)p * n + jm] = om[p];
     }
   }
 }
+
 
 // ---------------------------------------------------------------- pass R
 __device__ void finalize_block(DevState *st, const double *part, int nblocks,
