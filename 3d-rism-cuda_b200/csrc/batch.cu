@@ -4,7 +4,10 @@
 // them (solute = blockIdx.y), one batched cuFFT plan transforms all their
 // site pairs, each solute converges on its own device state word (a
 // finished solute's blocks idle), and the loop is the same captured graph.
+// Groups of different cells run concurrently: each group's child context
+// has its own stream and is driven from its own host thread.
 #include <map>
+#include <thread>
 #include <vector>
 
 #include "rism3d_impl.h"
@@ -37,12 +40,12 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
   // group by cell
   std::map<std::pair<int, double>, std::vector<int>> groups;
   for (int m = 0; m < nmol; ++m) groups[{grids[m], boxes[m]}].push_back(m);
-  int worst = RISM3D_OK;
+  // one child context per group, each on its own stream
+  std::vector<std::pair<Context *, const std::vector<int> *>> work;
   for (auto &kv : groups) {
     const int grid = kv.first.first;
     const double box = kv.first.second;
-    const std::vector<int> &mols = kv.second;
-    const int nb = (int)mols.size();
+    const int nb = (int)kv.second.size();
     Context *ch = nullptr;
     for (Context::Child &cc : p.children)
       if (cc.grid == grid && cc.box == box && cc.nb == nb) ch = cc.ctx;
@@ -50,7 +53,7 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
       rism3d_params cp = p.prm;
       cp.grid[0] = cp.grid[1] = cp.grid[2] = grid;
       cp.box[0] = cp.box[1] = cp.box[2] = box;
-      cp.stream = p.stream;          // children run on the parent's stream
+      cp.stream = nullptr;           // its own stream: groups run concurrently
       cp.verbose = 0;
       ch = new Context;
       std::string err;
@@ -64,10 +67,23 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
         delete ch;
         return rc;
       }
-      ch->own_stream = false;
       p.children.push_back({grid, nb, box, ch});
     }
-    // concatenate the group's atoms
+    work.push_back({ch, &kv.second});
+  }
+  // work queued on the caller's stream before this call comes first
+  cudaEvent_t start = nullptr;
+  if (!cuda_ok(p, cudaEventCreateWithFlags(&start, cudaEventDisableTiming), "batch") ||
+      !cuda_ok(p, cudaEventRecord(start, p.stream), "batch"))
+    return RISM3D_CUDA_ERROR;
+  // each group on its own host thread: potentials, solve, observables
+  std::vector<int> rcs(work.size(), RISM3D_OK);
+  auto run_group = [&](size_t gi) {
+    Context *ch = work[gi].first;
+    const std::vector<int> &mols = *work[gi].second;
+    const int nb = (int)mols.size();
+    cudaSetDevice(p.dev);
+    cudaStreamWaitEvent(ch->stream, start, 0);
     std::vector<int> cnt(nb);
     std::vector<double> s, e, qq, r;
     for (int b = 0; b < nb; ++b) {
@@ -92,11 +108,26 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
       if (rc == RISM3D_OK) rc = compute_atom_integrals(*ch, false);
       cudaEventRecord(ch->tm_obs.b, ch->stream);
     }
-    if (rc != RISM3D_OK) {
-      p.err = ch->err;
-      return rc;
+    if (rc == RISM3D_OK && cudaStreamSynchronize(ch->stream) != cudaSuccess) {
+      ch->err = "batch group: stream failed";
+      rc = RISM3D_CUDA_ERROR;
     }
-    cudaStreamSynchronize(ch->stream);
+    rcs[gi] = rc;
+  };
+  std::vector<std::thread> threads;
+  for (size_t gi = 1; gi < work.size(); ++gi) threads.emplace_back(run_group, gi);
+  if (!work.empty()) run_group(0);
+  for (std::thread &t : threads) t.join();
+  cudaEventDestroy(start);
+  int worst = RISM3D_OK;
+  for (size_t gi = 0; gi < work.size(); ++gi) {
+    Context *ch = work[gi].first;
+    if (rcs[gi] != RISM3D_OK) {
+      p.err = ch->err;
+      return rcs[gi];
+    }
+    const std::vector<int> &mols = *work[gi].second;
+    const int nb = (int)mols.size();
     float ms_s = 0, ms_i = 0, ms_o = 0;
     cudaEventElapsedTime(&ms_s, ch->tm_setup.a, ch->tm_setup.b);
     cudaEventElapsedTime(&ms_i, ch->tm_iter.a, ch->tm_iter.b);
@@ -105,7 +136,7 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
       rism3d_result rr = nb == 1 ? ch->res : ch->bres[b];
       if (nb == 1) { rr.iterations = ch->res.iterations; rr.status = ch->res.status; }
       rr.natv = p.natv;
-      rr.natom = cnt[b];
+      rr.natom = natoms[mols[b]];
       rr.ms_setup = ms_s;                        // group totals
       rr.ms_iterate = ms_i;
       rr.ms_observe = ms_o;
