@@ -126,6 +126,10 @@ k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
             acc[k][v] += p.y * s6 * (s6 - 1.0);
           }
         }
+        if (r2 >= 1600.0) {                 // r >= 40 A: e^-r is below FP64 resolution
+          afr[k] += at.w * ri;
+          continue;
+        }
         const double ra = r2 > 0.0 ? r2 * ri : 0.0;
         if (ra >= 1.0e-5) {                 // cal_Coulomb.cu:114-120
           const double qr = at.w * ri;
@@ -182,24 +186,33 @@ __global__ void k_phase_rows(int nx, int ny, int nz, double bx, double by, doubl
 }
 
 // fk on the owner half j < N/2 (cal_Coulomb.cu:125-149): the phase
-// e^{-ik.R} is the product of the three per-axis rows.
+// e^{-ik.R} is the product of the three per-axis rows.  A block covers whole
+// x rows (or one row segment when nx > blockDim): per atom tile, the y-z
+// phase product of each of the block's rows is formed once in shared memory,
+// and each thread adds q e^{-i kx X} (yz) with one coalesced row load.
+constexpr int kRowsMax = 10;    // rows a block of min(256, 8 nx) points can touch
+
 __global__ void __launch_bounds__(kThreads)
 k_potential_k(int nx, int ny, int nz, double bx, double by, double bz,
               const double *__restrict__ atoms_all, const int *__restrict__ aoff,
               const int *__restrict__ acnt, double ubeta,
               const double2 *__restrict__ ph_all, double2 *__restrict__ fkh) {
   __shared__ double sq[kTile];
+  __shared__ double2 syz[kRowsMax][kTile];
   const long long nh = (long long)nx * ny * nz / 2;
   const int sb = blockIdx.y;
   const double *__restrict__ atoms = atoms_all + 8 * (size_t)aoff[sb];
   const int natom = acnt[sb];
   const double2 *__restrict__ ph = ph_all + (size_t)aoff[sb] * (nx + ny + nz);
   fkh += (size_t)sb * nh;
-  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long jj = j < nh ? j : 0;
+  const long long jb = (long long)blockIdx.x * blockDim.x;      // first point of the block
+  const long long j = jb + threadIdx.x;
+  const long long jj = j < nh ? j : nh - 1;
   const int ix = (int)(jj % nx);
-  const long long r = jj / nx;
-  const int iy = (int)(r % ny), iz = (int)(r / ny);
+  const long long row = jj / nx, row0 = jb / nx;
+  const int lrow = (int)(row - row0);                           // row within the block
+  const int nrows = (int)(min(nh - 1, jb + (long long)blockDim.x - 1) / nx - row0) + 1;
+  const int iy = (int)(row % ny), iz = (int)(row / ny);
   const double kx = 2.0 * kPi * (ix - nx / 2.0 + 0.5) / bx;
   const double ky = 2.0 * kPi * (iy - ny / 2.0 + 0.5) / by;
   const double kz = 2.0 * kPi * (iz - nz / 2.0 + 0.5) / bz;
@@ -208,18 +221,23 @@ k_potential_k(int nx, int ny, int nz, double bx, double by, double bz,
   const int L = nx + ny + nz;
   double re = 0.0, im = 0.0;
   for (int t0 = 0; t0 < natom; t0 += kTile) {
+    const int m = min(kTile, natom - t0);
     __syncthreads();
-    for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
-      const int ia = t0 + i;
-      sq[i] = ia < natom ? 4.0 * kPi * atoms[8 * (size_t)ia + 3] : 0.0;
+    for (int i = threadIdx.x; i < kTile; i += blockDim.x)
+      sq[i] = i < m ? 4.0 * kPi * atoms[8 * (size_t)(t0 + i) + 3] : 0.0;
+    for (int e = threadIdx.x; e < nrows * m; e += blockDim.x) {
+      const int r = e / m, i = e - r * m;
+      const long long rw = row0 + r;
+      const int y = (int)(rw % ny), z = (int)(rw / ny);
+      const double2 *rowp = ph + (size_t)(t0 + i) * L;
+      const double2 py = rowp[nx + y], pz = rowp[nx + ny + z];
+      syz[r][i] = make_double2(py.x * pz.x - py.y * pz.y, py.x * pz.y + py.y * pz.x);
     }
     __syncthreads();
-    const int m = min(kTile, natom - t0);
     for (int i = 0; i < m; ++i) {
-      const double2 *row = ph + (size_t)(t0 + i) * L;
-      const double2 px = row[ix], py = row[nx + iy], pz = row[nx + ny + iz];
-      const double yzr = py.x * pz.x - py.y * pz.y, yzi = py.x * pz.y + py.y * pz.x;
-      const double cr = px.x * yzr - px.y * yzi, ci = px.x * yzi + px.y * yzr;
+      const double2 px = ph[(size_t)(t0 + i) * L + ix];
+      const double2 yz = syz[lrow][i];
+      const double cr = px.x * yz.x - px.y * yz.y, ci = px.x * yz.y + px.y * yz.x;
       re += sq[i] * cr;      // + 4 pi q cos(k.R)
       im += sq[i] * ci;      // - 4 pi q sin(k.R)
     }
@@ -286,8 +304,9 @@ int compute_potentials(Context &c) {
     return RISM3D_CUDA_ERROR;
   k_phase_rows<<<(unsigned)((L * c.natom + 255) / 256), 256, 0, c.stream>>>(
       c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], c.d_atoms, c.natom, ph);
-  long long blocks = (c.n / 2 + kThreads - 1) / kThreads;
-  k_potential_k<<<dim3((unsigned)blocks, c.nb), kThreads, 0, c.stream>>>(
+  const int thr = c.nx >= 32 ? kThreads : 8 * c.nx;        // at most kRowsMax rows per block
+  long long blocks = (c.n / 2 + thr - 1) / thr;
+  k_potential_k<<<dim3((unsigned)blocks, c.nb), thr, 0, c.stream>>>(
       c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], c.d_atoms,
       c.d_atom_off, c.d_atom_cnt, ubeta, ph, c.d_fkh);
   cudaFreeAsync(ph, c.stream);

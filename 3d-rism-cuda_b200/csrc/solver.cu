@@ -79,6 +79,7 @@ struct IterArgs {
   unsigned *count;          // blocks of pass R done (reset by the last one)
   double *hist;             // per-iteration rms (single solves, verbose) or null
   int hist_cap;
+  int nofk;                 // refinement: q cf fk cancels, fk is not read
 };
 
 // Batched solves: blockIdx.y selects the solute; every per-solute array is
@@ -412,7 +413,7 @@ __device__ __forceinline__ void kspace_pair(const IterArgs<T> &a, long long j, i
   constexpr int P = (V + 1) / 2;
   const StageParams *sp = a.sp;
   const int dir = ((ix + iy + iz) & 1) ? -1 : 1;
-  const double2 fk = a.fkh[j];
+  const double2 fk = a.nofk ? make_double2(0.0, 0.0) : a.fkh[j];
   // unpack the site pairs and finish the forward transform
   // (timeirvol * dv, fft3d.cu:32) and subtract q cf fk (mqvfk)
   C F[V];
@@ -985,7 +986,7 @@ int run_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
               const T *R0 = nullptr) {
   IterArgs<T> a = make_args<T>(c, sizeof(T) == 8);
   a.buf = buf; a.t = t; a.U = U; a.Y = Y; a.RP = RP;
-  if (REF) { a.R0 = R0; a.sp = c.d_stage_ref; }
+  if (REF) { a.R0 = R0; a.sp = c.d_stage_ref; a.nofk = 1; }
   a.hout = snapshot ? c.d_h : nullptr;
   a.gout = snapshot ? c.d_g : nullptr;
   a.tw = (const typename Cx<T>::t *)(sizeof(T) == 8 ? (void *)c.d_tw : (void *)c.d_twf);
