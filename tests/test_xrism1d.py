@@ -50,3 +50,36 @@ def test_bad_input_is_an_error():
         X.solve(rows, 298.0, ntab=1000, dr=0.05)          # not a power of two
     with pytest.raises(RismError):
         X.solve([rows[0][:9] + (-1.0,)], 298.0, ntab=256)  # negative density
+
+
+def test_cli_writes_a_table_the_3d_reader_accepts(tmp_path):
+    """bin/rism1d-b200 on a sites file: the written .xvk parses with the
+    reference's reader layout and equals the library call's table."""
+    import subprocess
+    from conftest import ROOT
+    from rism3d_b200 import xrism1d as X
+    rows, T, ntab, dr = X.read_sites(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    sites = tmp_path / "water.sites"
+    sites.write_text("# name spc sym sigma eps q x y z density\n" +
+                     "\n".join(" ".join(str(v) for v in r) for r in rows) + "\n")
+    out = tmp_path / "water_vv.xvk"
+    exe = os.path.join(ROOT, "3d-rism-cuda_b200", "bin", "rism1d-b200")
+    p = subprocess.run([exe, "-T", str(T), "-n", "1024", "-r", "0.1", "-e", "1e-10",
+                        str(sites), str(out)], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    back = F.read_xvk(str(out))
+    xvv, xt, _ = X.solve(rows, T, 1024, 0.1, convergence=1e-10)
+    assert back.ntab == 1024 and back.natv == 2
+    assert np.abs(back.xvv - xvv).max() < 1e-12
+    assert abs(back.xt - xt) < 1e-8 * xt
+
+
+def test_hnc_closure_converges_for_water():
+    """The HNC closure (no linearisation of exp) on the same water model:
+    converges, and its X(k) differs from KH only where g is large."""
+    from rism3d_b200 import xrism1d as X
+    rows, T, ntab, dr = X.read_sites(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    kh, xt_kh, _ = X.solve(rows, T, 1024, 0.1, closure=X.KH, convergence=1e-9)
+    hnc, xt_hnc, _ = X.solve(rows, T, 1024, 0.1, closure=X.HNC, convergence=1e-9)
+    assert np.all(np.isfinite(hnc)) and xt_hnc > 0
+    assert np.abs(hnc[:, :, -200:] - kh[:, :, -200:]).max() < 1e-2   # large k: intramolecular
