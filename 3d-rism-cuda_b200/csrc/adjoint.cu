@@ -36,7 +36,10 @@
 // pair term recomputed (cal_LJ.cu:57-71, cal_Coulomb.cu:109-121), and through
 // the k-space fk kernel with per-axis phase rows.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "rism3d_impl.h"
@@ -546,6 +549,8 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
   if (rc != RISM3D_OK) return rc;
   k_gprime<<<gt, kThreads, 0, c.stream>>>(tot, c.prm.closure, c.d_t, c.d_U, G);
   c.launches += 1;
+  static const bool trace = getenv("RISM3D_TRACE") && getenv("RISM3D_TRACE")[0] == '1';
+  const auto w0 = std::chrono::steady_clock::now();
   // Anderson-accelerated solve of G xi - (G - 1) L xi = (G - 1) w from xi = 0
   cudaMemsetAsync(xi, 0, sizeof(double) * tot, c.stream);
   cudaMemsetAsync(xs, 0, sizeof(double) * kDepth * tot, c.stream);
@@ -591,6 +596,7 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
     slot = (slot + 1) % kDepth;
   }
   if (it == maxit) { c.err = "adjoint solve did not converge"; return RISM3D_NOT_CONVERGED; }
+  const auto w1 = std::chrono::steady_clock::now();
   // weights from zeta; L xi is current (the loop leaves right after applyL)
   double *W = xs;                               // history no longer needed
   SiteW sv{};
@@ -637,6 +643,12 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
       !cuda_ok(c, cudaMemcpyAsync(hk.data(), sum_k, sizeof(double) * hk.size(), cudaMemcpyDeviceToHost, c.stream), "adjoint") ||
       !cuda_ok(c, cudaStreamSynchronize(c.stream), "adjoint"))
     return RISM3D_CUDA_ERROR;
+  if (trace) {
+    const auto w2 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[rism3d] adjoint: %d Anderson steps %.1f ms, back-projection %.1f ms\n", it,
+            std::chrono::duration<double, std::milli>(w1 - w0).count(),
+            std::chrono::duration<double, std::milli>(w2 - w1).count());
+  }
   // the charge-up factor of the last stage is already in the site charges
   for (int u = 0; u < A; ++u) {
     const double *o = &hr[(size_t)u * NOUT], *kk = &hk[(size_t)u * 4];

@@ -199,11 +199,16 @@ k_atom_integrals(int nx, int ny, int nz, double drx, double dry, double drz,
 // layout as k_atom_integrals with GRAD = 0.  Coordinates are carried as FP32
 // (hi, lo) pairs, so dx = (x_hi - X_hi) + (x_lo - X_lo) is accurate to FP32
 // relative precision of dx itself without any FP64 work in the pair loop.
-// The cutoff r < sigma/2 is tested on r^2; points within 2e-5 of a cutoff
-// re-test in FP64.  Each thread carries NA_T atoms (block: NA_T x 128
-// atoms) for independent work per shared-memory point.
+// Per site the loop accumulates g (s/r)^6 ((s/r)^6 - 1) and g / r; the
+// factors 4 eps_uv and q_u q_v cc are applied per tile in FP64.  The cutoff
+// r < sigma/2 zeroes g (r^2 is clamped at 1e-4 so the masked terms stay
+// finite; every unmasked point lies beyond the smallest cutoff, 0.1 A);
+// points within 2e-5 of a cutoff re-test it in FP64.  Each thread carries
+// NA_T atoms; grid points come through shared memory in tiles of kSeTile.
+constexpr int kSeTile = 512;
+
 template <int V, int NA_T>
-__global__ void __launch_bounds__(kAtomsPerBlock, 4)
+__global__ void __launch_bounds__(kAtomsPerBlock, V <= 5 ? 4 : 2)
 k_atom_se32(int nx, int ny, int nz, double drx, double dry, double drz,
             const double *__restrict__ g, const double *__restrict__ atoms_all,
             const int *__restrict__ aoff, const int *__restrict__ acnt, int natom_tot,
@@ -213,14 +218,15 @@ k_atom_se32(int nx, int ny, int nz, double drx, double dry, double drz,
   const double *__restrict__ atoms = atoms_all + 8 * (size_t)aoff[sb];
   const int natom = acnt[sb];
   g += (size_t)sb * V * (size_t)nx * ny * nz;
-  __shared__ float4 ph[kPtsTile];           // x_hi y_hi z_hi
-  __shared__ float4 pl[kPtsTile];           // x_lo y_lo z_lo
-  __shared__ float pg[V][kPtsTile];
+  __shared__ float4 ph[kSeTile];            // x_hi y_hi z_hi
+  __shared__ float4 pl[kSeTile];            // x_lo y_lo z_lo
+  __shared__ float pg[V][kSeTile];
   const long long n = (long long)nx * ny * nz;
   int ia[NA_T];
   bool live[NA_T], any = false;
   float Xh[NA_T], Yh[NA_T], Zh[NA_T], Xl[NA_T], Yl[NA_T], Zl[NA_T];
-  float s6v[NA_T][V], e4[NA_T][V], qq[NA_T][V], hs2[NA_T][V];
+  float s6v[NA_T][V], hs2[NA_T][V], blo[NA_T][V], bhi[NA_T][V];
+  double e4[NA_T][V], qq[NA_T][V];
 #pragma unroll
   for (int a = 0; a < NA_T; ++a) {
     ia[a] = blockIdx.x * kAtomsPerBlock * NA_T + a * kAtomsPerBlock + threadIdx.x;
@@ -238,9 +244,11 @@ k_atom_se32(int nx, int ny, int nz, double drx, double dry, double drz,
       const double sg = (su + sv.sig[v]) * 0.5;  // cal_LJ.cu:28
       const double sg2 = sg * sg;
       s6v[a][v] = (float)(sg2 * sg2 * sg2);
-      e4[a][v] = (float)(4.0 * sqrt(eu * sv.eps[v]));
-      qq[a][v] = (float)(qu * sv.q[v] * cc);
+      e4[a][v] = 4.0 * sqrt(eu * sv.eps[v]);
+      qq[a][v] = qu * sv.q[v] * cc;
       hs2[a][v] = (float)(0.25 * sg2);
+      blo[a][v] = (float)(0.25 * sg2 * (1.0 - 2.0e-5));
+      bhi[a][v] = (float)(0.25 * sg2 * (1.0 + 2.0e-5));
     }
   }
   double acc[NA_T][2 * V];
@@ -250,9 +258,9 @@ k_atom_se32(int nx, int ny, int nz, double drx, double dry, double drz,
     for (int k = 0; k < 2 * V; ++k) acc[a][k] = 0.0;
   const long long j0 = (long long)blockIdx.y * chunk;
   const long long j1 = min(n, j0 + chunk);
-  for (long long base = j0; base < j1; base += kPtsTile) {
+  for (long long base = j0; base < j1; base += kSeTile) {
     __syncthreads();
-    for (int i = threadIdx.x; i < kPtsTile; i += blockDim.x) {
+    for (int i = threadIdx.x; i < kSeTile; i += blockDim.x) {
       const long long j = base + i;
       if (j < j1) {
         const long long r = j / nx;
@@ -273,7 +281,7 @@ k_atom_se32(int nx, int ny, int nz, double drx, double dry, double drz,
     }
     __syncthreads();
     if (!any) continue;
-    const int m = (int)min((long long)kPtsTile, j1 - base);
+    const int m = (int)min((long long)kSeTile, j1 - base);
     float tl[NA_T][2 * V];
 #pragma unroll
     for (int a = 0; a < NA_T; ++a)
@@ -290,32 +298,32 @@ k_atom_se32(int nx, int ny, int nz, double drx, double dry, double drz,
         const float dy = (h.y - Yh[a]) + (l.y - Yl[a]);
         const float dz = (h.z - Zh[a]) + (l.z - Zl[a]);
         const float r2 = dx * dx + dy * dy + dz * dz;
-        const float ri = rsqrtf(r2);
+        const float ri = rsqrtf(fmaxf(r2, 1.0e-4f));
         const float ir2 = ri * ri;
         const float ir6 = ir2 * ir2 * ir2;
 #pragma unroll
         for (int v = 0; v < V; ++v) {
           bool inside = r2 < hs2[a][v];
-          if (fabsf(r2 - hs2[a][v]) < 2.0e-5f * hs2[a][v]) {   // rare: exact test
+          if (r2 > blo[a][v] && r2 < bhi[a][v]) {   // rare: exact test
             const double *p = atoms + 8 * (size_t)ia[a];
             const double ex = ((double)h.x + l.x) - p[0], ey = ((double)h.y + l.y) - p[1],
                          ez = ((double)h.z + l.z) - p[2];
             inside = sqrt(ex * ex + ey * ey + ez * ez) < (p[4] + sv.sig[v]) * 0.25;
           }
+          const float w = inside ? 0.0f : gv[v];
           const float rs6i = s6v[a][v] * ir6;
-          const float lj = e4[a][v] * rs6i * (rs6i - 1.0f) * gv[v];
-          const float es = qq[a][v] * ri * gv[v];
-          // cutoff r < sigma/2 (selects, so r = 0 with its infinite terms
-          // inside the cutoff contributes exactly 0)
-          tl[a][v] += inside ? 0.0f : lj;
-          tl[a][V + v] += inside ? 0.0f : es;
+          tl[a][v] = fmaf(w, rs6i * (rs6i - 1.0f), tl[a][v]);
+          tl[a][V + v] = fmaf(w, ri, tl[a][V + v]);
         }
       }
     }
 #pragma unroll
     for (int a = 0; a < NA_T; ++a)
 #pragma unroll
-      for (int k = 0; k < 2 * V; ++k) acc[a][k] += (double)tl[a][k];
+      for (int v = 0; v < V; ++v) {
+        acc[a][v] += e4[a][v] * (double)tl[a][v];
+        acc[a][V + v] += qq[a][v] * (double)tl[a][V + v];
+      }
   }
 #pragma unroll
   for (int a = 0; a < NA_T; ++a) {
@@ -393,8 +401,9 @@ int atoms_v(Context &c, bool forces) {
   const int A = c.natom;            // all solutes
   int amax = 0;
   for (int x : c.atom_cnt) amax = std::max(amax, x);
-  // FP32 SE (mixed contexts, no forces): kSeAtoms atoms per thread
-  constexpr int kSeAtoms = V <= 4 ? 2 : 1;
+  // FP32 SE (mixed contexts, no forces): kSeAtoms atoms per thread (two for
+  // up to 2 sites: more would spill under the 4-blocks-per-SM bound)
+  constexpr int kSeAtoms = V <= 2 ? 2 : 1;
   const bool se32 = !forces && c.prm.precision == RISM3D_MIXED;
   const int per_block = kAtomsPerBlock * (se32 ? kSeAtoms : 1);
   const int tiles = (amax + per_block - 1) / per_block;
@@ -402,7 +411,8 @@ int atoms_v(Context &c, bool forces) {
   int nchunk = (148 * 8 + tiles * c.nb - 1) / (tiles * c.nb);
   if (nchunk < 1) nchunk = 1;
   long long chunk = (c.n + nchunk - 1) / nchunk;
-  chunk = ((chunk + kPtsTile - 1) / kPtsTile) * kPtsTile;
+  const int tile = se32 ? kSeTile : kPtsTile;
+  chunk = ((chunk + tile - 1) / tile) * tile;
   nchunk = (int)((c.n + chunk - 1) / chunk);
   size_t need = (size_t)nchunk * A * NA + (size_t)A * NA;
   if ((int)need > c.natom_part_cap) {
