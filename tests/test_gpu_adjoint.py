@@ -122,10 +122,13 @@ def test_autograd_function_routes_backward_through_the_adjoint(tight):
 def test_protein_scale_gradients_match_central_differences():
     """The 846-atom solute at 256^3 (KH), solves converged to 1e-11: adjoint
     d mu/dq of three seeded atoms against central differences (step 1e-4 e)
-    to 1e-5 relative, d mu/dx (step 1e-3 A) to 1e-3 relative -- the position
-    differences themselves move by ~1e-3 between steps of 1e-3 and 5e-3 A,
-    so that is their own accuracy -- and every atom's position gradient
-    against cal_grad forces (1%, the long-range mismatch term)."""
+    to 1e-5 relative; d mu/dx against central differences extrapolated to a
+    zero step.  The KH closure switches from e^x to 1 + x at x = 0, so mu is
+    only once differentiable in the positions and the position differences
+    carry an error linear in the step (measured ~5x larger at 5e-3 A than at
+    1e-3 A); 2 D(h) - D(2h) removes it, leaving 2e-4.  Every atom's position
+    gradient is also checked against cal_grad forces (1%: the long-range
+    mismatch term)."""
     case, _, _ = load_case("cfg2_protein846_kh", conv=1e-11)
     s = _solver(case)
     s.solve()
@@ -134,13 +137,17 @@ def test_protein_scale_gradients_match_central_differences():
     assert np.abs(dulj + due - dR).max() <= 1e-2 * np.abs(dR).max()
     rng = np.random.default_rng(4)
     atoms = rng.choice(len(case.q), 3, replace=False)
+
+    def dx(u, h):
+        xp, xm = case.xyz.copy(), case.xyz.copy()
+        xp[u, 0] += h; xm[u, 0] -= h
+        return (_mu(s, case, xyz=xp) - _mu(s, case, xyz=xm)) / (2 * h)
+
     for u in atoms:
         qp, qm = case.q.copy(), case.q.copy()
         qp[u] += 1e-4; qm[u] -= 1e-4
         fdq = (_mu(s, case, q=qp) - _mu(s, case, q=qm)) / 2e-4
         assert abs(fdq - dq[u]) <= 1e-5 * abs(fdq), (u, fdq, dq[u])
-        xp, xm = case.xyz.copy(), case.xyz.copy()
-        xp[u, 0] += 1e-3; xm[u, 0] -= 1e-3
-        fdx = (_mu(s, case, xyz=xp) - _mu(s, case, xyz=xm)) / 2e-3
-        assert abs(fdx - dR[u, 0]) <= 1e-3 * abs(fdx), (u, fdx, dR[u, 0])
+        fdx = 2.0 * dx(u, 1e-3) - dx(u, 2e-3)
+        assert abs(fdx - dR[u, 0]) <= 2e-4 * abs(fdx), (u, fdx, dR[u, 0])
     s.close()
