@@ -63,10 +63,10 @@ void free_device(Context &c) {
                   c.d_U, c.d_t, c.d_Y, c.d_RP, c.d_buf, c.d_h, c.d_g,
                   c.f_U, c.f_t, c.f_Y, c.f_RP, c.f_buf, c.f_R0, c.f_x0, c.d_part, c.d_state,
                   c.d_stage, c.d_stage_ref, c.d_obs, c.d_atom_part, c.chi.d_coef, c.d_xs,
-                  c.d_atom_off, c.d_atom_cnt};
+                  c.d_atom_off, c.d_atom_cnt, c.d_esp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  c.d_u = c.d_e = c.d_fr = nullptr; c.d_fkh = nullptr; c.d_atoms = nullptr;
+  c.d_u = c.d_e = c.d_fr = nullptr; c.d_fkh = nullptr; c.d_atoms = nullptr; c.d_esp = nullptr;
   c.d_tw = nullptr; c.d_twf = nullptr; c.d_U = c.d_t = c.d_Y = c.d_RP = nullptr;
   c.d_buf = nullptr; c.d_h = c.d_g = nullptr;
   c.f_U = c.f_t = c.f_Y = c.f_RP = nullptr; c.f_buf = nullptr; c.f_R0 = c.f_x0 = nullptr;
@@ -476,7 +476,36 @@ int rism3d_grad(rism3d_ctx *x, double *dq, double *dsig, double *deps, double *d
   Context &c = x->c;
   cudaSetDevice(c.dev);
   if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
+  if (c.d_esp) {
+    c.err = "gradients are not defined with an ESP cube potential (it does not follow the solute)";
+    return RISM3D_BAD_STATE;
+  }
   return compute_adjoint(c, dq, dsig, deps, dR);
+}
+
+int rism3d_set_esp(rism3d_ctx *x, const double *esp) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (c.nb != 1) { c.err = "an ESP cube is for single-solute contexts"; return RISM3D_BAD_STATE; }
+  if (!esp) {
+    if (c.d_esp) cudaFree(c.d_esp);
+    c.d_esp = nullptr;
+  } else {
+    if (!c.d_esp && !cuda_ok(c, cudaMalloc(&c.d_esp, sizeof(double) * c.n), "alloc esp"))
+      return RISM3D_CUDA_ERROR;
+    if (!cuda_ok(c, cudaMemcpyAsync(c.d_esp, esp, sizeof(double) * c.n, cudaMemcpyHostToDevice,
+                                    c.stream), "copy esp"))
+      return RISM3D_CUDA_ERROR;
+  }
+  if (!c.have_solute)
+    return cuda_ok(c, cudaStreamSynchronize(c.stream), "copy esp") ? RISM3D_OK : RISM3D_CUDA_ERROR;
+  int rc = compute_potentials(c);                 // the solute's grids follow at once
+  if (rc != RISM3D_OK) return rc;
+  if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "potentials")) return RISM3D_CUDA_ERROR;
+  c.solved = false;
+  c.have_forces = false;
+  return RISM3D_OK;
 }
 
 int rism3d_get_grid(rism3d_ctx *x, int which, double *host) {
@@ -532,8 +561,8 @@ int rism3d_initialize(rism3d_ctx **out, const char *control, const char *structu
                       int precision) {
   if (!out || !control) { g_create_err = "null argument"; return RISM3D_BAD_INPUT; }
   *out = nullptr;
-  if ((esp && *esp) || (hs && *hs)) {
-    g_create_err = "ESP cube and RMDFT inputs are not supported by this build";
+  if (hs && *hs) {
+    g_create_err = "RMDFT (hard-sphere file) is not supported by this build";
     return RISM3D_BAD_INPUT;
   }
   io::ControlFile cf;
@@ -568,6 +597,15 @@ int rism3d_initialize(rism3d_ctx **out, const char *control, const char *structu
   if (q0) for (double &v : q) v = 0.0;                        // solute.cu:45-49
   rc = rism3d_set_solvent(x, sf.natv, sf.rho.data(), sf.q.data(), sf.sig.data(), sf.eps.data(),
                           sf.temper, sf.xt, sf.ntab, sf.dr, sf.xvv.data());
+  if (rc == RISM3D_OK && esp && *esp) {                       // cal_Coulomb.cu:41-96
+    std::vector<double> cube;
+    if (!io::read_esp_cube(esp, p.grid, cube, err)) {
+      c.err = err;
+      rc = RISM3D_BAD_INPUT;
+    } else {
+      rc = rism3d_set_esp(x, cube.data());
+    }
+  }
   if (rc == RISM3D_OK)
     rc = rism3d_set_solute(x, (int)q.size(), cf.sig.data(), cf.eps.data(), q.data(), xyz.data());
   if (rc != RISM3D_OK) {

@@ -241,6 +241,48 @@ bool write_qv(const std::string &path, const int grid[3], const double dr[3],
   return (bool)o;
 }
 
+bool read_esp_cube(const std::string &path, const int grid[3], std::vector<double> &esp,
+                   std::string &err) {
+  std::ifstream in(path.c_str());
+  if (!in) { err = "Error during read esp file: " + path; return false; }
+  std::string line;
+  std::getline(in, line);
+  std::getline(in, line);
+  int natom = 0, di = 0;
+  double x0, y0, z0;
+  if (!(in >> natom >> x0 >> y0 >> z0 >> di)) {
+    err = "Error reading atom count and origin.";
+    return false;
+  }
+  int cnt[3];
+  double axis[3];
+  for (int d = 0; d < 3; ++d)
+    if (!(in >> cnt[d] >> axis[0] >> axis[1] >> axis[2])) {
+      err = "Error reading the cube axes of " + path;
+      return false;
+    }
+  if (cnt[0] != grid[0] || cnt[1] != grid[1] || cnt[2] != grid[2]) {
+    err = "Error. cube file doesn't match input.";
+    return false;
+  }
+  for (int i = 0; i < natom; ++i) {
+    int z;
+    double a, b, c, d;
+    if (!(in >> z >> a >> b >> c >> d)) { err = "Error reading the cube atoms of " + path; return false; }
+  }
+  const size_t nx = grid[0], ny = grid[1], nz = grid[2];
+  esp.assign(nx * ny * nz, 0.0);
+  for (size_t ix = 0; ix < nx; ++ix)
+    for (size_t iy = 0; iy < ny; ++iy)
+      for (size_t iz = 0; iz < nz; ++iz)
+        if (!(in >> esp[ix + nx * (iy + ny * iz)])) {
+          err = "short ESP cube " + path;
+          esp.clear();
+          return false;
+        }
+  return true;
+}
+
 bool write_tuv(const std::string &path, const int grid[3], int natv, const double *t, long long n) {
   std::ofstream o(path.c_str());
   if (!o) return false;

@@ -20,6 +20,8 @@
 // per-tile FP64 accumulation and the e^-r factor beyond 20 A in FP32 (there
 // it is below 2e-9, so fr keeps FP64 accuracy); fr itself, 1/r and the
 // sums stay FP64.
+#include <algorithm>
+
 #include "rism3d_impl.h"
 
 namespace rism3d {
@@ -281,6 +283,16 @@ int launch_potential_r(Context &c) {
   return RISM3D_OK;
 }
 
+// ESP cube in place of the point-charge potential (cal_Coulomb.cu:88-90):
+// e = esp hartree / (kB T), so the stored short-range part is esr = e - fr;
+// fr and fk keep the point-charge forms.
+__global__ void k_esp_esr(long long n, const double *__restrict__ esp, double ubeta,
+                          const double *__restrict__ fr, double *__restrict__ esr) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x)
+    esr[j] = esp[j] * ubeta - fr[j];
+}
+
 int compute_potentials(Context &c) {
   SiteLJ sl{};
   for (int v = 0; v < c.natv; ++v) { sl.sig[v] = c.sigv[v]; sl.eps[v] = c.epsv[v]; }
@@ -312,6 +324,13 @@ int compute_potentials(Context &c) {
   cudaFreeAsync(ph, c.stream);
   if (!cuda_ok(c, cudaGetLastError(), "k_potential_k")) return RISM3D_CUDA_ERROR;
   c.launches += 3;
+  if (c.d_esp && c.nb == 1) {
+    const long long eb = std::min<long long>((c.n + kThreads - 1) / kThreads, 148 * 16);
+    k_esp_esr<<<(unsigned)eb, kThreads, 0, c.stream>>>(
+        c.n, c.d_esp, kHartree / (kBoltzmann * c.temper), c.d_fr, c.d_e);
+    if (!cuda_ok(c, cudaGetLastError(), "k_esp_esr")) return RISM3D_CUDA_ERROR;
+    c.launches += 1;
+  }
   return RISM3D_OK;
 }
 

@@ -146,6 +146,7 @@ struct Context {
   double *d_u = nullptr;     // [V][N] beta u_LJ
   double *d_e = nullptr;     // [N]   beta sum q e^-r / r (short-range Coulomb)
   double *d_fr = nullptr;    // [N]   beta long-range part
+  double *d_esp = nullptr;   // [N]   ESP cube (Hartree/e) replacing the point-charge e, or null
   double2 *d_fkh = nullptr;  // [N/2] beta fk on the owner half of k space
   double *d_atoms = nullptr; // [A][8] x y z q sig eps pad (all solutes)
   int *d_atom_off = nullptr; // [nb] first atom of each solute

@@ -62,6 +62,11 @@ bool write_euv(const std::string &path, int natom, int natv, const double *euv);
 // output_qv.cu:7-36
 bool write_qv(const std::string &path, const int grid[3], const double dr[3],
               const double *qv_times_dv, long long n);
+// cal_Coulomb.cu:41-88: ESP cube (two comment lines; natom, origin and one
+// more number; three axis lines whose counts must equal `grid`; natom atom
+// lines; values with z fastest).  esp receives [N] values, x fastest, Hartree/e.
+bool read_esp_cube(const std::string &path, const int grid[3], std::vector<double> &esp,
+                   std::string &err);
 // write_tuv.cu:7-33 / read_tuv.cu:6-34
 bool write_tuv(const std::string &path, const int grid[3], int natv, const double *t, long long n);
 bool read_tuv(const std::string &path, const int grid[3], int natv, std::vector<double> &t,

@@ -25,7 +25,8 @@ EXPORTS = ["rism3d_create", "rism3d_set_solvent", "rism3d_set_solute", "rism3d_s
            "rism3d_solve", "rism3d_euv", "rism3d_forces", "rism3d_grad", "rism3d_get_grid",
            "rism3d_solve_batch", "rism3d_destroy", "rism3d_last_error",
            "rism3d_initialize", "rism3d_iterate", "rism3d_output",
-           "rism3d_refresh_potentials", "rism3d_kernel_launches", "rism3d_time_kernel"]
+           "rism3d_refresh_potentials", "rism3d_kernel_launches", "rism3d_time_kernel",
+           "rism3d_set_esp"]
 
 
 class RismError(RuntimeError):
@@ -94,6 +95,7 @@ def lib():
         L.rism3d_iterate.argtypes = [vp, C.c_int]
         L.rism3d_output.argtypes = [vp]
         L.rism3d_refresh_potentials.argtypes = [vp]
+        L.rism3d_set_esp.argtypes = [vp, d]
         L.rism3d_kernel_launches.argtypes = [vp]
         L.rism3d_kernel_launches.restype = C.c_longlong
         L.rism3d_time_kernel.argtypes = [vp, C.c_int, C.c_int, d]
@@ -154,6 +156,12 @@ class Solver:
         sig, eps, q, xyz = _f64(sig), _f64(eps), _f64(q), _f64(np.asarray(xyz).reshape(-1, 3))
         self._check(lib().rism3d_set_solute(self.h, len(q), _dp(sig), _dp(eps), _dp(q), _dp(xyz)))
         self.natom = len(q)
+
+    def set_esp(self, esp):
+        """ESP cube values [N] (Hartree/e, x fastest) replacing the point-charge
+        potential in the closure; None removes it (rism3d_set_esp)."""
+        self._keep_esp = None if esp is None else _f64(np.asarray(esp).ravel())
+        self._check(lib().rism3d_set_esp(self.h, _dp(self._keep_esp)))
 
     def set_tuv(self, t):
         self._keep_t = None if t is None else _f64(t)

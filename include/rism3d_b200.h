@@ -146,6 +146,14 @@ int rism3d_forces(rism3d_ctx *ctx, double *dulj, double *due);
 int rism3d_grad(rism3d_ctx *ctx, double *dmu_dq, double *dmu_dsig,
                 double *dmu_deps, double *dmu_dR);
 
+/* ESP cube potential (cal_Coulomb.cu:41-96, the reference's -e input):
+ * esp[N] in Hartree/e on the cell grid, x fastest, replaces the point-charge
+ * Coulomb potential e that enters the closure (e = esp hartree / (kB T));
+ * the long-range fr / fk stay the point-charge forms, as in the reference.
+ * NULL removes it.  Applies to the current solute at once and to every
+ * later one; rism3d_grad refuses while it is set.  Single-solute contexts. */
+int rism3d_set_esp(rism3d_ctx *ctx, const double *esp);
+
 /* Recompute the potential grids from the solute already on the device
  * (no host->device traffic); the next rism3d_solve starts from them. */
 int rism3d_refresh_potentials(rism3d_ctx *ctx);
@@ -209,8 +217,10 @@ const char *rism3d_last_error(const rism3d_ctx *ctx);
  * rism3d_initialize == RISM3D::initialize(control, structure, esp, hs,
  * centering, q0) (initialize.cu:4-13): reads the .inp (and optional
  * structure file), the .xvk named in it, centres the solute, zeroes the
- * charges when q0, and computes the potential grids.  esp (ESP cube) and
- * hs (RMDFT hard-sphere file) must be NULL or "" in this build.
+ * charges when q0, and computes the potential grids.  esp names an ESP
+ * cube (NULL or "" for none; its grid must equal the control file's, else
+ * BAD_INPUT with the reference's message); hs (RMDFT hard-sphere file) must
+ * be NULL or "" in this build.
  * `device` selects the GPU (main.cu -d) and `precision` the arithmetic. */
 int rism3d_initialize(rism3d_ctx **ctx, const char *control,
                       const char *structure, const char *esp, const char *hs,

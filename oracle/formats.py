@@ -7,6 +7,7 @@ parsers:
 * control file ``.inp`` / structure file   -- read_input.cu:21-89
 * solute centring                          -- solute.cu:13-43
 * solvent susceptibility file ``.xvk``     -- solvent_read.cc:10-86
+* ESP cube ``-e``                          -- cal_Coulomb.cu:41-88
 * physical constants                       -- physical.h:4-17
 """
 from __future__ import annotations
@@ -141,6 +142,29 @@ def read_xvk(path: str) -> Solvent:
     xvv = np.array([float(x) for x in data[:need]]).reshape(ntab, natv, natv)
     xvv = np.ascontiguousarray(xvv.transpose(1, 2, 0))
     return Solvent(natv, rhov, qv, sigv, epsv, temper, xt, ntab, dr, xvv, sites)
+
+
+def read_esp_cube(path: str, grid) -> np.ndarray:
+    """cal_Coulomb.cu:41-88: two comment lines; natom, origin and one more
+    number; three axis lines whose counts must equal the cell grid; natom
+    atom lines (skipped); then the values with z fastest.  Returns the
+    values [N] in the solver's layout (x fastest), in Hartree/e."""
+    with open(path) as f:
+        f.readline(); f.readline()
+        tok = f.read().split()
+    natom = int(tok[0])
+    pos = 5                                          # natom x0 y0 z0 di
+    counts = []
+    for _ in range(3):
+        counts.append(int(tok[pos])); pos += 4
+    if tuple(counts) != tuple(int(g) for g in grid):
+        raise ValueError("cube file doesn't match input")
+    pos += 5 * natom
+    nx, ny, nz = counts
+    vals = np.array([float(v) for v in tok[pos:pos + nx * ny * nz]])
+    if vals.size != nx * ny * nz:
+        raise ValueError("short ESP cube %s" % path)
+    return np.ascontiguousarray(vals.reshape(nx, ny, nz).transpose(2, 1, 0)).ravel()
 
 
 def parse_xmu(path: str) -> dict:

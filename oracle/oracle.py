@@ -35,6 +35,7 @@ class OracleInput(C.Structure):
         ("chargeup", C.c_int),
         ("t_init", C.POINTER(C.c_double)),
         ("verbose", C.c_int),
+        ("esp", C.POINTER(C.c_double)),
     ]
 
 
@@ -82,7 +83,7 @@ class Case:
 
     def __init__(self, grid, box, solvent: F.Solvent, sig, eps, q, xyz,
                  closure=0, conv=1e-6, maxstep=10000, count=2, m=0.6, mp=0.2,
-                 chargeup=0, t_init=None):
+                 chargeup=0, t_init=None, esp=None):
         self.grid = tuple(int(g) for g in grid)
         self.box = tuple(float(b) for b in box)
         self.sv = solvent
@@ -91,6 +92,7 @@ class Case:
         self.closure, self.conv, self.maxstep = closure, conv, maxstep
         self.count, self.m, self.mp, self.chargeup = count, m, mp, chargeup
         self.t_init = None if t_init is None else _f64(t_init)
+        self.esp = None if esp is None else _f64(esp).ravel()
         self._keep = []
 
     @property
@@ -113,6 +115,7 @@ class Case:
         s.count, s.m, s.mp, s.chargeup = self.count, self.m, self.mp, self.chargeup
         s.t_init = _p(self.t_init)
         s.verbose = verbose
+        s.esp = _p(self.esp)
         return s
 
 

@@ -259,7 +259,9 @@ struct Problem {
   }
 };
 
-// cal_LJ.cu:4-72 and cal_Coulomb.cu:8-155 (no ESP cube)
+// cal_LJ.cu:4-72 and cal_Coulomb.cu:8-155; with an ESP cube the closure's
+// e is the cube times hartree / (kB T) (cal_Coulomb.cu:88-90) while fr and fk
+// stay the point-charge forms
 void potentials(const Problem &P, double *u, double *e, double *fr, cd *fk) {
   const OracleInput *in = P.in;
   const int na = in->natom, nv = P.nv;
@@ -304,7 +306,7 @@ void potentials(const Problem &P, double *u, double *e, double *fr, cd *fk) {
         dfr += in->q[iu];
       }
     }
-    e[ip] = de * ubeta;
+    e[ip] = in->esp ? in->esp[ip] * (kHartree / (kBoltzmann * in->temper)) : de * ubeta;
     fr[ip] = dfr * ubeta;
     double kx, ky, kz;
     P.kvec(ip, kx, ky, kz);

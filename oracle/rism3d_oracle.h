@@ -45,6 +45,8 @@ typedef struct {
   int chargeup;         /* -c stages, 0 = none */
   const double *t_init; /* optional restart t_uv [natv][N] (read_tuv.cu) */
   int verbose;
+  const double *esp;    /* optional ESP cube values [N], Hartree/e, x fastest
+                           (cal_Coulomb.cu:41-96); replaces the point-charge e */
 } OracleInput;
 
 typedef struct {

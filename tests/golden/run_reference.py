@@ -20,17 +20,27 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 BIN = os.path.join(ROOT, "oracle", "_ref", "3drism-cuda")
 
 CASES = ["test1", "test1_tight", "test2", "test2_tight", "test3", "test4", "test4_tight",
-         "cfg0_chain12", "cfg1_globule300", "cfg2_protein846_kh"]
+         "cfg0_chain12", "cfg1_globule300", "cfg2_protein846_kh", "cfg0_esp"]
+# ESP-cube cases (-e, cal_Coulomb.cu:41-96): name -> control file reused;
+# the cube comes from make_esp.py
+ESP_CASES = {"cfg0_esp": "cfg0_chain12"}
 
 
 def run(case, outdir):
     d = os.path.join(outdir, case)
     os.makedirs(d, exist_ok=True)
-    shutil.copyfile(os.path.join(HERE, case + ".inp"), os.path.join(d, case + ".inp"))
-    solvent = open(os.path.join(HERE, case + ".inp")).read().split()[4]   # read_input.cu:42
+    src = os.path.join(HERE, ESP_CASES.get(case, case) + ".inp")
+    shutil.copyfile(src, os.path.join(d, case + ".inp"))
+    solvent = open(src).read().split()[4]                                  # read_input.cu:42
     shutil.copyfile(os.path.join(HERE, solvent), os.path.join(d, solvent))
+    args = [case + ".inp"]
+    if case in ESP_CASES:
+        sys.path.insert(0, HERE)
+        import make_esp
+        make_esp.write_cube(src, os.path.join(d, case + ".cube"))
+        args = ["-e", case + ".cube"] + args
     t0 = time.perf_counter()
-    p = subprocess.run(["timeout", "900", BIN, case + ".inp"], cwd=d,
+    p = subprocess.run(["timeout", "900", BIN] + args, cwd=d,
                        capture_output=True, text=True)
     wall = time.perf_counter() - t0
     open(os.path.join(d, "stdout.log"), "w").write(p.stdout + p.stderr)

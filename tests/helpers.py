@@ -20,12 +20,41 @@ def load_case(name, **over):
     return case, ctrl, sol
 
 
+# the -e (ESP cube) case: control file it reuses
+ESP_CASES = {"cfg0_esp": "cfg0_chain12"}
+
+
+def esp_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_esp", os.path.join(GOLDEN, "make_esp.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_esp_case(name="cfg0_esp", cube=None):
+    """The control file of ESP_CASES[name], uncentred (-e implies -f,
+    main.cu:37-41), with the ESP cube of tests/golden/make_esp.py; `cube`
+    (a path) writes the cube file too and reads the values back from it."""
+    inp = os.path.join(GOLDEN, ESP_CASES[name] + ".inp")
+    case, ctrl, sol = O.case_from_inp(inp, centering=False)
+    mod = esp_module()
+    if cube is None:
+        _, _, case.esp = mod.esp_values(inp)
+    else:
+        mod.write_cube(inp, cube)
+        case.esp = F.read_esp_cube(cube, case.grid)
+    return case, ctrl, sol
+
+
 def product_solver(case, precision=0, **kw):
     import rism3d_b200 as R
     s = R.Solver(case.grid, case.box, closure=case.closure, convergence=case.conv,
                  maxstep=case.maxstep, an2=(case.count, case.m, case.mp),
                  precision=precision, **kw)
     s.set_solvent_obj(case.sv)
+    if getattr(case, "esp", None) is not None:
+        s.set_esp(case.esp)
     s.set_solute(case.sig, case.eps, case.q, case.xyz)
     return s
 

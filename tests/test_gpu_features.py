@@ -223,6 +223,82 @@ def test_bad_inputs_are_errors_not_exits(tmp_path):
     assert p.returncode == 1 and "short chi table" in p.stderr
 
 
+def test_esp_cube_cli_matches_reference_executable(tmp_path):
+    """-e ESP cube (cal_Coulomb.cu:41-96) through the drop-in executable: the
+    same cube and control file as the reference executable's recorded run;
+    -e also switches centring off (main.cu:37-41).  A cube on another grid
+    is refused with the reference's message, as an error status."""
+    from helpers import esp_module
+    d = tmp_path / "esp"
+    d.mkdir()
+    src = os.path.join(GOLDEN, "cfg0_chain12.inp")
+    shutil.copyfile(src, str(d / "cfg0_esp.inp"))
+    shutil.copyfile(os.path.join(GOLDEN, "tip3p_cfg_vv.xvk"), str(d / "tip3p_cfg_vv.xvk"))
+    esp_module().write_cube(src, str(d / "cfg0_esp.cube"))
+    p = subprocess.run([CLI, "-e", "cfg0_esp.cube", "cfg0_esp.inp"], cwd=str(d),
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    got = F.parse_xmu(str(d / "cfg0_esp.xmu"))
+    ref = ref_xmu("cfg0_esp")
+    summary = json.load(open(os.path.join(GOLDEN, "ref_b200", "summary.json")))
+    assert set(got) == set(ref)
+    for k in ("SFE_SC", "SFE_SC_HNC", "SFE_GF"):
+        assert abs(got[k] - ref[k]) < MU_TOL, (k, got[k], ref[k])
+    assert abs(got["PMV"] - ref["PMV"]) < 2e-5
+    assert abs(got["SE"] - ref["SE"]) < 1e-3 * abs(ref["SE"])
+    # SE_LJ: -18.8 J/mol with the cube, +45.4 for the same solve without it
+    assert abs(got["SE_LJ"] - ref["SE_LJ"]) < 5.0
+    assert abs(p.stdout.count(" Step = ") - summary["cfg0_esp"]["iterations"]) <= 1
+    lines = open(str(d / "cfg0_esp.cube")).read().split("\n")
+    lines[3] = lines[3].replace("   64", "   32", 1)
+    (d / "bad.cube").write_text("\n".join(lines))
+    p = subprocess.run([CLI, "-e", "bad.cube", "cfg0_esp.inp"], cwd=str(d),
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 1 and "cube file doesn't match input" in p.stderr
+
+
+def test_esp_cube_matches_oracle_and_disables_gradients(tmp_path):
+    import rism3d_b200 as R
+    from helpers import load_esp_case
+    case, _, _ = load_esp_case(cube=str(tmp_path / "c.cube"))
+    o, r, s = both(case)
+    assert abs(r["iterations"] - o["iterations"]) <= 1
+    assert abs(r["sfe_sc"] - o["sfe_sc"]) < 1.0
+    assert rel_err(s.grid_array(R.GRID_H), o["h"]) < 1e-4
+    with pytest.raises(R.RismError) as e:
+        s.grad()
+    assert e.value.code == R.BAD_STATE
+    s.set_esp(None)                       # back to the point-charge potential
+    r0 = s.solve()
+    s.grad()
+    plain = O.solve(O.Case(case.grid, case.box, case.sv, case.sig, case.eps, case.q, case.xyz,
+                           case.closure, case.conv, case.maxstep, case.count, case.m, case.mp))
+    assert abs(r0["sfe_sc"] - plain["sfe_sc"]) < 1.0
+    s.close()
+
+
+def test_esp_of_the_point_charges_leaves_the_solve_unchanged():
+    """An ESP equal to the point-charge potential (Hartree/e, bohr; r < 1e-5 A
+    terms skipped as cal_Coulomb.cu:112-119) reproduces the plain solve."""
+    case, _, _ = load_case("cfg0_chain12")
+    s = product_solver(case)
+    r0 = s.solve()
+    n = case.grid[0]
+    ax = (np.arange(n) - n // 2) * (case.box[0] / n)
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    phi = np.zeros(X.shape)
+    for q, (x, y, z) in zip(case.q, case.xyz):
+        rr = np.sqrt((X - x) ** 2 + (Y - y) ** 2 + (Z - z) ** 2)
+        with np.errstate(divide="ignore"):
+            phi += np.where(rr >= 1e-5, q * F.BOHR / rr, 0.0)
+    s.set_esp(np.ascontiguousarray(phi.transpose(2, 1, 0)).ravel())
+    r1 = s.solve()
+    assert r1["iterations"] == r0["iterations"]
+    for k in ("sfe_sc", "sfe_gf", "pmv", "se"):
+        assert abs(r1[k] - r0[k]) <= 1e-8 * abs(r0[k]) + 1e-9, (k, r1[k], r0[k])
+    s.close()
+
+
 @pytest.mark.parametrize("name,prec", [("cfg1_globule300", 1), ("cfg2_protein846_kh", 0),
                                        ("cfg2_protein846_kh", 1), ("test4", 0), ("test4", 1)])
 def test_large_cases_match_reference_executable(name, prec):

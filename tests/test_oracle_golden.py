@@ -66,3 +66,47 @@ def test_tight_convergence_pins(golden):
     # (oracle 9.95e-10 at step 75, reference 1.0048e-9 then 2.8e-10 at 76)
     assert abs(res["iterations"] - summary["test1_tight"]["iterations"]) <= 1
     assert abs(res["ibeta"] * res["xmu_sc"].sum() - ref["SFE_SC"]) < 1e-3
+
+
+def test_oracle_esp_cube_reproduces_reference_binary(tmp_path, golden):
+    """-e (cal_Coulomb.cu:41-96): the reference executable run with the cube
+    of tests/golden/make_esp.py (Gaussian-smeared charges) on the 12-atom
+    chain; the oracle reads the same cube text and reproduces the .xmu and
+    the iteration count."""
+    from helpers import load_esp_case
+    case, _, _ = load_esp_case(cube=str(tmp_path / "c.cube"))
+    res = O.solve(case)
+    summary = json.load(open(os.path.join(golden, "ref_b200", "summary.json")))
+    assert res["iterations"] == summary["cfg0_esp"]["iterations"]
+    got = oracle_xmu(res, tmp_path, case.closure, case.sv.natv)
+    ref = ref_xmu("cfg0_esp")
+    for k in KEYS:
+        assert abs(got[k] - ref[k]) <= 2e-5 + 2e-9 * abs(ref[k]), (k, got[k], ref[k])
+    # the cube is not the point-charge potential: the same uncentred solve
+    # without it lands 45 J/mol away in mu_ex and 64 J/mol in SE_LJ
+    case.esp = None
+    plain = oracle_xmu(O.solve(case), tmp_path, case.closure, case.sv.natv)
+    assert abs(plain["SFE_SC"] - ref["SFE_SC"]) > 30.0
+    assert abs(plain["SE_LJ"] - ref["SE_LJ"]) > 50.0
+
+
+def test_esp_of_the_point_charges_reproduces_the_coulomb_grid():
+    """An ESP equal to the point-charge potential in Hartree/e (distances in
+    bohr, the r < 1e-5 A terms skipped as cal_Coulomb.cu:112-119 does) gives
+    the same e grid: the cube's hartree / (kB T) scale against the
+    point-charge hartree bohr / (kB T)."""
+    case, _, _ = load_case("cfg0_chain12")
+    case.grid, case.box = (32, 32, 32), (16.0, 16.0, 16.0)
+    _, e0, fr0, _ = O.potentials(case)
+    n = case.grid[0]
+    ax = (np.arange(n) - n // 2) * (case.box[0] / n)
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    phi = np.zeros(X.shape)
+    for q, (x, y, z) in zip(case.q, case.xyz):
+        r = np.sqrt((X - x) ** 2 + (Y - y) ** 2 + (Z - z) ** 2)
+        with np.errstate(divide="ignore"):
+            phi += np.where(r >= 1e-5, q * F.BOHR / r, 0.0)
+    case.esp = np.ascontiguousarray(phi.transpose(2, 1, 0)).ravel()
+    _, e1, fr1, _ = O.potentials(case)
+    assert np.array_equal(fr0, fr1)
+    assert np.abs(e1 - e0).max() <= 1e-12 * np.abs(e0).max()
