@@ -63,10 +63,11 @@ void free_device(Context &c) {
                   c.d_U, c.d_t, c.d_Y, c.d_RP, c.d_buf, c.d_h, c.d_g,
                   c.f_U, c.f_t, c.f_Y, c.f_RP, c.f_buf, c.f_R0, c.f_x0, c.d_part, c.d_state,
                   c.d_stage, c.d_stage_ref, c.d_obs, c.d_atom_part, c.chi.d_coef, c.d_xs,
-                  c.d_atom_off, c.d_atom_cnt, c.d_esp};
+                  c.d_atom_off, c.d_atom_cnt, c.d_esp, c.d_rm_ccoef, c.d_rm_k2, c.d_rm_hcoef};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   c.d_u = c.d_e = c.d_fr = nullptr; c.d_fkh = nullptr; c.d_atoms = nullptr; c.d_esp = nullptr;
+  c.d_rm_ccoef = c.d_rm_k2 = c.d_rm_hcoef = nullptr; c.rmdft = false;
   c.d_tw = nullptr; c.d_twf = nullptr; c.d_U = c.d_t = c.d_Y = c.d_RP = nullptr;
   c.d_buf = nullptr; c.d_h = c.d_g = nullptr;
   c.f_U = c.f_t = c.f_Y = c.f_RP = nullptr; c.f_buf = nullptr; c.f_R0 = c.f_x0 = nullptr;
@@ -92,7 +93,8 @@ void free_device(Context &c) {
   c.d_count = nullptr;
   if (c.plan64) cufftDestroy(c.plan64);
   if (c.plan32) cufftDestroy(c.plan32);
-  c.plan64 = c.plan32 = 0;
+  if (c.plan1) cufftDestroy(c.plan1);
+  c.plan64 = c.plan32 = c.plan1 = 0;
   c.plans_ok = false;
 }
 
@@ -402,7 +404,60 @@ int rism3d_set_solvent(rism3d_ctx *x, int natv, const double *rho, const double 
                        const double *sig, const double *eps, double temperature, double xt,
                        int ntab, double dr, const double *xvv) {
   if (!x) return RISM3D_BAD_INPUT;
+  rism3d_set_rmdft(x, nullptr, 0, nullptr, nullptr, nullptr, 0.0, 0.0);  // tables follow the solvent
   return context_set_solvent(x->c, natv, rho, q, sig, eps, temperature, xt, ntab, dr, xvv);
+}
+
+int rism3d_set_rmdft(rism3d_ctx *x, const double *cvk, int ntab2, const double *k,
+                     const double *chs, const double *w, double pfhs, double w0) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  for (double **p : {&c.d_rm_ccoef, &c.d_rm_k2, &c.d_rm_hcoef}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  c.rmdft = false;
+  if (!cvk) return RISM3D_OK;
+  if (c.nb != 1) { c.err = "RMDFT is for single-solute contexts"; return RISM3D_BAD_STATE; }
+  if (!c.have_solvent) { c.err = "set the solvent first"; return RISM3D_BAD_STATE; }
+  if (ntab2 < 4 || !k || !chs || !w || !std::isfinite(w0) || !(pfhs >= 0.0 && pfhs < 1.0)) {
+    c.err = "bad RMDFT hard-sphere table";
+    return RISM3D_BAD_INPUT;
+  }
+  for (int i = 1; i < ntab2; ++i)
+    if (!(k[i] > k[i - 1])) { c.err = "RMDFT hard-sphere knots must increase"; return RISM3D_BAD_INPUT; }
+  // the table must reach the grid's largest |k| (solvent_spline2.cu:16-19)
+  const double kx = 2.0 * kPi * (c.nx / 2.0 - 0.5) / c.prm.box[0];
+  const double ky = 2.0 * kPi * (c.ny / 2.0 - 0.5) / c.prm.box[1];
+  const double kz = 2.0 * kPi * (c.nz / 2.0 - 0.5) / c.prm.box[2];
+  if (sqrt(kx * kx + ky * ky + kz * kz) > k[ntab2 - 1]) {
+    c.err = "insufficient maximal T tabulated";
+    return RISM3D_BAD_INPUT;
+  }
+  const int V = c.natv, nt = c.chi.ntab;
+  std::vector<double> xp(nt), cc((size_t)nt * V * V * 4), hc((size_t)ntab2 * 8);
+  for (int i = 0; i < nt; ++i) xp[i] = c.chi.dk * (i + 1);      // solvent_spline.cu:50-62
+  for (int ab = 0; ab < V * V; ++ab)
+    spline_coefficients(xp.data(), cvk + (size_t)ab * nt, nt, &cc[(size_t)ab * 4],
+                        (size_t)V * V * 4);
+  spline_coefficients(k, chs, ntab2, &hc[0], 8);                 // solvent_spline2.cu:33-56
+  spline_coefficients(k, w, ntab2, &hc[4], 8);
+  if (!cuda_ok(c, cudaMalloc(&c.d_rm_ccoef, sizeof(double) * cc.size()), "alloc RMDFT") ||
+      !cuda_ok(c, cudaMalloc(&c.d_rm_k2, sizeof(double) * ntab2), "alloc RMDFT") ||
+      !cuda_ok(c, cudaMalloc(&c.d_rm_hcoef, sizeof(double) * hc.size()), "alloc RMDFT") ||
+      !cuda_ok(c, cudaMemcpy(c.d_rm_ccoef, cc.data(), sizeof(double) * cc.size(),
+                             cudaMemcpyHostToDevice), "copy RMDFT") ||
+      !cuda_ok(c, cudaMemcpy(c.d_rm_k2, k, sizeof(double) * ntab2, cudaMemcpyHostToDevice),
+               "copy RMDFT") ||
+      !cuda_ok(c, cudaMemcpy(c.d_rm_hcoef, hc.data(), sizeof(double) * hc.size(),
+                             cudaMemcpyHostToDevice), "copy RMDFT"))
+    return RISM3D_CUDA_ERROR;
+  c.rm_ntab2 = ntab2;
+  c.rm_pfhs = pfhs;
+  c.rm_w0 = w0;
+  c.rmdft = true;
+  return RISM3D_OK;
 }
 
 int rism3d_set_solute(rism3d_ctx *x, int natom, const double *sig, const double *eps,
@@ -436,6 +491,7 @@ int rism3d_solve(rism3d_ctx *x, int chargeup, rism3d_result *res) {
   cudaEventRecord(c.tm_obs.a, c.stream);
   rc = compute_observables(c);
   if (rc == RISM3D_OK) rc = compute_atom_integrals(c, false);
+  if (rc == RISM3D_OK) rc = compute_rmdft(c);                // output.cu:25
   cudaEventRecord(c.tm_obs.b, c.stream);
   if (rc != RISM3D_OK) return rc;
   if (!cuda_ok(c, cudaStreamSynchronize(c.stream), "solve")) return RISM3D_CUDA_ERROR;
@@ -561,10 +617,6 @@ int rism3d_initialize(rism3d_ctx **out, const char *control, const char *structu
                       int precision) {
   if (!out || !control) { g_create_err = "null argument"; return RISM3D_BAD_INPUT; }
   *out = nullptr;
-  if (hs && *hs) {
-    g_create_err = "RMDFT (hard-sphere file) is not supported by this build";
-    return RISM3D_BAD_INPUT;
-  }
   io::ControlFile cf;
   std::string err;
   std::string st = structure ? structure : "";
@@ -597,6 +649,25 @@ int rism3d_initialize(rism3d_ctx **out, const char *control, const char *structu
   if (q0) for (double &v : q) v = 0.0;                        // solute.cu:45-49
   rc = rism3d_set_solvent(x, sf.natv, sf.rho.data(), sf.q.data(), sf.sig.data(), sf.eps.data(),
                           sf.temper, sf.xt, sf.ntab, sf.dr, sf.xvv.data());
+  if (rc == RISM3D_OK && hs && *hs) {                         // solvent_read.cc:88-140
+    io::SolventFile cv;
+    io::HardSphereFile hf;
+    const size_t dot = svpath.rfind('.');
+    const std::string cvk = (dot == std::string::npos ? svpath : svpath.substr(0, dot)) + ".cvk";
+    if (!io::read_xvk(cvk, cv, err)) {
+      c.err = "cvk file could not be opened! (" + err + ")";
+      rc = RISM3D_BAD_INPUT;
+    } else if (cv.natv != sf.natv || cv.ntab != sf.ntab) {
+      c.err = "the .cvk table does not match the .xvk (sites or rows)";
+      rc = RISM3D_BAD_INPUT;
+    } else if (!io::read_hard_sphere(hs, hf, err)) {
+      c.err = err;
+      rc = RISM3D_BAD_INPUT;
+    } else {
+      rc = rism3d_set_rmdft(x, cv.xvv.data(), hf.ntab2, hf.k.data(), hf.chs.data(), hf.w.data(),
+                            hf.pfhs, hf.w0);
+    }
+  }
   if (rc == RISM3D_OK && esp && *esp) {                       // cal_Coulomb.cu:41-96
     std::vector<double> cube;
     if (!io::read_esp_cube(esp, p.grid, cube, err)) {
@@ -659,6 +730,7 @@ int rism3d_output(rism3d_ctx *x) {
     }
     xv.se = c.res.se; xv.se_lj = c.res.se_lj; xv.se_es = c.res.se_es;
     xv.pmv_l = c.res.pmv; xv.pressure = c.res.pressure; xv.correction = c.res.correction;
+    xv.rmdft = c.rmdft; xv.sfe_rmdft = c.res.sfe_rmdft;
     if (!io::write_xmu(c.fname + (c.zero ? ".xmu0" : ".xmu"), xv)) { c.err = "cannot write .xmu"; return RISM3D_BAD_INPUT; }
   }
   if (has('d')) {

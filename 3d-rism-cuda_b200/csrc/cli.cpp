@@ -1,6 +1,7 @@
 // rism3d-b200: drop-in for the reference executable (main.cu:6-64).
 // Same flags: -c charge-up stages, -d device, -i control file, -s structure
-// file, -r hard-sphere file (RMDFT, rejected), -e ESP cube (as in the
+// file, -r hard-sphere file (RMDFT correction; reads the .cvk beside the
+// solvent file too), -e ESP cube (as in the
 // reference it also disables centring), -f (no centring; takes an
 // argument, getopt "f:"), -z zero solute charges (.xmu0).  Extra: -p 1 runs
 // the FP32-bulk + FP64-polish iteration (default 0 = plain FP64).

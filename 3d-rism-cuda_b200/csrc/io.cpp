@@ -138,6 +138,9 @@ bool write_xmu(const std::string &path, const XmuValues &x) {
   std::ofstream o(path.c_str());
   if (!o) return false;
   o << " $RESULT" << std::endl;
+  if (x.rmdft)
+    o << "SFE_RMDFT= " << std::fixed << std::setprecision(5) << x.sfe_rmdft << " !(J/mol)"
+      << std::endl << std::endl;
   double s = 0;
   for (int v = 0; v < x.natv; ++v) s += x.sfec_sc[v];
   o << "SFE_SC= " << std::fixed << std::setprecision(5) << s << " !(J/mol)" << std::endl;
@@ -280,6 +283,31 @@ bool read_esp_cube(const std::string &path, const int grid[3], std::vector<doubl
           esp.clear();
           return false;
         }
+  return true;
+}
+
+bool read_hard_sphere(const std::string &path, HardSphereFile &hs, std::string &err) {
+  std::ifstream in(path.c_str());
+  if (!in) { err = "Hardsphare file could not be opened!"; return false; }
+  std::string line;
+  int ntab2 = 0;
+  if (!std::getline(in, line) || !(std::istringstream(line) >> ntab2) || ntab2 < 4) {
+    err = "bad row count in hard-sphere file " + path;
+    return false;
+  }
+  if (!std::getline(in, line) || !(std::istringstream(line) >> hs.pfhs >> hs.w0)) {
+    err = "bad packing fraction line in hard-sphere file " + path;
+    return false;
+  }
+  hs.ntab2 = ntab2;
+  hs.k.resize(ntab2);
+  hs.chs.resize(ntab2);
+  hs.w.resize(ntab2);
+  for (int i = 0; i < ntab2; ++i)
+    if (!std::getline(in, line) || !(std::istringstream(line) >> hs.k[i] >> hs.chs[i] >> hs.w[i])) {
+      err = "short hard-sphere file " + path;
+      return false;
+    }
   return true;
 }
 

@@ -147,6 +147,13 @@ struct Context {
   double *d_e = nullptr;     // [N]   beta sum q e^-r / r (short-range Coulomb)
   double *d_fr = nullptr;    // [N]   beta long-range part
   double *d_esp = nullptr;   // [N]   ESP cube (Hartree/e) replacing the point-charge e, or null
+  // RMDFT correction (cal_rmdft.cu): solvent c(k) and site 0's hard-sphere table
+  bool rmdft = false;
+  double rm_pfhs = 0.0, rm_w0 = 0.0;
+  int rm_ntab2 = 0;
+  double *d_rm_ccoef = nullptr;  // [ntab][V*V][4] spline of c(k) on the chi knots
+  double *d_rm_k2 = nullptr;     // [ntab2] hard-sphere table knots
+  double *d_rm_hcoef = nullptr;  // [ntab2][2][4] splines of chi_hs(k) and w(k)
   double2 *d_fkh = nullptr;  // [N/2] beta fk on the owner half of k space
   double *d_atoms = nullptr; // [A][8] x y z q sig eps pad (all solutes)
   int *d_atom_off = nullptr; // [nb] first atom of each solute
@@ -180,6 +187,7 @@ struct Context {
   int natom_part_cap = 0;
 
   cufftHandle plan64 = 0, plan32 = 0;
+  cufftHandle plan1 = 0;     // one Z2Z transform of the cell (RMDFT), made on first use
   bool plans_ok = false;
   // one captured iteration per precision, reused by every solve
   cudaGraphExec_t graph64 = nullptr, graph32 = nullptr, graph32r = nullptr;
@@ -227,6 +235,12 @@ int build_twiddles(Context &c);
 int compute_potentials(Context &c);               // potential.cu
 int launch_potential_r(Context &c);               // potential.cu (timing hook)
 int upload_chi(Context &c);                       // solver.cu
+// spline.cc:4-43: natural cubic spline through (xp[k], yp[k]), k < np; writes
+// {y_k, b_k, c_k, d_k} (y + b t + c t^2 + d t^3 on interval k; zero
+// coefficients on the last knot) to out[k * stride + 0..3]
+void spline_coefficients(const double *xp, const double *yp, int np, double *out,
+                         size_t stride);            // solver.cu
+int compute_rmdft(Context &c);                     // rmdft.cu
 int run_solve(Context &c, int chargeup);          // solver.cu
 int compute_observables(Context &c);              // observe.cu
 int compute_atom_integrals(Context &c, bool forces);  // observe.cu

@@ -46,6 +46,8 @@ struct XmuValues {
   int closure = 0;
   double sfec_sc[8], sfec_sc_hnc[8], sfec_gf[8];
   double se, se_lj, se_es, pmv_l, pressure, correction;
+  bool rmdft = false;        // SFE_RMDFT line first (output_xmu.cu:25-28)
+  double sfe_rmdft = 0;
 };
 bool write_xmu(const std::string &path, const XmuValues &x);
 // output_grad.cu:7-30 (values already times dv)
@@ -67,6 +69,15 @@ bool write_qv(const std::string &path, const int grid[3], const double dr[3],
 // lines; values with z fastest).  esp receives [N] values, x fastest, Hartree/e.
 bool read_esp_cube(const std::string &path, const int grid[3], std::vector<double> &esp,
                    std::string &err);
+// RMDFT hard-sphere table, the -r file (solvent_read.cc:118-140): line 1
+// ntab2; line 2 packing fraction and w(0) of site 0; then ntab2 rows
+// k, chi_hs(k), w(k)
+struct HardSphereFile {
+  int ntab2 = 0;
+  double pfhs = 0, w0 = 0;
+  std::vector<double> k, chs, w;
+};
+bool read_hard_sphere(const std::string &path, HardSphereFile &out, std::string &err);
 // write_tuv.cu:7-33 / read_tuv.cu:6-34
 bool write_tuv(const std::string &path, const int grid[3], int natv, const double *t, long long n);
 bool read_tuv(const std::string &path, const int grid[3], int natv, std::vector<double> &t,

@@ -1341,6 +1341,42 @@ int build_twiddles(Context &c) {
 
 // Natural cubic spline of every chi_ab table (same tridiagonal sweep as
 // spline.cc:4-43), uploaded as [knot][ab][y c0 c1 c2].
+void spline_coefficients(const double *xp, const double *yp, int np, double *out,
+                         size_t stride) {
+  std::vector<double> a(np), b(np), cc(np), d(np), s(np);
+  const int m = np - 2;
+  for (int k = 1; k <= m; ++k) {
+    double hl = xp[k] - xp[k - 1], hr = xp[k + 1] - xp[k];
+    a[k] = hl / (hl + hr);
+    b[k] = 1 - a[k];
+    double q1 = (yp[k + 1] - yp[k]) / hr, q2 = (yp[k] - yp[k - 1]) / hl;
+    cc[k] = 6.0 * ((q1 - q2) / (hl + hr));
+    d[k] = 2.0;
+  }
+  for (int k = 1; k < m; ++k) {
+    b[k] = b[k] / d[k];
+    cc[k] = cc[k] / d[k];
+    d[k + 1] = d[k + 1] - a[k + 1] * b[k];
+    cc[k + 1] = cc[k + 1] - a[k + 1] * cc[k];
+  }
+  s[m] = cc[m] / d[m];
+  for (int k = m - 1; k >= 1; --k) s[k] = cc[k] - b[k] * s[k + 1];
+  s[0] = s[m + 1] = 0.0;
+  for (int k = 0; k < np; ++k) {
+    double *o = out + (size_t)k * stride;
+    o[0] = yp[k];
+    o[1] = o[2] = o[3] = 0.0;
+    if (k <= m) {
+      double h = xp[k + 1] - xp[k];
+      double c1 = s[k] / 2.0;
+      double c2 = (s[k + 1] - s[k]) / (6.0 * h);
+      o[1] = (yp[k + 1] - yp[k]) / h - c1 * h - c2 * h * h;
+      o[2] = c1;
+      o[3] = c2;
+    }
+  }
+}
+
 int upload_chi(Context &c) {
   const int V = c.natv, nt = c.ntab;
   c.chi.ntab = nt;
@@ -1357,41 +1393,10 @@ int upload_chi(Context &c) {
   std::vector<double> xp(nt);
   for (int i = 0; i < nt; ++i) xp[i] = c.chi.dk * (i + 1);
   std::vector<double> tab((size_t)nt * V * V * 4, 0.0);
-  std::vector<double> a(nt), b(nt), cc(nt), d(nt), s(nt);
   for (int va = 0; va < V; ++va)
-    for (int vb = 0; vb < V; ++vb) {
-      const double *yp = &c.xvv_host[((size_t)va * V + vb) * nt];
-      const int m = nt - 2;
-      for (int k = 1; k <= m; ++k) {
-        double hl = xp[k] - xp[k - 1], hr = xp[k + 1] - xp[k];
-        a[k] = hl / (hl + hr);
-        b[k] = 1 - a[k];
-        double q1 = (yp[k + 1] - yp[k]) / hr, q2 = (yp[k] - yp[k - 1]) / hl;
-        cc[k] = 6.0 * ((q1 - q2) / (hl + hr));
-        d[k] = 2.0;
-      }
-      for (int k = 1; k < m; ++k) {
-        b[k] = b[k] / d[k];
-        cc[k] = cc[k] / d[k];
-        d[k + 1] = d[k + 1] - a[k + 1] * b[k];
-        cc[k + 1] = cc[k + 1] - a[k + 1] * cc[k];
-      }
-      s[m] = cc[m] / d[m];
-      for (int k = m - 1; k >= 1; --k) s[k] = cc[k] - b[k] * s[k + 1];
-      s[0] = s[m + 1] = 0.0;
-      for (int k = 0; k < nt; ++k) {
-        double *o = &tab[((size_t)k * V * V + va * V + vb) * 4];
-        o[0] = yp[k];
-        if (k <= m) {
-          double h = xp[k + 1] - xp[k];
-          double c1 = s[k] / 2.0;
-          double c2 = (s[k + 1] - s[k]) / (6.0 * h);
-          o[1] = (yp[k + 1] - yp[k]) / h - c1 * h - c2 * h * h;
-          o[2] = c1;
-          o[3] = c2;
-        }
-      }
-    }
+    for (int vb = 0; vb < V; ++vb)
+      spline_coefficients(xp.data(), &c.xvv_host[((size_t)va * V + vb) * nt], nt,
+                          &tab[(size_t)(va * V + vb) * 4], (size_t)V * V * 4);
   // the captured iteration graphs embed the table pointers
   if (c.graph64) { cudaGraphExecDestroy(c.graph64); c.graph64 = nullptr; }
   if (c.graph32) { cudaGraphExecDestroy(c.graph32); c.graph32 = nullptr; }

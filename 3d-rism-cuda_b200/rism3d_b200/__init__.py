@@ -26,7 +26,7 @@ EXPORTS = ["rism3d_create", "rism3d_set_solvent", "rism3d_set_solute", "rism3d_s
            "rism3d_solve_batch", "rism3d_destroy", "rism3d_last_error",
            "rism3d_initialize", "rism3d_iterate", "rism3d_output",
            "rism3d_refresh_potentials", "rism3d_kernel_launches", "rism3d_time_kernel",
-           "rism3d_set_esp"]
+           "rism3d_set_esp", "rism3d_set_rmdft"]
 
 
 class RismError(RuntimeError):
@@ -51,7 +51,8 @@ class Result(C.Structure):
                 ("pressure", C.c_double), ("correction", C.c_double), ("se", C.c_double),
                 ("se_lj", C.c_double), ("se_es", C.c_double), ("rms", C.c_double),
                 ("iterations", C.c_int), ("iterations_fp32", C.c_int), ("status", C.c_int),
-                ("ms_setup", C.c_double), ("ms_iterate", C.c_double), ("ms_observe", C.c_double)]
+                ("ms_setup", C.c_double), ("ms_iterate", C.c_double), ("ms_observe", C.c_double),
+                ("sfe_rmdft", C.c_double)]
 
     def as_dict(self):
         d = {}
@@ -96,6 +97,7 @@ def lib():
         L.rism3d_output.argtypes = [vp]
         L.rism3d_refresh_potentials.argtypes = [vp]
         L.rism3d_set_esp.argtypes = [vp, d]
+        L.rism3d_set_rmdft.argtypes = [vp, d, C.c_int, d, d, d, C.c_double, C.c_double]
         L.rism3d_kernel_launches.argtypes = [vp]
         L.rism3d_kernel_launches.restype = C.c_longlong
         L.rism3d_time_kernel.argtypes = [vp, C.c_int, C.c_int, d]
@@ -162,6 +164,18 @@ class Solver:
         potential in the closure; None removes it (rism3d_set_esp)."""
         self._keep_esp = None if esp is None else _f64(np.asarray(esp).ravel())
         self._check(lib().rism3d_set_esp(self.h, _dp(self._keep_esp)))
+
+    def set_rmdft(self, cvk, k=None, chs=None, w=None, pfhs=0.0, w0=0.0):
+        """RMDFT tables (rism3d_set_rmdft): cvk [natv][natv][ntab] on the chi
+        knots and site 0's hard-sphere table k, chs, w with its packing
+        fraction and w(0); cvk None switches the correction off."""
+        if cvk is None:
+            self._check(lib().rism3d_set_rmdft(self.h, None, 0, None, None, None, 0.0, 0.0))
+            return
+        self._keep_rm = [_f64(cvk), _f64(k), _f64(chs), _f64(w)]
+        cv, kk, cs, ww = self._keep_rm
+        self._check(lib().rism3d_set_rmdft(self.h, _dp(cv), len(kk), _dp(kk), _dp(cs), _dp(ww),
+                                           float(pfhs), float(w0)))
 
     def set_tuv(self, t):
         self._keep_t = None if t is None else _f64(t)

@@ -20,7 +20,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["potential.cu", "solver.cu", "observe.cu", "adjoint.cu", "batch.cu",
-           "noalloc.cu", "capi.cpp", "io.cpp", "xrism1d.cpp"]
+           "noalloc.cu", "rmdft.cu", "capi.cpp", "io.cpp", "xrism1d.cpp"]
 
 
 def _ccbin():
@@ -42,7 +42,7 @@ def _newer(target, deps):
 def _compile(src, verbose=False):
     s = os.path.join(CSRC, src)
     o = os.path.join(OBJ, src + ".o")
-    hdrs = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".h")]
+    hdrs = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     hdrs.append(os.path.join(ROOT, "include", "rism3d_b200.h"))
     if _newer(o, [s] + hdrs):
         cmd = [NVCC] + _flags() + ["-c", s, "-o", o]

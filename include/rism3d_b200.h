@@ -94,6 +94,8 @@ typedef struct {
   double ms_setup;        /* potential grids + chi table (device time) */
   double ms_iterate;
   double ms_observe;
+  double sfe_rmdft;       /* SFE_RMDFT, J/mol (output_xmu.cu:25-28); 0 unless
+                             rism3d_set_rmdft tables are set */
 } rism3d_result;
 
 typedef struct rism3d_ctx rism3d_ctx;
@@ -153,6 +155,20 @@ int rism3d_grad(rism3d_ctx *ctx, double *dmu_dq, double *dmu_dsig,
  * NULL removes it.  Applies to the current solute at once and to every
  * later one; rism3d_grad refuses while it is set.  Single-solute contexts. */
 int rism3d_set_esp(rism3d_ctx *ctx, const double *esp);
+
+/* RMDFT free-energy correction (the reference's -r option,
+ * cal_rmdft.cu:5-115, tables of solvent_read.cc:88-140 and
+ * solvent_spline2.cu:7-103).  cvk[natv][natv][ntab]: the solvent direct
+ * correlation c(k) on the knots of the chi table (the .cvk file beside the
+ * .xvk; same layout as xvv).  Site 0's hard-sphere table (the -r file):
+ * ntab2 rows of k[i] (ascending), chs[i] (hard-sphere chi(k)) and w[i]
+ * (weight function), its packing fraction pfhs and w(k = 0) w0.  Every
+ * later solve reports SFE_RMDFT in rism3d_result.sfe_rmdft and the .xmu.
+ * cvk NULL switches it off.  Call after rism3d_set_solvent; BAD_INPUT when
+ * the hard-sphere table ends below the grid's largest |k|.  Single-solute
+ * contexts. */
+int rism3d_set_rmdft(rism3d_ctx *ctx, const double *cvk, int ntab2, const double *k,
+                     const double *chs, const double *w, double pfhs, double w0);
 
 /* Recompute the potential grids from the solute already on the device
  * (no host->device traffic); the next rism3d_solve starts from them. */
@@ -219,8 +235,8 @@ const char *rism3d_last_error(const rism3d_ctx *ctx);
  * structure file), the .xvk named in it, centres the solute, zeroes the
  * charges when q0, and computes the potential grids.  esp names an ESP
  * cube (NULL or "" for none; its grid must equal the control file's, else
- * BAD_INPUT with the reference's message); hs (RMDFT hard-sphere file) must
- * be NULL or "" in this build.
+ * BAD_INPUT with the reference's message); hs names the RMDFT hard-sphere
+ * file (NULL or "" for none), which also reads the .cvk beside the .xvk. 
  * `device` selects the GPU (main.cu -d) and `precision` the arithmetic. */
 int rism3d_initialize(rism3d_ctx **ctx, const char *control,
                       const char *structure, const char *esp, const char *hs,

@@ -167,6 +167,36 @@ def read_esp_cube(path: str, grid) -> np.ndarray:
     return np.ascontiguousarray(vals.reshape(nx, ny, nz).transpose(2, 1, 0)).ravel()
 
 
+@dataclass
+class HardSphere:
+    """RMDFT hard-sphere table (solvent_read.cc:118-140): site 0's packing
+    fraction and w(0), then rows k, chi_hs(k), w(k)."""
+    ntab2: int
+    pfhs: float
+    wfk0: float
+    k: np.ndarray
+    chs: np.ndarray
+    w: np.ndarray
+
+
+def read_hard_sphere(path: str) -> HardSphere:
+    with open(path) as f:
+        lines = f.read().split("\n")
+    ntab2 = int(lines[0].split()[0])
+    pf, w0 = (float(x) for x in lines[1].split()[:2])
+    rows = np.array([[float(x) for x in ln.split()[:3]] for ln in lines[2:2 + ntab2]])
+    if rows.shape != (ntab2, 3):
+        raise ValueError("short hard-sphere table %s" % path)
+    return HardSphere(ntab2, pf, w0, rows[:, 0].copy(), rows[:, 1].copy(), rows[:, 2].copy())
+
+
+def read_cvk(xvk_path: str) -> np.ndarray:
+    """solvent_read.cc:94-116: the solvent c(k) table next to the .xvk (same
+    stem, extension .cvk, same layout as the chi table); [natv][natv][ntab]."""
+    stem = xvk_path[:xvk_path.rfind(".")] if "." in xvk_path else xvk_path
+    return read_xvk(stem + ".cvk").xvv
+
+
 def parse_xmu(path: str) -> dict:
     """Key = value lines of an .xmu file (output_xmu.cu:7-111)."""
     out = {}

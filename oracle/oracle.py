@@ -36,6 +36,11 @@ class OracleInput(C.Structure):
         ("t_init", C.POINTER(C.c_double)),
         ("verbose", C.c_int),
         ("esp", C.POINTER(C.c_double)),
+        ("cvv", C.POINTER(C.c_double)),
+        ("ntab2", C.c_int),
+        ("ttab2", C.POINTER(C.c_double)), ("chs", C.POINTER(C.c_double)),
+        ("wfk", C.POINTER(C.c_double)),
+        ("pfhs", C.c_double), ("wfk0", C.c_double),
     ]
 
 
@@ -49,6 +54,7 @@ class OracleResult(C.Structure):
         ("correction", C.c_double), ("rms", C.c_double),
         ("iterations", C.c_int), ("status", C.c_int),
         ("t_setup", C.c_double), ("t_iter", C.c_double), ("t_obs", C.c_double),
+        ("sfe_rmdft", C.c_double),
     ]
 
 
@@ -83,7 +89,7 @@ class Case:
 
     def __init__(self, grid, box, solvent: F.Solvent, sig, eps, q, xyz,
                  closure=0, conv=1e-6, maxstep=10000, count=2, m=0.6, mp=0.2,
-                 chargeup=0, t_init=None, esp=None):
+                 chargeup=0, t_init=None, esp=None, cvv=None, hs=None):
         self.grid = tuple(int(g) for g in grid)
         self.box = tuple(float(b) for b in box)
         self.sv = solvent
@@ -93,6 +99,8 @@ class Case:
         self.count, self.m, self.mp, self.chargeup = count, m, mp, chargeup
         self.t_init = None if t_init is None else _f64(t_init)
         self.esp = None if esp is None else _f64(esp).ravel()
+        self.cvv = None if cvv is None else _f64(cvv)     # RMDFT: .cvk table
+        self.hs = hs                                       # RMDFT: F.HardSphere
         self._keep = []
 
     @property
@@ -116,6 +124,13 @@ class Case:
         s.t_init = _p(self.t_init)
         s.verbose = verbose
         s.esp = _p(self.esp)
+        if self.cvv is not None and self.hs is not None:
+            hs = [_f64(self.hs.k), _f64(self.hs.chs), _f64(self.hs.w)]
+            self._keep += hs
+            s.cvv = _p(self.cvv)
+            s.ntab2 = self.hs.ntab2
+            s.ttab2, s.chs, s.wfk = [_p(a) for a in hs]
+            s.pfhs, s.wfk0 = self.hs.pfhs, self.hs.wfk0
         return s
 
 
@@ -141,6 +156,8 @@ def solve(case: Case, want_grids=False, verbose=0):
     trace = np.zeros(max(1, case.maxstep * (case.chargeup + 1)))
     rc = L.oracle_solve(C.byref(s), C.byref(r), _p(g), _p(h), _p(t), _p(euv),
                         _p(dulj), _p(due), _p(trace))
+    if rc == -4:
+        raise ValueError("insufficient maximal T tabulated (hard-sphere table)")
     if rc != 0:
         raise RuntimeError("oracle_solve failed: %d" % rc)
     res = {k: getattr(r, k) for k, _ in OracleResult._fields_
@@ -190,10 +207,13 @@ def spline_eval(xp, yp, xq):
     return yq
 
 
-def write_xmu(res: dict, path: str, closure: int, natv: int):
+def write_xmu(res: dict, path: str, closure: int, natv: int, rmdft: bool = False):
     """output_xmu.cu:7-111 (fixed, 5 decimals)."""
     ib = res["ibeta"]
     L = [" $RESULT"]
+    if rmdft:                                        # output_xmu.cu:25-28
+        L.append("SFE_RMDFT= %.5f !(J/mol)" % res["sfe_rmdft"])
+        L.append("")
     L.append("SFE_SC= %.5f !(J/mol)" % (ib * res["xmu_sc"].sum()))
     L += ["  SFEC_SC(%d)= %.5f" % (i, ib * res["xmu_sc"][i]) for i in range(natv)]
     L.append("")

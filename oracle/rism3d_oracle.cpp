@@ -327,7 +327,8 @@ void potentials(const Problem &P, double *u, double *e, double *fr, cd *fk) {
 // (spline each X[a][b] at the unique |k|).  Returns 0 or -1 when the
 // largest |k| exceeds the table (solvent_spline.cu:18-21).
 int chi_table(const Problem &P, std::vector<int> &indga,
-              std::vector<double> &xuniq /* [nv][nv][nga] */, int &nga) {
+              std::vector<double> &xuniq /* [nv][nv][nga] */, int &nga,
+              std::vector<double> *ga_out = nullptr) {
   const OracleInput *in = P.in;
   std::vector<double> g2(P.n);
   for (size_t ip = 0; ip < P.n; ++ip) {
@@ -358,6 +359,7 @@ int chi_table(const Problem &P, std::vector<int> &indga,
   double dk = M_PI / (in->dr * ntab);           // solvent_read.cc:82-86
   for (int i = 0; i < ntab; ++i) ttab[i] = dk * (i + 1);
   if (ga[nga - 1] > ttab[ntab - 1]) return -1;
+  if (ga_out) *ga_out = ga;
   const int nv = P.nv;
   xuniq.assign((size_t)nv * nv * nga, 0.0);
   std::vector<double> c0, c1, c2;
@@ -391,6 +393,124 @@ double grid_sum(const Problem &P, F f) {
   double s = 0.0;
   for (long r = 0; r < rows; ++r) s += part[r];
   return s;
+}
+
+// excp_fd.cc:1-6: derivative of the hard-sphere excess free-energy density
+// at packing fraction pf and density dens
+double excp_fd(double pf, double dens) {
+  return (4.0 - 2.0 * pf) / ((1.0 - pf) * (1.0 - pf) * (1.0 - pf)) * (pf / dens);
+}
+
+// cal_rmdft.cu:5-115 with the tables of solvent_spline2.cu:7-103: the
+// solvent c(k) (.cvk) and the hard-sphere chi and weight of site 0 splined
+// at the unique |k|; cvva_vv -= chs_v rho_0 / rho_v; then
+//   xmu1 = -sum rho_v h_v,  w_v = F^-1[sum_v' c_vv' rho_v' H_v'],
+//   xmu2 = sum rho_v w_v,   xmu3 = sum rho_v w_v h_v,
+//   n_v = rho_0 + F^-1[rho_0 w_v H_v],
+//   f_v = rho_0 ((h_v + 1) excp_fd(a n_v, n_v) - excp_fd(pf_v, rho_0)), a = pf_v / rho_0,
+//   eda = sum rho_v ((F^-1[w_v F f_v] + e_v)(h_v + 1) - e_v),
+//         e_v = rho_0 excp_fd(pf_v, rho_0) w_v(0),
+// returning (xmu1 + xmu2 + xmu3 / 2 - eda) dv.  The file supplies site 0's
+// hard-sphere data only; the other sites' tables are zero (the reference
+// leaves them uninitialised).  h is transformed in place forth and back
+// as the reference does.  Returns 0, or -4 when the hard-sphere table does
+// not reach the largest |k| (solvent_spline2.cu:16-19).
+int rmdft(const Problem &P, const Shifted3D &fft, const std::vector<int> &indga,
+          const std::vector<double> &ga, std::vector<cd> huv, double *result) {
+  const OracleInput *in = P.in;
+  const int nv = P.nv, nga = (int)ga.size(), ntab = in->ntab, nt2 = in->ntab2;
+  const size_t n = P.n;
+  if (ga[nga - 1] > in->ttab2[nt2 - 1]) return -4;
+  std::vector<double> ttab(ntab);
+  const double dk = M_PI / (in->dr * ntab);
+  for (int i = 0; i < ntab; ++i) ttab[i] = dk * (i + 1);
+  std::vector<double> c0, c1, c2;
+  std::vector<double> cva((size_t)nv * nv * nga), chsa((size_t)nv * nga, 0.0),
+      wfka((size_t)nv * nga, 0.0), pf(nv, 0.0), w0(nv, 0.0);
+  for (int a = 0; a < nv; ++a)
+    for (int b = 0; b < nv; ++b) {               // solvent_spline.cu:50-62
+      const double *y = in->cvv + ((size_t)a * nv + b) * ntab;
+      spline_coe(ntab, ttab.data(), y, c0, c1, c2);
+      for (int i = 0; i < nga; ++i)
+        cva[((size_t)a * nv + b) * nga + i] = splint(ntab, ttab.data(), y, c0, c1, c2, ga[i]);
+    }
+  spline_coe(nt2, in->ttab2, in->chs, c0, c1, c2);
+  for (int i = 0; i < nga; ++i) chsa[i] = splint(nt2, in->ttab2, in->chs, c0, c1, c2, ga[i]);
+  spline_coe(nt2, in->ttab2, in->wfk, c0, c1, c2);
+  for (int i = 0; i < nga; ++i) wfka[i] = splint(nt2, in->ttab2, in->wfk, c0, c1, c2, ga[i]);
+  pf[0] = in->pfhs;
+  w0[0] = in->wfk0;
+  const double rho0 = in->rhov[0];
+  for (int v = 0; v < nv; ++v)                   // solvent_spline2.cu:65-70
+    for (int i = 0; i < nga; ++i)
+      cva[((size_t)v * nv + v) * nga + i] -= chsa[(size_t)v * nga + i] * rho0 / in->rhov[v];
+  double xmu1 = 0.0;
+  for (int v = 0; v < nv; ++v) {
+    const cd *h = &huv[(size_t)v * n];
+    xmu1 -= grid_sum(P, [&](size_t i) { return h[i].real(); }) * in->rhov[v];
+  }
+  for (int v = 0; v < nv; ++v) fft.forward(&huv[(size_t)v * n]);
+  std::vector<cd> work((size_t)nv * n);
+  for (int v = 0; v < nv; ++v) {                 // cal_dwork
+#pragma omp parallel for schedule(static)
+    for (long ip = 0; ip < (long)n; ++ip) {
+      const int ig = indga[ip];
+      cd s(0.0, 0.0);
+      for (int b = 0; b < nv; ++b)
+        s += huv[(size_t)b * n + ip] * (cva[((size_t)v * nv + b) * nga + ig] * in->rhov[b]);
+      work[(size_t)v * n + ip] = s;
+    }
+  }
+  for (int v = 0; v < nv; ++v) {
+    fft.inverse(&huv[(size_t)v * n]);
+    fft.inverse(&work[(size_t)v * n]);
+  }
+  double xmu2 = 0.0, xmu3 = 0.0;
+  for (int v = 0; v < nv; ++v) {
+    const cd *w = &work[(size_t)v * n];
+    xmu2 += grid_sum(P, [&](size_t i) { return w[i].real(); }) * in->rhov[v];
+  }
+  for (int v = 0; v < nv; ++v) {
+    const cd *w = &work[(size_t)v * n], *h = &huv[(size_t)v * n];
+    xmu3 += grid_sum(P, [&](size_t i) { return w[i].real() * h[i].real(); }) * in->rhov[v];
+  }
+  for (int v = 0; v < nv; ++v) fft.forward(&huv[(size_t)v * n]);
+  for (int v = 0; v < nv; ++v) {                 // rho0wfkhk
+    cd *w = &work[(size_t)v * n];
+    const cd *h = &huv[(size_t)v * n];
+#pragma omp parallel for schedule(static)
+    for (long ip = 0; ip < (long)n; ++ip) w[ip] = h[ip] * (rho0 * wfka[(size_t)v * nga + indga[ip]]);
+  }
+  for (int v = 0; v < nv; ++v) {
+    fft.inverse(&huv[(size_t)v * n]);
+    fft.inverse(&work[(size_t)v * n]);
+  }
+  for (int v = 0; v < nv; ++v) {                 // rho0, rho0guvfmbex
+    cd *w = &work[(size_t)v * n];
+    const cd *h = &huv[(size_t)v * n];
+    const double bex = excp_fd(pf[v], rho0), a = pf[v] / rho0;
+#pragma omp parallel for schedule(static)
+    for (long ip = 0; ip < (long)n; ++ip) {
+      const double dens = w[ip].real() + rho0;
+      w[ip] = cd(rho0 * ((h[ip].real() + 1.0) * excp_fd(a * dens, dens) - bex), 0.0);
+    }
+  }
+  for (int v = 0; v < nv; ++v) {                 // wfka between the transforms
+    cd *w = &work[(size_t)v * n];
+    fft.forward(w);
+#pragma omp parallel for schedule(static)
+    for (long ip = 0; ip < (long)n; ++ip) w[ip] *= wfka[(size_t)v * nga + indga[ip]];
+    fft.inverse(w);
+  }
+  double eda = 0.0;
+  for (int v = 0; v < nv; ++v) {                 // cal_eda
+    const cd *w = &work[(size_t)v * n], *h = &huv[(size_t)v * n];
+    const double ex = rho0 * excp_fd(pf[v], rho0) * w0[v];
+    eda += grid_sum(P, [&](size_t i) { return (w[i].real() + ex) * (h[i].real() + 1.0) - ex; }) *
+           in->rhov[v];
+  }
+  *result = (xmu1 + xmu2 + 0.5 * xmu3 - eda) * P.dv;
+  return 0;
 }
 
 // anderson.cu:87-112
@@ -475,9 +595,9 @@ extern "C" int oracle_solve(const OracleInput *in, OracleResult *out,
   std::vector<cd> fk(n);
   potentials(P, u.data(), e.data(), fr.data(), fk.data());
   std::vector<int> indga;
-  std::vector<double> xu;
+  std::vector<double> xu, ga;
   int nga;
-  if (chi_table(P, indga, xu, nga)) return -3;
+  if (chi_table(P, indga, xu, nga, &ga)) return -3;
   Shifted3D fft(P.nx, P.ny, P.nz, in->bx, in->by, in->bz);
   double w1 = omp_get_wtime();
   out->t_setup = w1 - w0;
@@ -746,6 +866,12 @@ extern "C" int oracle_solve(const OracleInput *in, OracleResult *out,
   if (h_out)
     for (size_t i = 0; i < (size_t)nv * n; ++i) h_out[i] = huv[i].real();
   if (t_out) std::copy(t.begin(), t.end(), t_out);
+  if (in->cvv) {                        // output.cu:25
+    double dft = 0.0;
+    int rc = rmdft(P, fft, indga, ga, huv, &dft);
+    if (rc) return rc;
+    out->sfe_rmdft = ibeta * dft;
+  }
   out->t_obs = omp_get_wtime() - w2;
   return 0;
 }

@@ -47,6 +47,12 @@ typedef struct {
   int verbose;
   const double *esp;    /* optional ESP cube values [N], Hartree/e, x fastest
                            (cal_Coulomb.cu:41-96); replaces the point-charge e */
+  /* optional RMDFT correction (cal_rmdft.cu:5-115, solvent_read.cc:88-140,
+     solvent_spline2.cu:7-103); cvv NULL = off */
+  const double *cvv;    /* [natv][natv][ntab] solvent c(k) on the chi knots (.cvk) */
+  int ntab2;            /* rows of the hard-sphere table */
+  const double *ttab2, *chs, *wfk;  /* [ntab2]: k, hard-sphere chi(k), weight w(k) */
+  double pfhs, wfk0;    /* packing fraction and w(k = 0); site 0 only */
 } OracleInput;
 
 typedef struct {
@@ -64,6 +70,7 @@ typedef struct {
   int iterations;                 /* total over charge-up stages */
   int status;                     /* 0 converged, 1 diverged, 2 maxstep */
   double t_setup, t_iter, t_obs;  /* wall seconds: potentials+chi, loop, output */
+  double sfe_rmdft;               /* J/mol, when RMDFT tables are given */
 } OracleResult;
 
 /* Full solve + observables.  Optional outputs (may be NULL):

@@ -45,6 +45,27 @@ def subsample_xvk(src, dst, step=4):
     open(dst, "w").write("\n".join(head + rows) + "\n")
 
 
+RMDFT_SRC = "/root/reference/example_rmdft"
+
+
+def rmdft_inputs():
+    """RMDFT example (example_rmdft: benzene in water, hard-sphere table
+    287.xsv), with the benzene atoms inline, on the example's own cell
+    (64 A, 256^3) and on a 64^3 cell of 32 A for the CPU oracle.  The tables
+    are copied whole: the reference leaves the hard-sphere rows of sites >= 1
+    uninitialised (solvent_read.cc:124-127 allocates them with new[]), and
+    only allocations as large as the example's 16384 rows came back zeroed
+    in its runs; smaller tables gave it heap garbage."""
+    for src, dst in (("h2o_vv.xvk", "rmdft_h2o_vv.xvk"), ("h2o_vv.cvk", "rmdft_h2o_vv.cvk"),
+                     ("287.xsv", "rmdft_287.xsv")):
+        shutil.copyfile(os.path.join(RMDFT_SRC, src), os.path.join(DST, dst))
+    atoms = open(os.path.join(RMDFT_SRC, "benzene")).read().strip().split("\n")
+    for name, box, grid in (("rmdft_benzene", 64, 256), ("rmdft_benzene64", 32, 64)):
+        head = [" m    0  20220301", " KH", " rmdft_h2o_vv.xvk", " 1.0e-6   10000", " 2   0.6   0.2",
+                "  %d  %d  %d" % (box, box, box), "  %d  %d  %d" % (grid, grid, grid)]
+        open(os.path.join(DST, name + ".inp"), "w").write("\n".join(head + atoms) + "\n")
+
+
 def main():
     if not os.path.isdir(SRC):
         sys.exit("reference examples not mounted")
@@ -53,6 +74,7 @@ def main():
     subsample_xvk(os.path.join(SRC, "naclaq_vv.xvk"), os.path.join(DST, "naclaq_sub4_vv.xvk"))
     for name in ("test1", "test2"):
         tighten(os.path.join(DST, name + ".inp"), os.path.join(DST, name + "_tight.inp"))
+    rmdft_inputs()
 
 
 if __name__ == "__main__":

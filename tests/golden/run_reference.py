@@ -20,10 +20,17 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 BIN = os.path.join(ROOT, "oracle", "_ref", "3drism-cuda")
 
 CASES = ["test1", "test1_tight", "test2", "test2_tight", "test3", "test4", "test4_tight",
-         "cfg0_chain12", "cfg1_globule300", "cfg2_protein846_kh", "cfg0_esp"]
+         "cfg0_chain12", "cfg1_globule300", "cfg2_protein846_kh", "cfg0_esp",
+         "rmdft_benzene"]
 # ESP-cube cases (-e, cal_Coulomb.cu:41-96): name -> control file reused;
 # the cube comes from make_esp.py
 ESP_CASES = {"cfg0_esp": "cfg0_chain12"}
+# RMDFT cases (-r, cal_rmdft.cu): hard-sphere table; the .cvk sits beside the
+# .xvk.  Only the example's own cell: the reference reads the hard-sphere rows
+# of sites >= 1 from uninitialised memory, which came back zeroed in this run
+# and held garbage on the 64^3 cell (SFE_RMDFT -12430.7 against -4422.5 with
+# zeros; ~1e128 with MALLOC_PERTURB_=165 on both cells).
+RMDFT_CASES = {"rmdft_benzene": "rmdft_287.xsv"}
 
 
 def run(case, outdir):
@@ -34,6 +41,11 @@ def run(case, outdir):
     solvent = open(src).read().split()[4]                                  # read_input.cu:42
     shutil.copyfile(os.path.join(HERE, solvent), os.path.join(d, solvent))
     args = [case + ".inp"]
+    if case in RMDFT_CASES:
+        cvk = solvent[:solvent.rfind(".")] + ".cvk"
+        shutil.copyfile(os.path.join(HERE, cvk), os.path.join(d, cvk))
+        shutil.copyfile(os.path.join(HERE, RMDFT_CASES[case]), os.path.join(d, RMDFT_CASES[case]))
+        args = ["-r", RMDFT_CASES[case]] + args
     if case in ESP_CASES:
         sys.path.insert(0, HERE)
         import make_esp

@@ -47,12 +47,24 @@ def load_esp_case(name="cfg0_esp", cube=None):
     return case, ctrl, sol
 
 
+def load_rmdft_case(name="rmdft_benzene64"):
+    """An RMDFT control file with its .cvk (beside the .xvk) and the
+    hard-sphere table rmdft_287.xsv (the -r input)."""
+    case, ctrl, sol = O.case_from_inp(os.path.join(GOLDEN, name + ".inp"))
+    case.cvv = F.read_cvk(os.path.join(GOLDEN, ctrl.fsolvent))
+    case.hs = F.read_hard_sphere(os.path.join(GOLDEN, "rmdft_287.xsv"))
+    return case, ctrl, sol
+
+
 def product_solver(case, precision=0, **kw):
     import rism3d_b200 as R
     s = R.Solver(case.grid, case.box, closure=case.closure, convergence=case.conv,
                  maxstep=case.maxstep, an2=(case.count, case.m, case.mp),
                  precision=precision, **kw)
     s.set_solvent_obj(case.sv)
+    if getattr(case, "cvv", None) is not None and getattr(case, "hs", None) is not None:
+        hs = case.hs
+        s.set_rmdft(case.cvv, hs.k, hs.chs, hs.w, hs.pfhs, hs.wfk0)
     if getattr(case, "esp", None) is not None:
         s.set_esp(case.esp)
     s.set_solute(case.sig, case.eps, case.q, case.xyz)

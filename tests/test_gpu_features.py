@@ -223,6 +223,53 @@ def test_bad_inputs_are_errors_not_exits(tmp_path):
     assert p.returncode == 1 and "short chi table" in p.stderr
 
 
+def _run_rmdft_cli(tmp_path, name):
+    d = tmp_path / name
+    d.mkdir()
+    for f in (name + ".inp", "rmdft_h2o_vv.xvk", "rmdft_h2o_vv.cvk", "rmdft_287.xsv"):
+        shutil.copyfile(os.path.join(GOLDEN, f), str(d / f))
+    p = subprocess.run([CLI, "-r", "rmdft_287.xsv", name + ".inp"], cwd=str(d),
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout + p.stderr
+    return F.parse_xmu(str(d / (name + ".xmu"))), p.stdout
+
+
+def test_rmdft_cli_matches_reference_executable(tmp_path):
+    """-r hard-sphere table + .cvk (cal_rmdft.cu:5-115) through the drop-in
+    executable on the reference's own RMDFT example (256^3): the .xmu of the
+    reference executable run on the same files, SFE_RMDFT line first."""
+    name = "rmdft_benzene"
+    got, out = _run_rmdft_cli(tmp_path, name)
+    ref = ref_xmu(name)
+    summary = json.load(open(os.path.join(GOLDEN, "ref_b200", "summary.json")))
+    assert list(got)[0] == "SFE_RMDFT" and set(got) == set(ref)
+    for k in ("SFE_SC", "SFE_SC_HNC", "SFE_GF"):
+        assert abs(got[k] - ref[k]) < MU_TOL, (k, got[k], ref[k])
+    assert abs(got["SFE_RMDFT"] - ref["SFE_RMDFT"]) < 0.01    # observed: equal to all digits
+    assert abs(got["PMV"] - ref["PMV"]) < 2e-5
+    n_ref = summary[name]["iterations"]
+    assert abs(out.count(" Step = ") - n_ref) <= max(2, 0.05 * n_ref)
+
+
+def test_rmdft_matches_oracle_and_switches_off():
+    import rism3d_b200 as R
+    from helpers import load_rmdft_case
+    case, _, _ = load_rmdft_case()
+    o, r, s = both(case)
+    assert abs(r["iterations"] - o["iterations"]) <= 1
+    assert abs(r["sfe_rmdft"] - o["sfe_rmdft"]) < 0.5, (r["sfe_rmdft"], o["sfe_rmdft"])
+    assert abs(r["sfe_sc"] - o["sfe_sc"]) < 1.0
+    # a hard-sphere table that stops below the grid's largest |k| is refused
+    hs = case.hs
+    cut = int(np.searchsorted(hs.k, 5.0))
+    with pytest.raises(R.RismError) as e:
+        s.set_rmdft(case.cvv, hs.k[:cut], hs.chs[:cut], hs.w[:cut], hs.pfhs, hs.wfk0)
+    assert e.value.code == R.BAD_INPUT
+    s.set_rmdft(None)
+    assert s.solve()["sfe_rmdft"] == 0.0
+    s.close()
+
+
 def test_esp_cube_cli_matches_reference_executable(tmp_path):
     """-e ESP cube (cal_Coulomb.cu:41-96) through the drop-in executable: the
     same cube and control file as the reference executable's recorded run;

@@ -110,3 +110,28 @@ def test_esp_of_the_point_charges_reproduces_the_coulomb_grid():
     _, e1, fr1, _ = O.potentials(case)
     assert np.array_equal(fr0, fr1)
     assert np.abs(e1 - e0).max() <= 1e-12 * np.abs(e0).max()
+
+
+def test_oracle_rmdft_reproduces_reference_binary(tmp_path, golden):
+    """-r (cal_rmdft.cu:5-115): the reference's own RMDFT example (benzene in
+    water, 256^3 cell of 64 A, its .cvk and hard-sphere tables), run by the
+    reference executable on a B200; the oracle reproduces the .xmu, the
+    SFE_RMDFT line included, to its printed digits (about 100 s here: the
+    only deterministic reference output for RMDFT, since the reference takes
+    the hard-sphere rows of sites >= 1 from uninitialised memory, which held
+    garbage on smaller cells)."""
+    from helpers import load_rmdft_case
+    case, _, _ = load_rmdft_case("rmdft_benzene")
+    res = O.solve(case)
+    summary = json.load(open(os.path.join(golden, "ref_b200", "summary.json")))
+    assert res["iterations"] == summary["rmdft_benzene"]["iterations"]
+    got = oracle_xmu_rmdft(res, tmp_path, case)
+    ref = ref_xmu("rmdft_benzene")
+    for k in KEYS + ["SFE_RMDFT"]:
+        assert abs(got[k] - ref[k]) <= 2e-5 + 2e-9 * abs(ref[k]), (k, got[k], ref[k])
+
+
+def oracle_xmu_rmdft(res, tmp_path, case):
+    p = tmp_path / "r.xmu"
+    O.write_xmu(res, str(p), case.closure, case.sv.natv, rmdft=True)
+    return F.parse_xmu(str(p))
