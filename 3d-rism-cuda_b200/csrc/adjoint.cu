@@ -397,7 +397,7 @@ struct Scratch {
   explicit Scratch(Context &cc) : c(cc) {}
   template <typename T> T *get(size_t count) {
     void *p = nullptr;
-    if (cudaMallocAsync(&p, sizeof(T) * count, c.stream) != cudaSuccess) return nullptr;
+    if (pool_alloc(c, &p, sizeof(T) * count) != cudaSuccess) return nullptr;
     ptrs.push_back(p);
     return (T *)p;
   }

@@ -5,6 +5,7 @@
 // fallback.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -44,6 +45,8 @@ void context_release(Context &c) {
   }
   if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);
   c.stream = nullptr;
+  if (c.pool) cudaMemPoolDestroy(c.pool);
+  c.pool = nullptr;
 }
 
 bool cuda_ok(Context &c, cudaError_t e, const char *what) {
@@ -236,6 +239,22 @@ int context_init(Context &c, const rism3d_params *p, int nb, std::string &err) {
     err = "cannot create a CUDA stream";
     return RISM3D_CUDA_ERROR;
   }
+  {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = c.dev;
+    uint64_t keep = ~0ull;
+    if (cudaMemPoolCreate(&c.pool, &props) != cudaSuccess ||
+        cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+      err = "cannot create a CUDA memory pool";
+      if (c.pool) cudaMemPoolDestroy(c.pool);
+      c.pool = nullptr;
+      if (c.own_stream) cudaStreamDestroy(c.stream);
+      c.stream = nullptr;
+      return RISM3D_CUDA_ERROR;
+    }
+  }
   c.nx = p->grid[0]; c.ny = p->grid[1]; c.nz = p->grid[2];
   c.n = (long long)c.nx * c.ny * c.nz;
   c.vol = p->box[0] * p->box[1] * p->box[2];             // cell.cc:9-14
@@ -272,6 +291,8 @@ int context_init(Context &c, const rism3d_params *p, int nb, std::string &err) {
     free_device(c);
     if (c.own_stream) cudaStreamDestroy(c.stream);
     c.stream = nullptr;
+    cudaMemPoolDestroy(c.pool);
+    c.pool = nullptr;
     return RISM3D_CUDA_ERROR;
   }
   return RISM3D_OK;
@@ -490,7 +511,10 @@ int rism3d_solve(rism3d_ctx *x, int chargeup, rism3d_result *res) {
   if (rc != RISM3D_OK) return rc;
   cudaEventRecord(c.tm_obs.a, c.stream);
   rc = compute_observables(c);
-  if (rc == RISM3D_OK) rc = compute_atom_integrals(c, false);
+  // SE: from the grids for one solute with the point-charge potential; per
+  // (site, atom) pairs otherwise (an ESP cube is not the atoms' potential)
+  if (rc == RISM3D_OK)
+    rc = (c.nb == 1 && !c.d_esp) ? compute_se_from_grids(c) : compute_atom_integrals(c, false);
   if (rc == RISM3D_OK) rc = compute_rmdft(c);                // output.cu:25
   cudaEventRecord(c.tm_obs.b, c.stream);
   if (rc != RISM3D_OK) return rc;
@@ -505,10 +529,24 @@ int rism3d_solve(rism3d_ctx *x, int chargeup, rism3d_result *res) {
   return RISM3D_OK;
 }
 
+// the per-(site, atom) pair integrals (and forces) after a solve whose SE
+// came from the grids; the reported SE totals stay those of the solve
+static int atom_integrals_keep_se(Context &c, bool forces) {
+  const double se = c.res.se, lj = c.res.se_lj, es = c.res.se_es;
+  int rc = compute_atom_integrals(c, forces);
+  c.res.se = se; c.res.se_lj = lj; c.res.se_es = es;
+  return rc;
+}
+
 int rism3d_euv(rism3d_ctx *x, double *euv) {
   if (!x || !euv) return RISM3D_BAD_INPUT;
   Context &c = x->c;
+  cudaSetDevice(c.dev);
   if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
+  if (c.euv.empty()) {
+    int rc = atom_integrals_keep_se(c, false);
+    if (rc != RISM3D_OK) return rc;
+  }
   std::copy(c.euv.begin(), c.euv.end(), euv);
   return RISM3D_OK;
 }
@@ -519,7 +557,7 @@ int rism3d_forces(rism3d_ctx *x, double *dulj, double *due) {
   cudaSetDevice(c.dev);
   if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
   if (!c.have_forces) {
-    int rc = compute_atom_integrals(c, true);
+    int rc = atom_integrals_keep_se(c, true);
     if (rc != RISM3D_OK) return rc;
   }
   std::copy(c.dulj.begin(), c.dulj.end(), dulj);
@@ -757,7 +795,13 @@ int rism3d_output(rism3d_ctx *x) {
     io::write_grid_text(c.fname + ".huv", c.prm.box, c.prm.grid, c.natom, c.q.data(), c.sig.data(),
                         c.eps.data(), c.xyz.data(), c.natv, buf.data(), c.n);
   }
-  if (has('e')) io::write_euv(c.fname + ".euv", c.natom, c.natv, c.euv.data());
+  if (has('e')) {
+    if (c.euv.empty()) {
+      int rc = atom_integrals_keep_se(c, false);
+      if (rc != RISM3D_OK) return rc;
+    }
+    io::write_euv(c.fname + ".euv", c.natom, c.natv, c.euv.data());
+  }
   if (has('q')) {
     buf.resize(n);
     fetch_grid(c, RISM3D_GRID_QV, buf.data());

@@ -489,6 +489,161 @@ int atoms_v(Context &c, bool forces) {
 
 }  // namespace
 
+// SE totals from the grids (single solute, point-charge potential).  The
+// reference's per-(site, atom) sums over r >= sigma_uv / 2 (cal_euv.cu:7-76)
+// add up, over the atoms, to one sum over the grid of g times the potential
+// grids the solve already holds -- u_v = sum_u beta u_LJ,uv with r^2 clamped
+// at 1e-4 (cal_LJ.cu:57-71) and e = esr + fr = beta sum_u q_u / r over
+// r >= 1e-5 (cal_Coulomb.cu:109-121) -- minus each atom's own terms at the
+// grid points inside its exclusion sphere r < sigma_uv / 2, where g is
+// essentially zero.  That is one streaming pass plus a few thousand points
+// per atom, in place of every (point, atom) pair.
+template <int V>
+__global__ void __launch_bounds__(kThreads)
+k_se_grid(long long n, const double *__restrict__ g, const double *__restrict__ u,
+          const double *__restrict__ esr, const double *__restrict__ fr, double *part) {
+  double acc[2 * V];
+#pragma unroll
+  for (int i = 0; i < 2 * V; ++i) acc[i] = 0.0;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const double e = esr[j] + fr[j];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const double gv = g[(size_t)v * n + j];
+      acc[v] += gv * u[(size_t)v * n + j];
+      acc[V + v] += gv * e;
+    }
+  }
+  __shared__ double red[kThreads / 32][2 * V];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int i = 0; i < 2 * V; ++i) {
+    double v = acc[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[wid][i] = v;
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < 2 * V) {
+    double t = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) t += red[w][threadIdx.x];
+    part[(size_t)blockIdx.x * 2 * V + threadIdx.x] = t;
+  }
+}
+
+// One atom per block: its LJ (beta units, clamped as in the grid) and q / r
+// (r >= 1e-5) terms times g at the grid points with r < sigma_uv / 2,
+// per site; part[atom][2V]
+template <int V>
+__global__ void __launch_bounds__(kThreads)
+k_se_core(int nx, int ny, int nz, double drx, double dry, double drz,
+          const double *__restrict__ g, const double *__restrict__ atoms, SiteAll sv,
+          double ikbt, double *part) {
+  const double *a = atoms + 8 * (size_t)blockIdx.x;
+  const double X = a[0], Y = a[1], Z = a[2], q = a[3];
+  double half[V], s2uv[V], e4[V], rmax = 0.0;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    const double sg = (a[4] + sv.sig[v]) * 0.5;                     // cal_euv.cu:31-32
+    half[v] = sg * 0.5;
+    s2uv[v] = sg * sg;
+    e4[v] = 4.0 * sqrt(a[5] * sv.eps[v]) * ikbt;
+    rmax = fmax(rmax, half[v]);
+  }
+  const long long n = (long long)nx * ny * nz;
+  // grid coordinates (i - n/2) d (cal_LJ.cu:54-56): the index box of the sphere
+  const int x0 = max(0, (int)floor((X - rmax) / drx) + nx / 2 - 1);
+  const int x1 = min(nx - 1, (int)ceil((X + rmax) / drx) + nx / 2 + 1);
+  const int y0 = max(0, (int)floor((Y - rmax) / dry) + ny / 2 - 1);
+  const int y1 = min(ny - 1, (int)ceil((Y + rmax) / dry) + ny / 2 + 1);
+  const int z0 = max(0, (int)floor((Z - rmax) / drz) + nz / 2 - 1);
+  const int z1 = min(nz - 1, (int)ceil((Z + rmax) / drz) + nz / 2 + 1);
+  const long long wx = x1 - x0 + 1, wy = y1 - y0 + 1, wz = z1 - z0 + 1;
+  const long long pts = (wx > 0 && wy > 0 && wz > 0) ? wx * wy * wz : 0;
+  double acc[2 * V];
+#pragma unroll
+  for (int i = 0; i < 2 * V; ++i) acc[i] = 0.0;
+  for (long long p = threadIdx.x; p < pts; p += blockDim.x) {
+    const int ix = x0 + (int)(p % wx);
+    const int iy = y0 + (int)((p / wx) % wy);
+    const int iz = z0 + (int)(p / (wx * wy));
+    const double dx = (ix - nx / 2) * drx - X, dy = (iy - ny / 2) * dry - Y,
+                 dz = (iz - nz / 2) * drz - Z;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double r = sqrt(r2);
+    const double ir2 = r2 < 1.0e-4 ? 1.0e4 : 1.0 / r2;
+    const long long j = ix + (long long)nx * (iy + (long long)ny * iz);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      if (r < half[v]) {
+        const double gv = g[(size_t)v * n + j];
+        const double s2 = s2uv[v] * ir2, s6 = s2 * s2 * s2;
+        acc[v] += gv * e4[v] * s6 * (s6 - 1.0);
+        if (r >= 1.0e-5) acc[V + v] += gv * q / r;
+      }
+    }
+  }
+  __shared__ double red[kThreads / 32][2 * V];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int i = 0; i < 2 * V; ++i) {
+    double v = acc[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[wid][i] = v;
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < 2 * V) {
+    double t = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) t += red[w][threadIdx.x];
+    part[(size_t)blockIdx.x * 2 * V + threadIdx.x] = t;
+  }
+}
+
+constexpr int kSeGridBlocks = 148 * 8;
+
+template <int V>
+int se_grid_v(Context &c) {
+  const int A = c.natom;
+  double *part = nullptr;
+  const size_t np = (size_t)(kSeGridBlocks + A) * 2 * V;
+  if (!cuda_ok(c, pool_alloc(c, (void **)&part, sizeof(double) * np), "SE partials"))
+    return RISM3D_CUDA_ERROR;
+  SiteAll sv{};
+  for (int v = 0; v < V; ++v) {
+    sv.sig[v] = c.sigv[v]; sv.eps[v] = c.epsv[v]; sv.q[v] = c.qv[v]; sv.rho[v] = c.rho[v];
+  }
+  const double ikbt = 1.0 / (kAvogadro * kBoltzmann * c.temper);
+  k_se_grid<V><<<kSeGridBlocks, kThreads, 0, c.stream>>>(c.n, c.d_g, c.d_u, c.d_e, c.d_fr, part);
+  k_se_core<V><<<A, kThreads, 0, c.stream>>>(c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_g,
+                                             c.d_atoms, sv, ikbt,
+                                             part + (size_t)kSeGridBlocks * 2 * V);
+  c.launches += 2;
+  std::vector<double> h(np);
+  bool ok = cuda_ok(c, cudaGetLastError(), "SE grid") &&
+            cuda_ok(c, cudaMemcpyAsync(h.data(), part, sizeof(double) * np, cudaMemcpyDeviceToHost,
+                                       c.stream), "SE grid");
+  cudaFreeAsync(part, c.stream);
+  if (!ok || !cuda_ok(c, cudaStreamSynchronize(c.stream), "SE grid")) return RISM3D_CUDA_ERROR;
+  double sg[2 * V] = {}, sc[2 * V] = {};
+  for (int b = 0; b < kSeGridBlocks; ++b)
+    for (int i = 0; i < 2 * V; ++i) sg[i] += h[(size_t)b * 2 * V + i];
+  for (int u = 0; u < A; ++u)
+    for (int i = 0; i < 2 * V; ++i) sc[i] += h[(size_t)(kSeGridBlocks + u) * 2 * V + i];
+  const double ibeta = kAvogadro * kBoltzmann * c.temper;               // J/mol per beta unit
+  const double ubeta = kHartree * kBohr / (kBoltzmann * c.temper);      // e grid per q / r
+  const double cc = kHartree * kBohr * kAvogadro;                       // cal_euv.cu:39
+  double slj = 0.0, ses = 0.0;
+  for (int v = 0; v < V; ++v) {
+    slj += c.rho[v] * ibeta * (sg[v] - sc[v]) * c.dv;
+    ses += c.rho[v] * c.qv[v] * cc * (sg[V + v] / ubeta - sc[V + v]) * c.dv;
+  }
+  c.res.se_lj = slj;
+  c.res.se_es = ses;
+  c.res.se = slj + ses;
+  c.euv.clear();                    // per-atom values on request (rism3d_euv)
+  return RISM3D_OK;
+}
+
 int compute_observables(Context &c) {
   switch (c.natv) {
     case 1: return observe_v<1>(c);
@@ -499,6 +654,20 @@ int compute_observables(Context &c) {
     case 6: return observe_v<6>(c);
     case 7: return observe_v<7>(c);
     case 8: return observe_v<8>(c);
+  }
+  return RISM3D_UNSUPPORTED_SHAPE;
+}
+
+int compute_se_from_grids(Context &c) {
+  switch (c.natv) {
+    case 1: return se_grid_v<1>(c);
+    case 2: return se_grid_v<2>(c);
+    case 3: return se_grid_v<3>(c);
+    case 4: return se_grid_v<4>(c);
+    case 5: return se_grid_v<5>(c);
+    case 6: return se_grid_v<6>(c);
+    case 7: return se_grid_v<7>(c);
+    case 8: return se_grid_v<8>(c);
   }
   return RISM3D_UNSUPPORTED_SHAPE;
 }

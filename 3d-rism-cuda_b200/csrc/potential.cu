@@ -312,7 +312,7 @@ int compute_potentials(Context &c) {
   if (!cuda_ok(c, cudaGetLastError(), "k_potential_r")) return RISM3D_CUDA_ERROR;
   const long long L = c.nx + c.ny + c.nz;
   double2 *ph = nullptr;
-  if (!cuda_ok(c, cudaMallocAsync(&ph, sizeof(double2) * L * c.natom, c.stream), "phase rows"))
+  if (!cuda_ok(c, pool_alloc(c, (void **)&ph, sizeof(double2) * L * c.natom), "phase rows"))
     return RISM3D_CUDA_ERROR;
   k_phase_rows<<<(unsigned)((L * c.natom + 255) / 256), 256, 0, c.stream>>>(
       c.nx, c.ny, c.nz, c.prm.box[0], c.prm.box[1], c.prm.box[2], c.d_atoms, c.natom, ph);

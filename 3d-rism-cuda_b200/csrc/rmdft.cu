@@ -257,8 +257,8 @@ int rmdft_v(Context &c) {
     return RISM3D_CUFFT_ERROR;
   double2 *buf = c.d_buf, *buf2 = nullptr;      // the solve is finished: buf is free
   double *part = nullptr;
-  if (!cuda_ok(c, cudaMallocAsync(&buf2, sizeof(double2) * n, c.stream), "RMDFT buffer") ||
-      !cuda_ok(c, cudaMallocAsync(&part, sizeof(double) * kRedBlocks * 4, c.stream), "RMDFT sums"))
+  if (!cuda_ok(c, pool_alloc(c, (void **)&buf2, sizeof(double2) * n), "RMDFT buffer") ||
+      !cuda_ok(c, pool_alloc(c, (void **)&part, sizeof(double) * kRedBlocks * 4), "RMDFT sums"))
     return RISM3D_CUDA_ERROR;
   RmArgs r{};
   r.n = n; r.nx = c.nx; r.ny = c.ny; r.nz = c.nz;

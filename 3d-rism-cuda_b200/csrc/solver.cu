@@ -1142,7 +1142,7 @@ int solve_v(Context &c, int chargeup) {
   cudaMemcpyAsync(c.d_stage, &sp, sizeof(sp), cudaMemcpyHostToDevice, c.stream);
   double *d_tinit = nullptr;
   if (restart) {
-    if (!cuda_ok(c, cudaMallocAsync(&d_tinit, sizeof(double) * V * n, c.stream), "alloc") ||
+    if (!cuda_ok(c, pool_alloc(c, (void **)&d_tinit, sizeof(double) * V * n), "alloc") ||
         !cuda_ok(c, cudaMemcpyAsync(d_tinit, c.t_init.data(), sizeof(double) * V * n, cudaMemcpyHostToDevice, c.stream), "copy"))
       return RISM3D_CUDA_ERROR;
   }
@@ -1153,7 +1153,7 @@ int solve_v(Context &c, int chargeup) {
   int status = RISM3D_OK;
   std::vector<DevState> fs(nb);
   StageParams *d_step = nullptr;
-  if (cu > 0 && !cuda_ok(c, cudaMallocAsync(&d_step, sizeof(StageParams), c.stream), "alloc"))
+  if (cu > 0 && !cuda_ok(c, pool_alloc(c, (void **)&d_step, sizeof(StageParams)), "alloc"))
     return RISM3D_CUDA_ERROR;
   for (int s = 0; s <= cu; ++s) {
     if (s > 0) {                                  // add_tuv (iterate.cu:43-47)

@@ -205,8 +205,10 @@ def run_ours(args, rank, world, dist):
     barrier(); torch.cuda.synchronize()
     torch.cuda.nvtx.range_push("fp64_solve")
     e0.record(stream)
+    res64 = []
     for _ in range(args.steps):
         fp64.refresh_potentials(); r64 = fp64.solve()
+        res64.append(r64)
     e1.record(stream)
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
@@ -270,10 +272,14 @@ def run_ours(args, rank, world, dist):
                    "l2": "state ~5 GB per solve >> 126 MB L2 (no flush needed)",
                    "parallelism": "replicas" if world > 1 else "1 GPU"},
         "fp64": {"s_per_solve": ms_fp64 / 1e3 / world, "iterations": r64["iterations"],
-                 "sfe_sc": r64["sfe_sc"]},
+                 "sfe_sc": r64["sfe_sc"],
+                 "per_solve_ms": [[round(r[k], 2) for k in ("ms_setup", "ms_iterate", "ms_observe")]
+                                  for r in res64]},
         "mixed": {"iterations": rm["iterations"], "iterations_fp32": rm["iterations_fp32"],
                   "sfe_sc": rm["sfe_sc"], "ms_setup": rm["ms_setup"],
-                  "ms_iterate": rm["ms_iterate"], "ms_observe": rm["ms_observe"]},
+                  "ms_iterate": rm["ms_iterate"], "ms_observe": rm["ms_observe"],
+                  "per_solve_ms": [[round(r[k], 2) for k in ("ms_setup", "ms_iterate", "ms_observe")]
+                                   for r in res]},
         "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
         "dmu_mixed_vs_fp64_j_per_mol": dmu, "dmu_within_0.01kcal": dmu <= 0.01 * KCAL,
         "e2e": {"value": s_e2e / world, "unit": "s/solve", "h2d_bytes_per_step": h2d,
