@@ -107,7 +107,11 @@ typedef struct rism3d_ctx rism3d_ctx;
 
 /* Allocate a context on params->device.  Replaces the implicit RISM3D
  * constructor + Cell::setup (cell.cc:8-22) + FFT3D::initialize
- * (fft3d.cu:4-19). */
+ * (fft3d.cu:4-19).  Besides its grids, the context owns a stream-ordered
+ * memory pool for per-solve scratch (potential phase rows, partial sums,
+ * the RMDFT buffer, the adjoint's history).  The pool keeps what it has
+ * allocated until rism3d_destroy; the device's default pool is not
+ * touched. */
 int rism3d_create(const rism3d_params *params, rism3d_ctx **ctx);
 
 /* Solvent sites after merging equivalent sites (solvent_read.cc:68-80):
@@ -199,6 +203,8 @@ int rism3d_solve_batch(rism3d_ctx *ctx, int nmol, const int *natoms,
                        const double *sig, const double *eps, const double *q,
                        const double *xyz, rism3d_result *results);
 
+/* Free the context: its grids, plans, stream (unless caller-owned), batch
+ * children and memory pool. */
 void rism3d_destroy(rism3d_ctx *ctx);
 
 /* Allocation-free mu_ex / PMV integrals.  No counterpart in the reference
