@@ -273,9 +273,12 @@ int rmdft_v(Context &c) {
   r.bex = fd_bulk(c.rm_pfhs, r.rho0);
   r.ex = r.rho0 * r.bex * c.rm_w0;
   const int gk = (int)std::min<long long>((n / 2 + kThr - 1) / kThr, 148 * 16);
+  bool fft_failed = false;
   auto fft = [&](cufftHandle pl, double2 *a, int d) {
-    return cufft_ok(c, cufftExecZ2Z(pl, (cufftDoubleComplex *)a, (cufftDoubleComplex *)a, d),
-                    "RMDFT transform");
+    const bool good = cufft_ok(
+        c, cufftExecZ2Z(pl, (cufftDoubleComplex *)a, (cufftDoubleComplex *)a, d), "RMDFT transform");
+    fft_failed = fft_failed || !good;
+    return good;
   };
   k_pack<<<kRedBlocks, kThr, 0, c.stream>>>(n, V, c.nx, c.ny, c.d_tw, c.d_h, buf);
   bool ok = fft(c.plan64, buf, CUFFT_FORWARD);
@@ -300,7 +303,7 @@ int rmdft_v(Context &c) {
   cudaFreeAsync(buf2, c.stream);
   cudaFreeAsync(part, c.stream);
   if (!ok || !cuda_ok(c, cudaStreamSynchronize(c.stream), "RMDFT"))
-    return c.err.find("cuFFT") != std::string::npos ? RISM3D_CUFFT_ERROR : RISM3D_CUDA_ERROR;
+    return fft_failed ? RISM3D_CUFFT_ERROR : RISM3D_CUDA_ERROR;
   double s[4] = {0.0, 0.0, 0.0, 0.0};
   for (int b = 0; b < kRedBlocks; ++b)
     for (int k = 0; k < 3; ++k) s[k] += hp[(size_t)b * 3 + k];

@@ -168,9 +168,10 @@ int rism3d_set_esp(rism3d_ctx *ctx, const double *esp);
  * ntab2 rows of k[i] (ascending), chs[i] (hard-sphere chi(k)) and w[i]
  * (weight function), its packing fraction pfhs and w(k = 0) w0.  Every
  * later solve reports SFE_RMDFT in rism3d_result.sfe_rmdft and the .xmu.
- * cvk NULL switches it off.  Call after rism3d_set_solvent; BAD_INPUT when
- * the hard-sphere table ends below the grid's largest |k|.  Single-solute
- * contexts. */
+ * cvk NULL switches it off, and so does any failed call.  Call after
+ * rism3d_set_solvent (which also switches it off); BAD_INPUT when the
+ * hard-sphere table ends below the grid's largest |k| or its knots do not
+ * increase.  Single-solute contexts. */
 int rism3d_set_rmdft(rism3d_ctx *ctx, const double *cvk, int ntab2, const double *k,
                      const double *chs, const double *w, double pfhs, double w0);
 
