@@ -30,7 +30,9 @@
 // agree at the solution.
 //
 // Kernels: the linear solve reuses the k-space OZ pass of the iteration
-// around cuFFT and is accelerated by Anderson mixing (depth 6); the gradient
+// around cuFFT and is accelerated by Anderson mixing (depth 6; per step one
+// fused pass forms the residual, the mixing vector and the Gram dots, and one
+// pass combines the stored mixing vectors); the gradient
 // back-propagates the weights through the potential-grid computation, one
 // atom per thread with grid points streamed through shared memory and every
 // pair term recomputed (cal_LJ.cu:57-71, cal_Coulomb.cu:109-121), and through
@@ -93,27 +95,33 @@ __global__ void k_gprime(long long tot, int closure, const double *t, const doub
   }
 }
 
-// r = (G - 1)(w + L xi) - G xi
-__global__ void k_residual(long long tot, const double *G, const double *w, const double *Lxi,
-                           const double *xi, double *r) {
-  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
-       f += (long long)gridDim.x * blockDim.x)
-    r[f] = (G[f] - 1.0) * (w[f] + Lxi[f]) - G[f] * xi[f];
-}
-
-// partial dot products of r with the first ns history residuals and with
-// itself (last row); summed in a fixed order by k_sum_rows
-__global__ void k_dots(long long tot, const double *r, const double *const *hist, int ns,
-                       double *part) {
+// One Anderson step's bookkeeping in one pass:
+//   r = (G - 1)(w + L xi) - G xi          into residual slot `slot`
+//   y = xi + eta r                        into mixing slot `slot`
+// and the partial dots of r with the first ns residual slots (the slot
+// itself contributes |r|^2) and |r|^2 (last row), summed in a fixed order by
+// k_sum_rows.  The other slots are read before the slot is written.
+__global__ void __launch_bounds__(kThreads)
+k_residual_dots(long long tot, const double *__restrict__ G, const double *__restrict__ w,
+                const double *__restrict__ Lxi, const double *__restrict__ xi, double eta,
+                double *const *rs, int slot, int ns, double *__restrict__ ys, double *part) {
   __shared__ double red[kThreads / 32][kDepth + 1];
   double acc[kDepth + 1];
+#pragma unroll
   for (int i = 0; i <= kDepth; ++i) acc[i] = 0.0;
+  double *__restrict__ rslot = rs[slot];
   for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
        f += (long long)gridDim.x * blockDim.x) {
-    const double x = r[f];
-    acc[kDepth] += x * x;
-    for (int i = 0; i < ns; ++i) acc[i] += x * hist[i][f];
+    const double g = G[f], x = xi[f];
+    const double r = (g - 1.0) * (w[f] + Lxi[f]) - g * x;
+#pragma unroll
+    for (int i = 0; i < kDepth; ++i)
+      if (i < ns) acc[i] += r * (i == slot ? r : rs[i][f]);
+    acc[kDepth] += r * r;
+    rslot[f] = r;
+    ys[f] = x + eta * r;
   }
+#pragma unroll
   for (int i = 0; i <= kDepth; ++i) {
     double v = acc[i];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -121,12 +129,13 @@ __global__ void k_dots(long long tot, const double *r, const double *const *hist
   }
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (lane == 0)
+#pragma unroll
     for (int i = 0; i <= kDepth; ++i) red[wid][i] = acc[i];
   __syncthreads();
   if (threadIdx.x <= kDepth) {
-    double s = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) s += red[w][threadIdx.x];
-    part[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = s;
+    double t = 0.0;
+    for (int v = 0; v < kThreads / 32; ++v) t += red[v][threadIdx.x];
+    part[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
   }
 }
 
@@ -145,19 +154,19 @@ __global__ void k_sum_rows(const double *part, int ncols, double *out) {
 }
 
 struct Mix {
-  const double *xs[kDepth];
-  const double *rs[kDepth];
+  const double *ys[kDepth];   // xi_i + eta r_i of the stored steps
   double c[kDepth];
   int ns;
-  double eta;
 };
 
-// xi = sum_i c_i (xi_i + eta r_i)
+// xi = sum_i c_i y_i, y_i = xi_i + eta r_i
 __global__ void k_combine(long long tot, Mix mx, double *xi) {
   for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
        f += (long long)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int i = 0; i < mx.ns; ++i) s += mx.c[i] * (mx.xs[i][f] + mx.eta * mx.rs[i][f]);
+#pragma unroll
+    for (int i = 0; i < kDepth; ++i)
+      if (i < mx.ns) s += mx.c[i] * mx.ys[i][f];
     xi[f] = s;
   }
 }
@@ -452,14 +461,14 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
   Scratch S(c);
   double *G = S.get<double>(tot), *w = S.get<double>(tot), *xi = S.get<double>(tot);
   double *Lxi = S.get<double>(tot), *tmp = S.get<double>(tot), *Om = S.get<double>(n);
-  double *xs = S.get<double>((size_t)kDepth * tot), *rs = S.get<double>((size_t)kDepth * tot);
+  double *ys = S.get<double>((size_t)kDepth * tot), *rs = S.get<double>((size_t)kDepth * tot);
   double *dpart = S.get<double>((size_t)(kDepth + 1) * kDotBlocks);
   double *dsum = S.get<double>(kDepth + 1);
   double **hist = S.get<double *>(kDepth);
   StageParams *sp0 = S.get<StageParams>(1), *spq = S.get<StageParams>(1);
   DevState *st0 = S.get<DevState>(1);
   double2 *buf = c.d_buf;                       // the solve is finished: reuse
-  if (!G || !w || !xi || !Lxi || !tmp || !Om || !xs || !rs || !dpart || !dsum || !hist ||
+  if (!G || !w || !xi || !Lxi || !tmp || !Om || !ys || !rs || !dpart || !dsum || !hist ||
       !sp0 || !spq || !st0) {
     c.err = "adjoint: out of device memory";
     return RISM3D_CUDA_ERROR;
@@ -506,7 +515,7 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
   const auto w0 = std::chrono::steady_clock::now();
   // Anderson-accelerated solve of G xi - (G - 1) L xi = (G - 1) w from xi = 0
   cudaMemsetAsync(xi, 0, sizeof(double) * tot, c.stream);
-  cudaMemsetAsync(xs, 0, sizeof(double) * kDepth * tot, c.stream);
+  cudaMemsetAsync(ys, 0, sizeof(double) * kDepth * tot, c.stream);
   cudaMemsetAsync(rs, 0, sizeof(double) * kDepth * tot, c.stream);
   std::vector<double> gram((size_t)kDepth * kDepth, 0.0), coef;
   double bnorm = -1.0;
@@ -516,14 +525,11 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
   for (; it < maxit; ++it) {
     rc = applyL(xi, Lxi);
     if (rc != RISM3D_OK) return rc;
-    double *r = rs + (size_t)slot * tot;
-    k_residual<<<gt, kThreads, 0, c.stream>>>(tot, G, w, Lxi, xi, r);
-    cudaMemcpyAsync(xs + (size_t)slot * tot, xi, sizeof(double) * tot, cudaMemcpyDeviceToDevice,
-                    c.stream);
     const int nd = ns < kDepth ? ns + 1 : kDepth;      // filled slots incl. this one
-    k_dots<<<kDotBlocks, kThreads, 0, c.stream>>>(tot, r, hist, nd, dpart);
+    k_residual_dots<<<kDotBlocks, kThreads, 0, c.stream>>>(
+        tot, G, w, Lxi, xi, eta, hist, slot, nd, ys + (size_t)slot * tot, dpart);
     k_sum_rows<<<kDepth + 1, kThreads, 0, c.stream>>>(dpart, kDotBlocks, dsum);
-    c.launches += 3;
+    c.launches += 2;
     double d[kDepth + 1];
     if (!cuda_ok(c, cudaMemcpyAsync(d, dsum, sizeof(d), cudaMemcpyDeviceToHost, c.stream), "adjoint") ||
         !cuda_ok(c, cudaStreamSynchronize(c.stream), "adjoint"))
@@ -538,10 +544,8 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
     anderson_coefficients(gram, ns, coef);
     Mix mx{};
     mx.ns = ns;
-    mx.eta = eta;
     for (int a = 0; a < ns; ++a) {
-      mx.xs[a] = xs + (size_t)a * tot;
-      mx.rs[a] = rs + (size_t)a * tot;
+      mx.ys[a] = ys + (size_t)a * tot;
       mx.c[a] = coef[a];
     }
     k_combine<<<gt, kThreads, 0, c.stream>>>(tot, mx, xi);
@@ -551,7 +555,7 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
   if (it == maxit) { c.err = "adjoint solve did not converge"; return RISM3D_NOT_CONVERGED; }
   const auto w1 = std::chrono::steady_clock::now();
   // weights from zeta; L xi is current (the loop leaves right after applyL)
-  double *W = xs;                               // history no longer needed
+  double *W = ys;                               // history no longer needed
   SiteW sv{};
   for (int v = 0; v < V; ++v) {
     sv.sig[v] = c.sigv[v]; sv.eps[v] = c.epsv[v]; sv.q[v] = c.qv[v] * c.cf_final; sv.rho[v] = c.rho[v];
