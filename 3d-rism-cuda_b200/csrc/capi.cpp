@@ -610,6 +610,24 @@ int rism3d_get_grid(rism3d_ctx *x, int which, double *host) {
   return fetch_grid(c, which, host);
 }
 
+int rism3d_get_grid_device(rism3d_ctx *x, int which, double *dev) {
+  if (!x || !dev) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (!c.have_solute) { c.err = "no solute"; return RISM3D_BAD_STATE; }
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, dev) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+      at.device != c.dev) {
+    cudaGetLastError();
+    c.err = "get_grid_device: not a device pointer on the context's GPU";
+    return RISM3D_BAD_INPUT;
+  }
+  int rc = device_grid(c, which, dev);
+  if (rc == RISM3D_OK && c.own_stream && !cuda_ok(c, cudaStreamSynchronize(c.stream), "get_grid_device"))
+    return RISM3D_CUDA_ERROR;
+  return rc;
+}
+
 void rism3d_destroy(rism3d_ctx *x) {
   if (!x) return;
   context_release(x->c);

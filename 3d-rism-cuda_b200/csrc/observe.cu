@@ -658,6 +658,72 @@ int compute_observables(Context &c) {
   return RISM3D_UNSUPPORTED_SHAPE;
 }
 
+// Result grids formed on the device into caller memory (rism3d_get_grid_device):
+// mode 0: out = a + b (e = esr + fr); 1: out_v = a_v + qcf_v b (t = t_SR + q cf fr);
+// 2: out_v = h_v - (a_v + qcf_v b) (c = h - t); 3: out = sum_v w_v g_v (cal_qv.cu:20-27)
+struct GridArgs {
+  double coef[kMaxSites];
+  int nv, mode;
+};
+
+__global__ void k_grid_out(long long n, GridArgs ga, const double *__restrict__ a,
+                           const double *__restrict__ b, const double *__restrict__ h,
+                           double *__restrict__ out) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    if (ga.mode == 0) {
+      out[j] = a[j] + b[j];
+    } else if (ga.mode == 3) {
+      double s = 0.0;
+      for (int v = 0; v < ga.nv; ++v) s += a[(size_t)v * n + j] * ga.coef[v];
+      out[j] = s;
+    } else {
+      const double fr = b[j];
+      for (int v = 0; v < ga.nv; ++v) {
+        const double t = a[(size_t)v * n + j] + ga.coef[v] * fr;
+        out[(size_t)v * n + j] = ga.mode == 1 ? t : h[(size_t)v * n + j] - t;
+      }
+    }
+  }
+}
+
+int device_grid(Context &c, int which, double *out) {
+  const long long n = c.n;
+  const size_t V = (size_t)c.natv;
+  auto copy = [&](const double *src, size_t cnt) {
+    return cuda_ok(c, cudaMemcpyAsync(out, src, sizeof(double) * cnt, cudaMemcpyDeviceToDevice,
+                                      c.stream), "get_grid_device") ? RISM3D_OK : RISM3D_CUDA_ERROR;
+  };
+  GridArgs ga{};
+  ga.nv = c.natv;
+  const double *a = nullptr, *b = nullptr, *h = nullptr;
+  switch (which) {
+    case RISM3D_GRID_U: return copy(c.d_u, V * n);
+    case RISM3D_GRID_FR: return copy(c.d_fr, n);
+    case RISM3D_GRID_E: ga.mode = 0; a = c.d_e; b = c.d_fr; break;
+    case RISM3D_GRID_G: case RISM3D_GRID_H: case RISM3D_GRID_T: case RISM3D_GRID_C:
+    case RISM3D_GRID_QV:
+      if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
+      if (which == RISM3D_GRID_G) return copy(c.d_g, V * n);
+      if (which == RISM3D_GRID_H) return copy(c.d_h, V * n);
+      if (which == RISM3D_GRID_QV) {
+        ga.mode = 3; a = c.d_g;
+        for (int v = 0; v < c.natv; ++v) ga.coef[v] = c.rho[v] * c.qv[v];
+      } else {
+        ga.mode = which == RISM3D_GRID_T ? 1 : 2; a = c.d_t; b = c.d_fr; h = c.d_h;
+        for (int v = 0; v < c.natv; ++v) ga.coef[v] = c.qv[v] * c.cf_final;
+      }
+      break;
+    default:
+      c.err = "unknown grid id";
+      return RISM3D_BAD_INPUT;
+  }
+  const long long blocks = std::min<long long>((n + kThreads - 1) / kThreads, 148 * 16);
+  k_grid_out<<<(unsigned)blocks, kThreads, 0, c.stream>>>(n, ga, a, b, h, out);
+  c.launches += 1;
+  return cuda_ok(c, cudaGetLastError(), "get_grid_device") ? RISM3D_OK : RISM3D_CUDA_ERROR;
+}
+
 int compute_se_from_grids(Context &c) {
   switch (c.natv) {
     case 1: return se_grid_v<1>(c);

@@ -250,6 +250,7 @@ int run_solve(Context &c, int chargeup);          // solver.cu
 int compute_observables(Context &c);              // observe.cu
 int compute_atom_integrals(Context &c, bool forces);  // observe.cu
 int compute_se_from_grids(Context &c);            // observe.cu: SE totals, one solute
+int device_grid(Context &c, int which, double *out);  // observe.cu: rism3d_get_grid_device
 int compute_adjoint(Context &c, double *dq, double *dsig, double *deps,
                     double *dR);                  // adjoint.cu
 // FP64 OZ k-space pass on a packed buffer (adjoint solve)

@@ -26,7 +26,7 @@ EXPORTS = ["rism3d_create", "rism3d_set_solvent", "rism3d_set_solute", "rism3d_s
            "rism3d_solve_batch", "rism3d_destroy", "rism3d_last_error",
            "rism3d_initialize", "rism3d_iterate", "rism3d_output",
            "rism3d_refresh_potentials", "rism3d_kernel_launches", "rism3d_time_kernel",
-           "rism3d_set_esp", "rism3d_set_rmdft"]
+           "rism3d_set_esp", "rism3d_set_rmdft", "rism3d_get_grid_device"]
 
 
 class RismError(RuntimeError):
@@ -97,6 +97,7 @@ def lib():
         L.rism3d_output.argtypes = [vp]
         L.rism3d_refresh_potentials.argtypes = [vp]
         L.rism3d_set_esp.argtypes = [vp, d]
+        L.rism3d_get_grid_device.argtypes = [vp, C.c_int, vp]
         L.rism3d_set_rmdft.argtypes = [vp, d, C.c_int, d, d, d, C.c_double, C.c_double]
         L.rism3d_kernel_launches.argtypes = [vp]
         L.rism3d_kernel_launches.restype = C.c_longlong
@@ -132,6 +133,7 @@ class Solver:
         if rc != OK:
             raise RismError(rc, L.rism3d_last_error(None).decode())
         self.h = h
+        self.device = device
         self.grid = tuple(p.grid)
         self.n = self.grid[0] * self.grid[1] * self.grid[2]
         self.natv = 0
@@ -191,6 +193,15 @@ class Solver:
         nsite = self.natv if which in (GRID_G, GRID_H, GRID_C, GRID_T, GRID_U) else 1
         out = np.zeros((nsite, self.n))
         self._check(lib().rism3d_get_grid(self.h, which, _dp(out)))
+        return out
+
+    def grid_tensor(self, which):
+        """The grid as a torch float64 tensor on the solver's GPU, formed on the
+        device with no host copy (rism3d_get_grid_device)."""
+        import torch
+        nsite = self.natv if which in (GRID_G, GRID_H, GRID_C, GRID_T, GRID_U) else 1
+        out = torch.empty((nsite, self.n), dtype=torch.float64, device="cuda:%d" % self.device)
+        self._check(lib().rism3d_get_grid_device(self.h, which, C.c_void_p(out.data_ptr())))
         return out
 
     def euv(self):

@@ -195,6 +195,14 @@ int rism3d_time_kernel(rism3d_ctx *ctx, int which, int reps, double *ms_per_laun
 /* Copy a result grid to host memory (see RISM3D_GRID_*). */
 int rism3d_get_grid(rism3d_ctx *ctx, int which, double *host);
 
+/* The same grid formed on the device into caller-owned device memory (a
+ * torch tensor's data pointer, a DLPack buffer, ...) on the context's GPU:
+ * no host traffic.  With a caller stream (rism3d_params.stream) the work is
+ * ordered on that stream and the call returns without waiting; with the
+ * context's own stream it waits for the copy.  BAD_INPUT for a pointer that
+ * is not device memory of the context's GPU. */
+int rism3d_get_grid_device(rism3d_ctx *ctx, int which, double *dev);
+
 /* Batched small solutes (no reference counterpart; the reference solves
  * one solute per process).  Solute m has natoms[m] atoms starting at
  * atom offset off[m] in the concatenated arrays, a cubic grid

@@ -390,6 +390,26 @@ def test_se_at_tight_convergence_matches_reference_executable(prec):
     s.close()
 
 
+def test_device_grids_equal_the_host_copies():
+    """rism3d_get_grid_device: every grid formed on the device into a torch
+    tensor equals rism3d_get_grid's host copy; host memory is refused."""
+    import rism3d_b200 as R
+    case, _, _ = load_case("cfg0_chain12")
+    s = product_solver(case)
+    s.solve()
+    for which in (R.GRID_G, R.GRID_H, R.GRID_C, R.GRID_T, R.GRID_U, R.GRID_E, R.GRID_FR,
+                  R.GRID_QV):
+        dev = s.grid_tensor(which).cpu().numpy()
+        host = s.grid_array(which)
+        assert dev.shape == host.shape
+        assert np.abs(dev - host).max() <= 1e-12 * max(np.abs(host).max(), 1.0), which
+    buf = np.zeros(case.n)
+    import ctypes
+    rc = R.lib().rism3d_get_grid_device(s.h, R.GRID_FR, ctypes.c_void_p(buf.ctypes.data))
+    assert rc == R.BAD_INPUT
+    s.close()
+
+
 def test_host_driven_iteration_matches_the_device_loop():
     """RISM3D_HOST_LOOP=1 drives the same iteration graphs from the host (the
     path used when conditional graph nodes are unavailable): same steps,
