@@ -118,7 +118,7 @@ def iter_bytes_per_point(V, s):
     return {"pass_a": 9 * V * s, "pass_k": 2 * V * s + 8, "pass_r": 5 * V * s}
 
 
-def survey_bytes_per_iter(n, V, s):
+def fused_pipeline_bytes_per_iter(n, V, s):
     """N (31 V s + 5 s + 4): minimal fused pipeline of the per-site design."""
     return n * (31 * V * s + 5 * s + 4)
 
@@ -296,14 +296,14 @@ def run_ours(args, rank, world, dist):
                     "%d atoms" % len(sol.q)},
         "kernels": kern,
         "bytes_per_iteration": {"fp64": sum(bpp64.values()) * n, "fp32": sum(bpp32.values()) * n,
-                                "survey_formula_fp64": survey_bytes_per_iter(n, V, 8)},
+                                "fused_pipeline_fp64": fused_pipeline_bytes_per_iter(n, V, 8)},
         # whole-iteration rate under the per-site byte model N (31 V s + 5 s + 4)
         # (FP32 bulk: 31 V x 4 B, the long-range terms at 8 B): bytes x steps /
         # iteration time; above the copy peak means the fused passes move fewer
         # bytes than that model assumes
         "iteration_rate": {
             "fp64": {"ms_iterate": r64["ms_iterate"], "steps": r64["iterations"],
-                     "model_gbs": survey_bytes_per_iter(n, V, 8) * r64["iterations"]
+                     "model_gbs": fused_pipeline_bytes_per_iter(n, V, 8) * r64["iterations"]
                      / (r64["ms_iterate"] * 1e6)},
             "mixed": {"ms_iterate": rm["ms_iterate"], "steps": rm["iterations"],
                       "model_gbs": n * (31 * V * 4 + 5 * 8 + 4) * rm["iterations"]
