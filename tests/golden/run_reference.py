@@ -20,7 +20,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 BIN = os.path.join(ROOT, "oracle", "_ref", "3drism-cuda")
 
 CASES = ["test1", "test1_tight", "test2", "test2_tight", "test3", "test4", "test4_tight",
-         "cfg0_chain12", "cfg1_globule300", "cfg2_protein846_kh", "cfg0_esp",
+         "cfg0_chain12", "cfg1_globule300", "cfg2_protein846_kh", "cfg2_protein846_hnc", "cfg0_esp",
          "rmdft_benzene"]
 # ESP-cube cases (-e, cal_Coulomb.cu:41-96): name -> control file reused;
 # the cube comes from make_esp.py
@@ -31,12 +31,15 @@ ESP_CASES = {"cfg0_esp": "cfg0_chain12"}
 # and held garbage on the 64^3 cell (SFE_RMDFT -12430.7 against -4422.5 with
 # zeros; ~1e128 with MALLOC_PERTURB_=165 on both cells).
 RMDFT_CASES = {"rmdft_benzene": "rmdft_287.xsv"}
+# cases run with extra flags: name -> (control file reused, flags)
+FLAG_CASES = {}
 
 
 def run(case, outdir):
     d = os.path.join(outdir, case)
     os.makedirs(d, exist_ok=True)
-    src = os.path.join(HERE, ESP_CASES.get(case, case) + ".inp")
+    base = FLAG_CASES[case][0] if case in FLAG_CASES else ESP_CASES.get(case, case)
+    src = os.path.join(HERE, base + ".inp")
     shutil.copyfile(src, os.path.join(d, case + ".inp"))
     solvent = open(src).read().split()[4]                                  # read_input.cu:42
     shutil.copyfile(os.path.join(HERE, solvent), os.path.join(d, solvent))
@@ -46,6 +49,8 @@ def run(case, outdir):
         shutil.copyfile(os.path.join(HERE, cvk), os.path.join(d, cvk))
         shutil.copyfile(os.path.join(HERE, RMDFT_CASES[case]), os.path.join(d, RMDFT_CASES[case]))
         args = ["-r", RMDFT_CASES[case]] + args
+    if case in FLAG_CASES:
+        args = FLAG_CASES[case][1] + args
     if case in ESP_CASES:
         sys.path.insert(0, HERE)
         import make_esp

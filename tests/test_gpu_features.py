@@ -358,12 +358,14 @@ def test_large_cases_match_reference_executable(name, prec):
         # FP32 refinement reaches the FP64 tolerance: two FP64 cycles
         assert r["iterations"] - r["iterations_fp32"] <= 3
     for k, key in (("sfe_sc", "SFE_SC"), ("sfe_sc_hnc", "SFE_SC_HNC"), ("sfe_gf", "SFE_GF")):
-        assert abs(r[k] - ref[key]) < MU_TOL, (k, r[k], ref[key])
+        if key in ref:                    # SFE_SC_HNC is printed for KH only
+            assert abs(r[k] - ref[key]) < MU_TOL, (k, r[k], ref[key])
     if prec == 0:
         # same AN2 trajectory; near the 1e-6 threshold the residual falls ~3%
         # per step and oscillates, so rounding-level differences of the
-        # transforms (cuFFT 3D vs the fused z pass) move the crossing step by
-        # a few percent (test4: 297 / 311 steps against the reference's 302)
+        # transforms (two sites per complex transform here, one per site in
+        # the reference) move the crossing step by a few percent (test4:
+        # 297 / 311 steps against the reference's 302)
         n_ref = summary[name]["iterations"]
         assert abs(r["iterations"] - n_ref) <= max(2, 0.05 * n_ref)
     assert abs(r["pmv"] - ref["PMV"]) < 1e-3
@@ -372,6 +374,26 @@ def test_large_cases_match_reference_executable(name, prec):
     # against the reference's 302 give 1.5e-4 relative, while both runs
     # converged to 1e-8 agree to 7e-7, see the tight-convergence pin below)
     assert abs(r["se"] - ref["SE"]) < 3e-4 * abs(ref["SE"])
+    s.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_hnc_protein_diverges_at_the_first_step_like_the_reference(prec):
+    """The 846-atom solute at 256^3 under HNC: the reference executable
+    prints one step (residual 5e12), then its second step's residual is not
+    finite and it reports "Calculation diverged." without printing that step
+    (iterate.cu:53-57 break before the print at :63); its .xmu holds nan.
+    The solve reports RISM3D_DIVERGED after the same two steps; the mixed
+    form's FP32 bulk hands the stage to FP64, which diverges too."""
+    import rism3d_b200 as R
+    case, _, _ = load_case("cfg2_protein846_hnc")
+    summary = json.load(open(os.path.join(GOLDEN, "ref_b200", "summary.json")))
+    assert summary["cfg2_protein846_hnc"]["iterations"] == 1
+    s = product_solver(case, precision=prec)
+    r = s.solve(allow_unconverged=True)
+    assert r["status"] == R.DIVERGED
+    if prec == 0:
+        assert r["iterations"] == summary["cfg2_protein846_hnc"]["iterations"] + 1
     s.close()
 
 
