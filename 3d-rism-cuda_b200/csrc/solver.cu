@@ -796,9 +796,31 @@ int grid_blocks(long long work) {
   return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
 
+// Blocks along x for a grid-stride pass of one solute: one full wave of the
+// kernel's resident blocks (SMs x blocks per SM at kThreads threads, from
+// its register and shared-memory use), so that no partial last wave leaves
+// most SMs idle.  With 2368 blocks, a kernel holding 5 blocks per SM ran 3.2
+// waves and one holding 3 ran 5.3.  Batched launches (solutes on y) keep
+// grid_blocks: their many waves make the tail small.
+template <typename K>
+int wave_blocks(K kernel, long long work, int nb) {
+  if (nb > 1) return grid_blocks(work);
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess ||
+      sms < 1 || per_sm < 1) {
+    cudaGetLastError();
+    return grid_blocks(work);
+  }
+  const long long need = (work + kThreads - 1) / kThreads, wave = (long long)sms * per_sm;
+  return (int)std::max(1LL, std::min(need, wave));
+}
+
 template <typename T, int V, int CLOS, bool REF>
 void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
-  const dim3 ba(grid_blocks(a.n), c.nb), bk(grid_blocks(a.n / 2), c.nb), br(a.nblocks, c.nb);
+  const dim3 ba(wave_blocks(k_pass_a<T, V, CLOS, REF>, a.n, c.nb), c.nb),
+      bk(wave_blocks(k_kspace<T, V>, a.n / 2, c.nb), c.nb), br(a.nblocks, c.nb);
   k_pass_a<T, V, CLOS, REF><<<ba, kThreads, 0, c.stream>>>(a);
   typedef typename Cx<T>::t C;
   if (sizeof(T) == 8) {
@@ -1087,7 +1109,9 @@ int refine_base(Context &c) {
   IterArgs<double> a = make_args<double>(c, true);
   a.buf = c.d_buf; a.t = c.d_t; a.U = c.d_U; a.Y = c.d_Y; a.RP = c.d_RP;
   a.tw = c.d_tw;
-  const dim3 ba(grid_blocks(c.n), nb), bk(grid_blocks(c.n / 2), nb);
+  const dim3 ba(wave_blocks(k_pass_a<double, V, CLOS, false>, c.n, nb), nb),
+      bk(wave_blocks(k_kspace<double, V>, c.n / 2, nb), nb),
+      bb(wave_blocks(k_refine_base<V, CLOS>, c.n, nb), nb);
   if (!cufft_ok(c, cufftSetStream(c.plan64, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
   k_pass_a<double, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a);
   if (!cufft_ok(c, cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)a.buf, (cufftDoubleComplex *)a.buf,
@@ -1097,7 +1121,7 @@ int refine_base(Context &c) {
   if (!cufft_ok(c, cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)a.buf, (cufftDoubleComplex *)a.buf,
                                 CUFFT_INVERSE), "refine base FFT"))
     return RISM3D_CUFFT_ERROR;
-  k_refine_base<V, CLOS><<<ba, kThreads, 0, c.stream>>>(a, c.f_R0, c.f_x0, c.f_t, c.f_Y);
+  k_refine_base<V, CLOS><<<bb, kThreads, 0, c.stream>>>(a, c.f_R0, c.f_x0, c.f_t, c.f_Y);
   k_phase_end<<<1, 128, 0, c.stream>>>(c.d_state, nb, kBase64, 0);
   c.launches += 6;
   return cuda_ok(c, cudaGetLastError(), "refine base") ? RISM3D_OK : RISM3D_CUDA_ERROR;
@@ -1277,12 +1301,15 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int ba = grid_blocks(a.n), bk = grid_blocks(a.n / 2);
+  // the launch shapes of the solve (launch_iteration)
+  const int ba = wave_blocks(k_pass_a<T, V, CLOS, false>, a.n, 1),
+            bar = wave_blocks(k_pass_a<T, V, CLOS, true>, a.n, 1),
+            bk = wave_blocks(k_kspace<T, V>, a.n / 2, 1);
   cudaEventRecord(e0, c.stream);
   for (int r = 0; r < reps; ++r) {
     switch (which) {
       case 0: case 10: k_pass_a<T, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a); break;
-      case 13: k_pass_a<T, V, CLOS, true><<<ba, kThreads, 0, c.stream>>>(a); break;
+      case 13: k_pass_a<T, V, CLOS, true><<<bar, kThreads, 0, c.stream>>>(a); break;
       case 1: case 11: k_kspace<T, V><<<bk, kThreads, 0, c.stream>>>(a); break;
       case 15: k_pass_r<T, V, CLOS, true><<<a.nblocks, kThreads, 0, c.stream>>>(a); break;
       default: k_pass_r<T, V, CLOS, false><<<a.nblocks, kThreads, 0, c.stream>>>(a); break;
@@ -1480,7 +1507,8 @@ template <int V>
 int oz_kspace_v(Context &c, double2 *buf, const StageParams *sp, DevState *st) {
   IterArgs<double> a = make_args<double>(c, true);
   a.buf = buf; a.sp = sp; a.st = st;
-  k_kspace<double, V><<<dim3(grid_blocks(c.n / 2), 1), kThreads, 0, c.stream>>>(a);
+  k_kspace<double, V><<<dim3(wave_blocks(k_kspace<double, V>, c.n / 2, 1), 1), kThreads, 0,
+                        c.stream>>>(a);
   c.launches += 1;
   return cuda_ok(c, cudaGetLastError(), "oz k-space") ? RISM3D_OK : RISM3D_CUDA_ERROR;
 }
