@@ -31,15 +31,12 @@ ESP_CASES = {"cfg0_esp": "cfg0_chain12"}
 # and held garbage on the 64^3 cell (SFE_RMDFT -12430.7 against -4422.5 with
 # zeros; ~1e128 with MALLOC_PERTURB_=165 on both cells).
 RMDFT_CASES = {"rmdft_benzene": "rmdft_287.xsv"}
-# cases run with extra flags: name -> (control file reused, flags)
-FLAG_CASES = {}
 
 
 def run(case, outdir):
     d = os.path.join(outdir, case)
     os.makedirs(d, exist_ok=True)
-    base = FLAG_CASES[case][0] if case in FLAG_CASES else ESP_CASES.get(case, case)
-    src = os.path.join(HERE, base + ".inp")
+    src = os.path.join(HERE, ESP_CASES.get(case, case) + ".inp")
     shutil.copyfile(src, os.path.join(d, case + ".inp"))
     solvent = open(src).read().split()[4]                                  # read_input.cu:42
     shutil.copyfile(os.path.join(HERE, solvent), os.path.join(d, solvent))
@@ -49,8 +46,6 @@ def run(case, outdir):
         shutil.copyfile(os.path.join(HERE, cvk), os.path.join(d, cvk))
         shutil.copyfile(os.path.join(HERE, RMDFT_CASES[case]), os.path.join(d, RMDFT_CASES[case]))
         args = ["-r", RMDFT_CASES[case]] + args
-    if case in FLAG_CASES:
-        args = FLAG_CASES[case][1] + args
     if case in ESP_CASES:
         sys.path.insert(0, HERE)
         import make_esp
