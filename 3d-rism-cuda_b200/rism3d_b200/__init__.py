@@ -40,7 +40,7 @@ class Params(C.Structure):
                 ("convergence", C.c_double), ("maxstep", C.c_int), ("an2_count", C.c_int),
                 ("an2_m", C.c_double), ("an2_mp", C.c_double), ("precision", C.c_int),
                 ("mixed_switch", C.c_double), ("device", C.c_int), ("verbose", C.c_int),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("batch_chunk_points", C.c_longlong)]
 
 
 class Result(C.Structure):
@@ -119,7 +119,7 @@ class Solver:
 
     def __init__(self, grid, box, closure=KH, convergence=1e-6, maxstep=10000,
                  an2=(2, 0.6, 0.2), precision=FP64, mixed_switch=0.0, device=0,
-                 verbose=0, stream=None):
+                 verbose=0, stream=None, batch_chunk_points=0):
         L = lib()
         p = Params()
         p.grid[:] = [int(g) for g in grid]
@@ -128,6 +128,7 @@ class Solver:
         p.an2_count, p.an2_m, p.an2_mp = int(an2[0]), float(an2[1]), float(an2[2])
         p.precision, p.mixed_switch, p.device, p.verbose = precision, mixed_switch, device, verbose
         p.stream = stream
+        p.batch_chunk_points = int(batch_chunk_points)
         h = C.c_void_p()
         rc = L.rism3d_create(C.byref(p), C.byref(h))
         if rc != OK:

@@ -72,6 +72,10 @@ typedef struct {
   void *stream;           /* caller-owned cudaStream_t for all work; NULL: the
                              context creates its own (the reference uses the
                              legacy default stream) */
+  long long batch_chunk_points; /* rism3d_solve_batch: solutes of one cell run
+                             in sub-batches of about this many grid points in
+                             all, which converge, finish and overlap on their
+                             own (0 = 2^20) */
 } rism3d_params;
 
 typedef struct {

@@ -49,6 +49,28 @@ def test_batch_matches_single_solves(precision):
     parent.close()
 
 
+def test_sub_batches_give_the_same_results():
+    """A cell's solutes split into sub-batches (batch_chunk_points = 2 x 32^3:
+    the three 32^3 solutes run as sub-batches of two and one, the two 48^3
+    and the two 64^3 ones one by one), each on its own child context and
+    stream: the same results as one batch per cell."""
+    import rism3d_b200 as R
+    sv = F.read_xvk(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    mols = _mols()
+    whole = R.Solver((32, 32, 32), (16.0, 16.0, 16.0))
+    whole.set_solvent_obj(sv)
+    ref = whole.solve_batch(mols)
+    whole.close()
+    split = R.Solver((32, 32, 32), (16.0, 16.0, 16.0), batch_chunk_points=2 * 32 ** 3)
+    split.set_solvent_obj(sv)
+    res = split.solve_batch(mols)
+    split.close()
+    for i in range(len(mols)):
+        assert res[i]["status"] == 0
+        assert abs(res[i]["sfe_sc"] - ref[i]["sfe_sc"]) < 1e-6 * abs(ref[i]["sfe_sc"]) + 1e-6, i
+        assert abs(res[i]["iterations"] - ref[i]["iterations"]) <= 1, i
+
+
 def test_batch_member_matches_oracle():
     import rism3d_b200 as R
     sv = F.read_xvk(os.path.join(GOLDEN, "h2o_vv.xvk"))
