@@ -1,11 +1,13 @@
 // Batched solves of many small solutes (rism3d_solve_batch).  The reference
 // solves one solute per process; here solutes with the same cubic cell are
-// solved together: every pass of the iteration is one launch over all of
-// them (solute = blockIdx.y), one batched cuFFT plan transforms all their
-// site pairs, each solute converges on its own device state word (a
-// finished solute's blocks idle), and the loop is the same captured graph.
-// Groups of different cells run concurrently: each group's child context
-// has its own stream and is driven from its own host thread.
+// solved together in sub-batches of about batch_chunk_points grid points:
+// every pass of the iteration is one launch over a sub-batch (solute =
+// blockIdx.y), one batched cuFFT plan transforms all its site pairs, each
+// solute converges on its own device state word (a finished solute's blocks
+// idle), and the loop is the same captured graph.  Sub-batches run
+// concurrently: each has its own child context and stream and is driven
+// from its own host thread, so a sub-batch that has converged stops paying
+// for the transforms of the others.
 #include <algorithm>
 #include <map>
 #include <thread>
