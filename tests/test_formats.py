@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 from scipy.interpolate import CubicSpline
 
+from conftest import GOLDEN
 from oracle import formats as F
 from oracle import oracle as O
 
@@ -104,3 +105,41 @@ def test_oracle_chi_grid_uses_unique_k(golden):
     # chi depends on |k| only: symmetric under x<->y<->z permutations
     assert np.allclose(x, x.transpose(0, 1, 2, 4, 3))
     assert np.allclose(x, x.transpose(0, 1, 4, 3, 2))
+
+
+def test_esp_cube_reader_orders_values_x_fastest(tmp_path):
+    """cal_Coulomb.cu:41-88: two comment lines, natom / origin / one more
+    number, three axis lines, natom atom lines, then values with z fastest;
+    the reader returns them x fastest and refuses a cube on another grid."""
+    nx, ny, nz = 4, 3, 2
+    vals = np.arange(nx * ny * nz, dtype=float) * 0.5          # cube order: ix, iy, iz
+    lines = ["comment", "comment", "    1    0.0    0.0    0.0    1",
+             "%5d 0.5 0.0 0.0" % nx, "%5d 0.0 0.5 0.0" % ny, "%5d 0.0 0.0 0.5" % nz,
+             "    8   -0.5   0.0   0.0   0.0"]
+    lines += [" ".join("%13.5E" % v for v in vals[i:i + 6]) for i in range(0, vals.size, 6)]
+    p = tmp_path / "t.cube"
+    p.write_text("\n".join(lines) + "\n")
+    got = F.read_esp_cube(str(p), (nx, ny, nz))
+    cube = vals.reshape(nx, ny, nz)
+    for ix, iy, iz in ((0, 0, 0), (3, 0, 1), (1, 2, 0), (3, 2, 1)):
+        assert got[ix + nx * (iy + ny * iz)] == cube[ix, iy, iz]
+    with pytest.raises(ValueError):
+        F.read_esp_cube(str(p), (4, 4, 2))
+
+
+def test_hard_sphere_table_and_cvk_beside_the_xvk(tmp_path):
+    """solvent_read.cc:88-140: the .cvk (same layout as the .xvk, same stem)
+    and the -r table (ntab2; packing fraction and w(0); rows k chs w)."""
+    p = tmp_path / "hs.xsv"
+    p.write_text("3\n0.4 1.05\n0 -700.0 1.05\n0.1 -690.5 1.04\n0.2 -680.25 1.02\n")
+    hs = F.read_hard_sphere(str(p))
+    assert hs.ntab2 == 3 and hs.pfhs == 0.4 and hs.wfk0 == 1.05
+    assert np.array_equal(hs.k, [0.0, 0.1, 0.2]) and hs.chs[2] == -680.25 and hs.w[1] == 1.04
+    p.write_text("4\n0.4 1.05\n0 -700.0 1.05\n")
+    with pytest.raises(ValueError):
+        F.read_hard_sphere(str(p))
+    xvk = os.path.join(GOLDEN, "rmdft_h2o_vv.xvk")
+    cvk = F.read_cvk(xvk)
+    sv = F.read_xvk(xvk)
+    assert cvk.shape == sv.xvv.shape
+    assert not np.allclose(cvk, sv.xvv)
