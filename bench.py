@@ -118,9 +118,12 @@ def iter_bytes_per_point(V, s):
     return {"pass_a": 9 * V * s, "pass_k": 2 * V * s + 8, "pass_r": 5 * V * s}
 
 
-def fused_pipeline_bytes_per_iter(n, V, s):
-    """N (31 V s + 5 s + 4): minimal fused pipeline of the per-site design."""
-    return n * (31 * V * s + 5 * s + 4)
+def fused_pipeline_bytes_per_iter(n, V, s, s_lr=None):
+    """N (31 V s + 5 s_lr + 4): minimal fused pipeline of the per-site design;
+    the long-range Coulomb grids (e, fr, fk) stay FP64 (s_lr = 8) in the
+    mixed form."""
+    s_lr = s if s_lr is None else s_lr
+    return n * (31 * V * s + 5 * s_lr + 4)
 
 
 def read_traffic(kernel):
@@ -297,7 +300,8 @@ def run_ours(args, rank, world, dist):
                     "%d atoms" % len(sol.q)},
         "kernels": kern,
         "bytes_per_iteration": {"fp64": sum(bpp64.values()) * n, "fp32": sum(bpp32.values()) * n,
-                                "fused_pipeline_fp64": fused_pipeline_bytes_per_iter(n, V, 8)},
+                                "fused_pipeline_fp64": fused_pipeline_bytes_per_iter(n, V, 8),
+                                "fused_pipeline_fp32": fused_pipeline_bytes_per_iter(n, V, 4, 8)},
         # whole-iteration rate under the per-site byte model N (31 V s + 5 s + 4)
         # (FP32 bulk: 31 V x 4 B, the long-range terms at 8 B): bytes x steps /
         # iteration time; above the copy peak means the fused passes move fewer
