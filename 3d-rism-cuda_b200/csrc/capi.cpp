@@ -22,7 +22,10 @@ struct rism3d_ctx {
   Context c;
 };
 
-static std::string g_create_err;
+// Errors of calls that have no context (create, initialize, the
+// allocation-free integrals): one message per host thread, so that threads
+// driving different GPUs never share the string.
+static thread_local std::string g_create_err;
 
 namespace rism3d {
 

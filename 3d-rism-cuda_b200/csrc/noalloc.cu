@@ -161,9 +161,19 @@ extern "C" int rism3d_exchem_noalloc(int closure, int natv, long long n, double 
     case 7: launch_c<7>(closure, n, nb, d_h, d_t, scratch, st); break;
     case 8: launch_c<8>(closure, n, nb, d_h, d_t, scratch, st); break;
   }
-  k_exchem_sum<<<4 * natv, kThreads, 0, st>>>(scratch, nb, sums);
+  // a launch that failed (no kernel image, bad configuration) must not let
+  // the copy below return the previous call's sums from the shared array
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    k_exchem_sum<<<4 * natv, kThreads, 0, st>>>(scratch, nb, sums);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_create_error(std::string("rism3d_exchem_noalloc: launch: ") + cudaGetErrorString(e));
+    return RISM3D_CUDA_ERROR;
+  }
   double raw[kSums];
-  cudaError_t e = cudaMemcpyAsync(raw, sums, sizeof(double) * 4 * natv, cudaMemcpyDeviceToHost, st);
+  e = cudaMemcpyAsync(raw, sums, sizeof(double) * 4 * natv, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     set_create_error(std::string("rism3d_exchem_noalloc: ") + cudaGetErrorString(e));

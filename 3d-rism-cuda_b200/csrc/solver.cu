@@ -887,11 +887,14 @@ cudaGraphExec_t capture(Context &c, const IterArgs<T> &a, cufftHandle plan) {
 __global__ void k_loop_cond(cudaGraphConditionalHandle h, DevState *st, int nb) {
   if (threadIdx.x != 0) return;
   bool more = false;
-  for (int b = 0; b < nb; ++b)
+  int cap = 1;                 // the largest step budget left to any solute
+  for (int b = 0; b < nb; ++b) {
     if (!(st[b].done && st[b].after_done >= 1)) more = true;
+    cap = max(cap, st[b].maxstep);
+  }
   const int loops = ++st[0].loops;
   st[0].bodies += 1;
-  const int cap = st[0].maxstep < 1000000 ? st[0].maxstep : 1000000;
+  cap = cap < 1000000 ? cap : 1000000;
   if (loops >= cap + 4) more = false;
   cudaGraphSetConditional(h, more ? 1u : 0u);
 }
@@ -1067,10 +1070,13 @@ int run_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
         if (!cuda_ok(c, cudaEventSynchronize(ev[k]), "iteration")) { status = RISM3D_CUDA_ERROR; break; }
         const DevState *ss = &c.h_state[(size_t)k * nb];
         bool all_done = true;
-        for (int b = 0; b < nb; ++b)
+        int cap = 1;
+        for (int b = 0; b < nb; ++b) {
           if (!ss[b].done) all_done = false;
+          cap = std::max(cap, ss[b].maxstep);
+        }
         if (all_done) stop = true;
-        if (launched > ss[0].maxstep + kLag + 2) stop = true;   // hard bound
+        if (launched > cap + kLag + 2) stop = true;   // hard bound
       }
       if (launched > c.prm.maxstep + kLag + 2) stop = true;
     }

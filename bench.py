@@ -339,9 +339,11 @@ def run_batch(args, dev, stream, rank=0, world=1, dist=False):
         F.centre(m.xyz)
         mols.append((m.sig, m.eps, m.q, m.xyz, m.grid[0], m.box[0]))
     n_total = len(mols)
+    mine = list(range(n_total))
     if dist:
         part = RP.partition_by_cost([RP.solve_cost(m[4] ** 3, len(m[2])) for m in mols], world)
-        mols = [mols[i] for i in part[rank]]
+        mine = part[rank]
+        mols = [mols[i] for i in mine]
     parent = R.Solver((48, 48, 48), (24.0, 24.0, 24.0), precision=R.MIXED, device=dev,
                       stream=stream.cuda_stream)
     parent.set_solvent_obj(sv)
@@ -375,11 +377,12 @@ def run_batch(args, dev, stream, rank=0, world=1, dist=False):
     s_loop = e0.elapsed_time(e1) / 1e3
     for c in ctxs.values():
         c.close()
-    ok = sum(1 for r in res if r["status"] == 0)
     dev_name = "cuda" if dist else None
+    # every rank's per-solute results, gathered into input order
+    allres = RP.gather_results(res, mine, n_total, dev_name)
+    ok = sum(1 for r in allres if r["status"] == 0)
     rate = RP.job_rate(len(mols), s_batch, dev_name)
     loop_rate = RP.job_rate(len(sample), s_loop, dev_name)
-    ok = int(RP.sum_over_ranks(ok, dev_name))
     s_batch = RP.max_over_ranks(s_batch, dev_name)
     return {"solves_per_s": rate, "n_mols": n_total, "converged": ok,
             "s_batch": s_batch, "loop_solves_per_s": loop_rate,

@@ -244,8 +244,11 @@ int rism3d_exchem_noalloc(int closure, int natv, long long n, double dv,
                           const double *d_h, const double *d_t, void *stream,
                           double *out);
 
-/* Last error message of ctx (or of the last failed create when ctx is
- * NULL). */
+/* Last error message of ctx, or, when ctx is NULL, of the last failed call
+ * without a context (create, initialize, exchem_noalloc) made by the calling
+ * host thread: that message is kept per thread, so threads that drive
+ * different GPUs do not overwrite each other's.  The pointer stays valid
+ * until the next such call on the same thread. */
 const char *rism3d_last_error(const rism3d_ctx *ctx);
 
 /* ---- file-driven API: the three public RISM3D methods -------------------

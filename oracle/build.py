@@ -14,7 +14,10 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "liboracle_rism3d.so")
-REF_SRC = "/root/reference/src-cuda"
+# The reference checkout: $RISM3D_REFERENCE, by default where the build
+# container mounts it.
+REFERENCE = os.environ.get("RISM3D_REFERENCE", "/root/reference")
+REF_SRC = os.path.join(REFERENCE, "src-cuda")
 REF_BIN = os.path.join(HERE, "_ref", "3drism-cuda")
 
 

@@ -3,9 +3,12 @@
 # (git-ignored; it travels to the GPU box beside the other built files).
 # The reference is used only as a checker and as the timed reference arm.
 #
-#   make -f oracle/ref.mk REF=/root/reference/src-cuda -j8
+#   make -f oracle/ref.mk REFERENCE=<reference checkout> -j8
 #
-REF     ?= /root/reference/src-cuda
+# REFERENCE (or the environment variable of that name) is the checkout of the
+# reference project; the default is where the build container mounts it.
+REFERENCE ?= /root/reference
+REF     ?= $(REFERENCE)/src-cuda
 OUT     ?= $(dir $(lastword $(MAKEFILE_LIST)))_ref
 CUDA    ?= /usr/local/cuda
 NVCC    ?= $(CUDA)/bin/nvcc

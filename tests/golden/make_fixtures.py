@@ -12,7 +12,10 @@ import os
 import shutil
 import sys
 
-SRC = "/root/reference/example"
+# The reference checkout: $RISM3D_REFERENCE, by default where the build
+# container mounts it.
+REFERENCE = os.environ.get("RISM3D_REFERENCE", "/root/reference")
+SRC = os.path.join(REFERENCE, "example")
 DST = os.path.dirname(os.path.abspath(__file__))
 
 FILES = ["test1.inp", "test2.inp", "test3.inp", "test4.inp", "test1_c", "test1_s",
@@ -45,7 +48,7 @@ def subsample_xvk(src, dst, step=4):
     open(dst, "w").write("\n".join(head + rows) + "\n")
 
 
-RMDFT_SRC = "/root/reference/example_rmdft"
+RMDFT_SRC = os.path.join(REFERENCE, "example_rmdft")
 
 
 def rmdft_inputs():

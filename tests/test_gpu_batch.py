@@ -83,3 +83,34 @@ def test_batch_member_matches_oracle():
     o = O.solve(O.Case((g, g, g), (L, L, L), sv, sig, eps, q, xyz))
     assert abs(res[1]["sfe_sc"] - o["sfe_sc"]) < MU_TOL
     assert abs(res[1]["pmv"] - o["pmv"] * 1000) < 1e-4
+
+
+def test_batch_config3_shapes_match_oracle():
+    """Config-3 shapes: one batch of three molecules from the seeded
+    256-molecule generator, one per grid class (48^3, 64^3 and 96^3 at
+    0.5 A), in the 4-site water + 0.1 M NaCl table, FP32 bulk + FP64 polish.
+    Every member, the 96^3 one included (outside the reference executable's
+    valid sizes: its block reductions need power-of-two rows), matches the
+    CPU FP64 oracle."""
+    import rism3d_b200 as R
+    import rism3d_b200.synth as S
+    sv = F.read_xvk(os.path.join(GOLDEN, "naclaq_sub4_vv.xvk"))
+    pick = {}
+    for m in S.small_batch(seed=3, nmol=256):
+        if m.grid[0] not in pick and m.natom <= 24:
+            pick[m.grid[0]] = m
+    mols = []
+    for g in (48, 64, 96):
+        m = pick[g]
+        F.centre(m.xyz)
+        mols.append((m.sig, m.eps, m.q, m.xyz, g, m.box[0]))
+    parent = R.Solver((48, 48, 48), (24.0, 24.0, 24.0), precision=R.MIXED)
+    parent.set_solvent_obj(sv)
+    res = parent.solve_batch(mols)
+    parent.close()
+    for i, (sig, eps, q, xyz, g, L) in enumerate(mols):
+        o = O.solve(O.Case((g, g, g), (L, L, L), sv, sig, eps, q, xyz))
+        assert res[i]["status"] == 0, g
+        assert abs(res[i]["sfe_sc"] - o["sfe_sc"]) < MU_TOL, (g, res[i]["sfe_sc"], o["sfe_sc"])
+        assert abs(res[i]["sfe_gf"] - o["sfe_gf"]) < MU_TOL, g
+        assert abs(res[i]["pmv"] - o["pmv"] * 1000) < 1e-4, g

@@ -346,8 +346,13 @@ def test_esp_of_the_point_charges_leaves_the_solve_unchanged():
     s.close()
 
 
-@pytest.mark.parametrize("name,prec", [("cfg1_globule300", 1), ("cfg2_protein846_kh", 0),
-                                       ("cfg2_protein846_kh", 1), ("test4", 0), ("test4", 1)])
+# cfg1: the 300-atom globule at 128^3 (FP64 plain method and FP32 bulk +
+# FP64 polish); test3: the reference's 754-atom solute with net charge -22 at
+# 128^3, its only large charged case; cfg2 / test4: 256^3.
+@pytest.mark.parametrize("name,prec", [("cfg1_globule300", 0), ("cfg1_globule300", 1),
+                                       ("test3", 0), ("test3", 1),
+                                       ("cfg2_protein846_kh", 0), ("cfg2_protein846_kh", 1),
+                                       ("test4", 0), ("test4", 1)])
 def test_large_cases_match_reference_executable(name, prec):
     case, _, _ = load_case(name)
     s = product_solver(case, precision=prec)
