@@ -35,17 +35,22 @@ struct SiteLJ {
   double eps[kMaxSites];
 };
 
-// Real-space grids.  Each thread owns two neighbouring points along x (one
-// row, the atom tile read once for both); per (point, atom) one refined
-// reciprocal square root gives 1/r, r and 1/r^2.  Beyond 40 A the factor
-// e^-r (< 4.3e-18) is dropped: there the reference's q (1 - e^-r) / r
-// already rounds to q / r.
+// Real-space grids.  A block covers a brick of 8 x 8 x 8 grid points and
+// each warp a compact 8 x 4 x 2 sub-brick (4 x 2 x 1 A at 0.5 A spacing);
+// each thread owns two neighbouring points along x (the atom tile read once
+// for both).  With compact warps the distance tests below (the e^-r branch,
+// the 40 A bound, the r^2 clamp) take the same side for nearly every lane,
+// where a warp along one x row (64 points, 32 A) diverged on every atom
+// within about 40 A.  Per (point, atom) one refined reciprocal square root
+// gives 1/r, r and 1/r^2.  Beyond 40 A the factor e^-r (< 4.3e-18) is
+// dropped: there the reference's q (1 - e^-r) / r already rounds to q / r.
 constexpr int kPts = 2;
+constexpr int kBrick = 8;        // brick edge (points); x: 4 threads x kPts
 
 template <int V, bool MIX>
 __global__ void __launch_bounds__(kThreads)
-k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
-              const double *__restrict__ atoms_all, const int *__restrict__ aoff,
+k_potential_r(int nx, int ny, int nz, int bricks_x, int bricks_y, double drx, double dry,
+              double drz, const double *__restrict__ atoms_all, const int *__restrict__ aoff,
               const int *__restrict__ acnt, SiteLJ sites, double ikbt, double ubeta,
               double *__restrict__ u, double *__restrict__ esr, double *__restrict__ fr) {
   __shared__ double4 sa[kTile];           // x y z q
@@ -59,17 +64,19 @@ k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
   u += (size_t)sb * V * n;
   esr += (size_t)sb * n;
   fr += (size_t)sb * n;
-  const long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * kPts;
-  double rx[kPts], ry = 0, rz = 0;
-  {
-    const long long jj = j < n ? j : 0;
-    const int ix = (int)(jj % nx);
-    const long long r = jj / nx;
-    const int iy = (int)(r % ny), iz = (int)(r / ny);
-    for (int k = 0; k < kPts; ++k) rx[k] = (ix + k - nx / 2) * drx;   // cal_LJ.cu:54-56
-    ry = (iy - ny / 2) * dry;
-    rz = (iz - nz / 2) * drz;
-  }
+  // brick of this block, sub-brick of this warp, points of this thread
+  const int b = blockIdx.x;
+  const int bxi = b % bricks_x, byz = b / bricks_x;
+  const int byi = byz % bricks_y, bzi = byz / bricks_y;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int ix = bxi * kBrick + (lane & 3) * kPts;
+  const int iy = byi * kBrick + (w & 1) * 4 + ((lane >> 2) & 3);
+  const int iz = bzi * kBrick + (w >> 1) * 2 + (lane >> 4);
+  // grid sizes are even, so ix < nx covers both points of the thread
+  const bool live = ix < nx && iy < ny && iz < nz;
+  double rx[kPts];
+  for (int k = 0; k < kPts; ++k) rx[k] = (ix + k - nx / 2) * drx;   // cal_LJ.cu:54-56
+  const double ry = (iy - ny / 2) * dry, rz = (iz - nz / 2) * drz;
   double acc[kPts][V], afr[kPts], aes[kPts];
 #pragma unroll
   for (int k = 0; k < kPts; ++k) {
@@ -94,6 +101,7 @@ k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
       }
     }
     __syncthreads();
+    if (!live) continue;
     const int m = min(kTile, natom - t0);
     float accf[kPts][V];
 #pragma unroll
@@ -159,9 +167,10 @@ k_potential_r(int nx, int ny, int nz, double drx, double dry, double drz,
         for (int v = 0; v < V; ++v) acc[k][v] += (double)accf[k][v];
     }
   }
+  if (!live) return;
+  const size_t j = (size_t)ix + (size_t)nx * ((size_t)iy + (size_t)ny * iz);
 #pragma unroll
   for (int k = 0; k < kPts; ++k) {
-    if (j + k >= n) break;
 #pragma unroll
     for (int v = 0; v < V; ++v) u[(size_t)v * n + j + k] = acc[k][v];
     fr[j + k] = afr[k] * ubeta;
@@ -249,16 +258,17 @@ k_potential_k(int nx, int ny, int nz, double bx, double by, double bz,
 
 template <int V>
 void launch_r(Context &c, const SiteLJ &sl, double ikbt, double ubeta) {
-  long long blocks = (c.n / kPts + kThreads - 1) / kThreads;
-  const dim3 grid((unsigned)blocks, c.nb);
+  const int bx = (c.nx + kBrick - 1) / kBrick, by = (c.ny + kBrick - 1) / kBrick,
+            bz = (c.nz + kBrick - 1) / kBrick;
+  const dim3 grid((unsigned)((long long)bx * by * bz), c.nb);
   if (c.prm.precision == RISM3D_MIXED)
     k_potential_r<V, true><<<grid, kThreads, 0, c.stream>>>(
-        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.d_atom_off, c.d_atom_cnt, sl,
-        ikbt, ubeta, c.d_u, c.d_e, c.d_fr);
+        c.nx, c.ny, c.nz, bx, by, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.d_atom_off,
+        c.d_atom_cnt, sl, ikbt, ubeta, c.d_u, c.d_e, c.d_fr);
   else
     k_potential_r<V, false><<<grid, kThreads, 0, c.stream>>>(
-        c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.d_atom_off, c.d_atom_cnt, sl,
-        ikbt, ubeta, c.d_u, c.d_e, c.d_fr);
+        c.nx, c.ny, c.nz, bx, by, c.dr[0], c.dr[1], c.dr[2], c.d_atoms, c.d_atom_off,
+        c.d_atom_cnt, sl, ikbt, ubeta, c.d_u, c.d_e, c.d_fr);
 }
 
 }  // namespace
