@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-cli", action="store_true",
+                   help="skip the whole-process timing of the drop-in executable")
+    p.add_argument("--cli-reps", type=int, default=3)
     p.add_argument("--cpu-iters", type=int, default=2,
                    help="iterations in the CPU-oracle sample")
     p.add_argument("--batch-mols", type=int, default=256,
@@ -244,6 +247,11 @@ def run_ours(args, rank, world, dist):
                            ("pass_r_fp64", 2, bpp64["pass_r"])):
         ms = fp64.time_kernel(kid, 20)
         kern[name] = {"ms": ms, "gbs": bpp * n / ms / 1e6}
+    # the real-space potential grids (LJ per site, esr, fr): pair evaluations/s
+    pairs = n * len(sol.q)
+    for name, solver in (("potential_r_mixed", mixed), ("potential_r_fp64", fp64)):
+        ms = solver.time_kernel(20, 3)
+        kern[name] = {"ms": ms, "gpairs_per_s": pairs / ms / 1e6}
     # adjoint gradients of mu_ex (all charges, LJ parameters, positions) on
     # the converged mixed solve: the exact discrete adjoint
     torch.cuda.synchronize()
@@ -255,6 +263,15 @@ def run_ours(args, rank, world, dist):
     adjoint_s = time.perf_counter() - t1
     mixed.close(); fp64.close()
     batch = run_batch(args, dev, stream, rank, world, dist) if args.batch_mols > 0 else None
+    cli = None
+    if rank == 0 and not args.no_cli:
+        c64, i64, f64 = time_cli(args, 0, args.cli_reps)
+        c32, i32, f32 = time_cli(args, 1, args.cli_reps)
+        cli = {"cli_fp64_s": c64, "cli_mixed_s": c32, "iterations_fp64": i64,
+               "iterations_mixed": i32, "sfe_sc_fp64": f64, "sfe_sc_mixed": f32,
+               "reps": args.cli_reps,
+               "what": "bin/rism3d-b200 on the same control file, whole-process wall time "
+                       "(context, file reads, solve, .xmu), as the reference executable is timed"}
     dom = "pass_a_fp32"
     achieved = kern[dom]["gbs"]
     traffic_pp = read_traffic("k_pass_a_fp32")
@@ -295,6 +312,7 @@ def run_ours(args, rank, world, dist):
                      "algorithmic_bytes_per_launch": bpp32["pass_a"] * n,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
         "batch": batch,
+        "cli": cli,
         "adjoint": {"s_per_gradient": adjoint_s, "timing": "second call (the first allocates scratch)",
                     "outputs": "d mu/d(q, sigma, eps, xyz) of all "
                     "%d atoms" % len(sol.q)},
@@ -392,6 +410,36 @@ def run_batch(args, dev, stream, rank=0, world=1, dist=False):
             "precision": "FP32 bulk + FP64 polish"}
 
 
+# ------------------------------------------------- whole-process drop-in
+def time_cli(args, prec, reps):
+    """Wall time of the drop-in executable (bin/rism3d-b200) as a whole
+    process on the workload's control file: CUDA context, file reads, the
+    solve and the .xmu output, the way the reference executable is timed
+    (its README times whole runs).  prec 0: plain FP64; 1: -p 1 (FP32 bulk
+    + FP64 polish).  Returns (mean seconds, iterations, SFE_SC)."""
+    exe = os.path.join(ROOT, "3d-rism-cuda_b200", "bin", "rism3d-b200")
+    work = tempfile.mkdtemp(prefix="rism_cli_")
+    ctrl, _, _ = workload()
+    shutil.copyfile(os.path.join(GOLDEN, WORKLOAD + ".inp"), os.path.join(work, WORKLOAD + ".inp"))
+    shutil.copyfile(os.path.join(GOLDEN, ctrl.fsolvent), os.path.join(work, ctrl.fsolvent))
+    dev = os.environ.get("LOCAL_RANK", "0")
+    times, iters, sfe = [], None, None
+    for i in range(1 + reps):                     # one untimed warm-up run
+        t0 = time.perf_counter()
+        p = subprocess.run([exe, "-d", dev, "-p", str(prec), WORKLOAD + ".inp"], cwd=work,
+                           capture_output=True, text=True, timeout=600)
+        dt = time.perf_counter() - t0
+        if p.returncode != 0:
+            raise RuntimeError("rism3d-b200 failed: " + p.stderr[-500:])
+        if i > 0:
+            times.append(dt)
+        iters = len(re.findall(r"Step = \d+", p.stdout))
+        out = open(os.path.join(work, WORKLOAD + ".xmu")).read()
+        sfe = float(re.search(r"SFE_SC=\s*(\S+)", out).group(1))
+    shutil.rmtree(work, ignore_errors=True)
+    return sum(times) / len(times), iters, sfe
+
+
 # ------------------------------------------------------------ CPU oracle
 def cpu_baseline(args):
     """The CPU FP64 OpenMP oracle on a bounded sample of the same solve:
@@ -450,9 +498,9 @@ def run_reference(args):
             "config": {"workload": "same control file, reference 3drism-cuda (FP64, AN2) built "
                                    "from its own sources for sm_100a, whole-process wall time",
                        "iterations": iters, "sfe_sc": sfe},
-            "cpu_baseline": {"value": v, "unit": "s/solve", "cores": 1, "kind": "reference",
-                             "sample": "whole reference executable per step (1 host thread "
-                                       "driving the same B200)"},
+            "reference_kind": "the reference's own CUDA executable on the same B200 (it has no "
+                              "CPU implementation of the path)",
+            "cpu_baseline": cpu_baseline(args),
             "e2e": {"value": v, "unit": "s/solve", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 

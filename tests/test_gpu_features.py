@@ -4,6 +4,7 @@ non-cubic cells, SE per (site, atom), the drop-in executable and its output
 files, input validation, and the reference executable's own 128^3/256^3
 outputs recorded on a B200 (tests/golden/ref_b200)."""
 import json
+import re
 import os
 import shutil
 import struct
@@ -463,3 +464,61 @@ def test_host_driven_iteration_matches_the_device_loop():
     for dev, host in zip(*res):
         assert dev[0] == host[0] and dev[1] == host[1]
         assert abs(dev[2] - host[2]) < 1e-6
+
+
+def _read_grid_text(path, natv):
+    """.huv / .cuv (output_huv.cu:7-45, output_cuv.cu:7-45): box, grid, the
+    solute block, natv, then one line of natv values per grid point."""
+    lines = open(path).read().split("\n")
+    natom = int(lines[2])
+    assert int(lines[3 + natom]) == natv
+    body = " ".join(lines[4 + natom:]).split()
+    return np.array(body, dtype=float).reshape(-1, natv).T
+
+
+def test_cli_grid_files_match_oracle_and_tuv_round_trip(tmp_path):
+    """The drop-in executable's .huv, .cuv and .qv payloads against the
+    oracle's grids (values only: the reference's solute block prints its
+    coordinates with a stride bug, output_cuv.cu:25-31), then the .tuv
+    restart file: a run with ksave != 0 writes it (iterate.cu:64-71,
+    write_tuv.cu:7-33) and the next run of the same input reads it back
+    (iterate.cu:25-33, read_tuv.cu:6-34) and converges within 3 steps to the
+    same result."""
+    d = tmp_path / "grids"
+    d.mkdir()
+    txt = open(os.path.join(GOLDEN, "cfg0_chain12.inp")).read()
+    txt = txt.replace(" m    0", " mhcq    1", 1)
+    (d / "cfg0_chain12.inp").write_text(txt)
+    solvent = txt.split()[4]
+    shutil.copyfile(os.path.join(GOLDEN, solvent), str(d / solvent))
+    p = subprocess.run([CLI, "cfg0_chain12.inp"], cwd=str(d), capture_output=True, text=True,
+                       timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    case, _, _ = load_case("cfg0_chain12")
+    o = O.solve(case, want_grids=True)
+    V, n = case.sv.natv, case.n
+    dv = case.box[0] * case.box[1] * case.box[2] / n
+    h = _read_grid_text(str(d / "cfg0_chain12.huv"), V)
+    c = _read_grid_text(str(d / "cfg0_chain12.cuv"), V)
+    assert h.shape == (V, n) and c.shape == (V, n)
+    # 6 significant digits in the files; the solve converged to 1e-6
+    assert rel_err(h, o["h"]) < 1e-4
+    assert rel_err(c, o["h"] - o["t"]) < 1e-4
+    qv = np.loadtxt(str(d / "cfg0_chain12.qv"))
+    assert qv.shape == (n, 4)
+    rq = np.asarray(case.sv.rhov) * np.asarray(case.sv.qv)
+    want_qv = (rq[:, None] * o["g"]).sum(axis=0) * dv          # cal_qv.cu:20-27
+    assert rel_err(qv[:, 3], want_qv) < 1e-4
+    # grid coordinates of the .qv lines (x fastest, centred)
+    assert np.allclose(qv[:3, 0], (np.arange(3) - case.grid[0] // 2) * case.box[0] / case.grid[0])
+    tuv = d / "cfg0_chain12.tuv"
+    assert tuv.exists()
+    first = F.parse_xmu(str(d / "cfg0_chain12.xmu"))
+    p2 = subprocess.run([CLI, "cfg0_chain12.inp"], cwd=str(d), capture_output=True, text=True,
+                        timeout=300)
+    assert p2.returncode == 0, p2.stdout + p2.stderr
+    steps = [int(x) for x in re.findall(r"Step = (\d+)", p2.stdout)]
+    assert 1 <= max(steps) <= 3, steps
+    second = F.parse_xmu(str(d / "cfg0_chain12.xmu"))
+    for k in ("SFE_SC", "SFE_GF"):
+        assert abs(second[k] - first[k]) < MU_TOL
