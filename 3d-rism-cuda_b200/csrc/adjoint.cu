@@ -42,6 +42,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <type_traits>
 #include <vector>
 
 #include "rism3d_impl.h"
@@ -86,13 +87,22 @@ __global__ void k_delta(long long n, int nv, const double *fr, const double *fin
   }
 }
 
-// closure derivative G = C'(x), x = t_SR - U_SR (KH: 1 for x >= 0, else e^x)
-__global__ void k_gprime(long long tot, int closure, const double *t, const double *U, double *G) {
+// closure derivative G = C'(x), x = t_SR - U_SR (KH: 1 for x >= 0, else e^x),
+// stored in the solve's precision T
+template <typename T>
+__global__ void k_gprime(long long tot, int closure, const double *t, const double *U, T *G) {
   for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
        f += (long long)gridDim.x * blockDim.x) {
     const double x = t[f] - U[f];
-    G[f] = (closure == 0 && x >= 0.0) ? 1.0 : exp(x);
+    G[f] = (T)((closure == 0 && x >= 0.0) ? 1.0 : exp(x));
   }
+}
+
+template <typename A, typename B>
+__global__ void k_cast(long long n, const A *src, B *dst) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x)
+    dst[j] = (B)src[j];
 }
 
 // One Anderson step's bookkeeping in one pass:
@@ -101,25 +111,30 @@ __global__ void k_gprime(long long tot, int closure, const double *t, const doub
 // and the partial dots of r with the first ns residual slots (the slot
 // itself contributes |r|^2) and |r|^2 (last row), summed in a fixed order by
 // k_sum_rows.  The other slots are read before the slot is written.
+// T is the storage precision of the solve (double or float); the residual
+// is formed and the dots are accumulated in FP64.
+template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_residual_dots(long long tot, const double *__restrict__ G, const double *__restrict__ w,
-                const double *__restrict__ Lxi, const double *__restrict__ xi, double eta,
-                double *const *rs, int slot, int ns, double *__restrict__ ys, double *part) {
+k_residual_dots(long long tot, const T *__restrict__ G, const T *__restrict__ w,
+                const T *__restrict__ Lxi, const T *__restrict__ xi, double eta,
+                T *const *rs, int slot, int ns, T *__restrict__ ys, double *part) {
   __shared__ double red[kThreads / 32][kDepth + 1];
   double acc[kDepth + 1];
 #pragma unroll
   for (int i = 0; i <= kDepth; ++i) acc[i] = 0.0;
-  double *__restrict__ rslot = rs[slot];
+  T *__restrict__ rslot = rs[slot];
   for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
        f += (long long)gridDim.x * blockDim.x) {
     const double g = G[f], x = xi[f];
-    const double r = (g - 1.0) * (w[f] + Lxi[f]) - g * x;
+    const double rd = (g - 1.0) * ((double)w[f] + (double)Lxi[f]) - g * x;
+    const T rt = (T)rd;
+    const double r = (double)rt;             // the stored value enters the dots
 #pragma unroll
     for (int i = 0; i < kDepth; ++i)
-      if (i < ns) acc[i] += r * (i == slot ? r : rs[i][f]);
+      if (i < ns) acc[i] += r * (i == slot ? r : (double)rs[i][f]);
     acc[kDepth] += r * r;
-    rslot[f] = r;
-    ys[f] = x + eta * r;
+    rslot[f] = rt;
+    ys[f] = (T)(x + eta * r);
   }
 #pragma unroll
   for (int i = 0; i <= kDepth; ++i) {
@@ -153,36 +168,39 @@ __global__ void k_sum_rows(const double *part, int ncols, double *out) {
   if (threadIdx.x == 0) out[k] = red[0];
 }
 
+template <typename T>
 struct Mix {
-  const double *ys[kDepth];   // xi_i + eta r_i of the stored steps
+  const T *ys[kDepth];        // xi_i + eta r_i of the stored steps
   double c[kDepth];
   int ns;
 };
 
-// xi = sum_i c_i y_i, y_i = xi_i + eta r_i
-__global__ void k_combine(long long tot, Mix mx, double *xi) {
+// xi = sum_i c_i y_i, y_i = xi_i + eta r_i (summed in FP64)
+template <typename T>
+__global__ void k_combine(long long tot, Mix<T> mx, T *xi) {
   for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < tot;
        f += (long long)gridDim.x * blockDim.x) {
     double s = 0.0;
 #pragma unroll
     for (int i = 0; i < kDepth; ++i)
-      if (i < mx.ns) s += mx.c[i] * mx.ys[i][f];
-    xi[f] = s;
+      if (i < mx.ns) s += mx.c[i] * (double)mx.ys[i][f];
+    xi[f] = (T)s;
   }
 }
 
 // zeta (L xi + w, or G xi / (G - 1) where G < 1/2), then the weights
 //   W_a = rho_a (g_a - zeta_a / 2),  Omega = sum_a rho_a q_a (zeta_a - h_a)
+template <typename T>
 __global__ void k_weights(long long n, int nv, const double *g, const double *h,
-                          const double *G, const double *xi, const double *Lxi,
+                          const T *G, const T *xi, const T *Lxi,
                           const double *w, SiteW sv, double *W, double *Om) {
   for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
        j += (long long)gridDim.x * blockDim.x) {
     double om = 0.0;
     for (int v = 0; v < nv; ++v) {
       const size_t i = (size_t)v * n + j;
-      const double gp = G[i];
-      const double zeta = gp < 0.5 ? gp * xi[i] / (gp - 1.0) : Lxi[i] + w[i];
+      const double gp = G[i], x = xi[i];
+      const double zeta = gp < 0.5 ? gp * x / (gp - 1.0) : (double)Lxi[i] + w[i];
       W[i] = sv.rho[v] * (g[i] - 0.5 * zeta);
       om += sv.rho[v] * sv.q[v] * (zeta - h[i]);
     }
@@ -193,7 +211,11 @@ __global__ void k_weights(long long n, int nv, const double *g, const double *h,
 // Real-space back-propagation, one atom per thread:
 //   W-weighted derivatives of beta u_LJ (N_A kB T units cancel) and of
 //   q_v e (x cc), plus the Omega-weighted derivative of fr (x cc / 2).
-template <int V>
+// 1/r comes from the refined reciprocal square root (1/r^2 as its square),
+// and e^-r is dropped beyond 40 A (below 4.3e-18, as in the potential
+// kernel).  MIX evaluates the LJ pair factors in FP32 (the FP32 variant);
+// the Coulomb and long-range terms and every sum stay FP64.
+template <int V, bool MIX>
 __global__ void __launch_bounds__(kAtomsPerBlock)
 k_adjoint_r(int nx, int ny, int nz, double drx, double dry, double drz,
             const double *__restrict__ W, const double *__restrict__ Om,
@@ -209,13 +231,17 @@ k_adjoint_r(int nx, int ny, int nz, double drx, double dry, double drz,
     const double *a = atoms + 8 * (size_t)ia;
     X = a[0]; Y = a[1]; Z = a[2]; qu = a[3]; su = a[4]; eu = a[5];
   }
-  double sg[V], sg2[V], euv[V], deps_fac[V], qc[V];
+  // per site: sigma_uv^2 and the prefactors of d/d sigma_u, d/d eps_u and
+  // the radial force of the LJ term
+  double sg2[V], fs[V], fe[V], ff[V], qc[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) {
-    sg[v] = (su + sv.sig[v]) * 0.5;               // cal_LJ.cu:28
-    sg2[v] = sg[v] * sg[v];
-    euv[v] = sqrt(eu * sv.eps[v]);               // cal_LJ.cu:29
-    deps_fac[v] = eu > 0.0 ? 0.5 * euv[v] / eu : 0.0;
+    const double sg = (su + sv.sig[v]) * 0.5;    // cal_LJ.cu:28
+    const double euv = sqrt(eu * sv.eps[v]);     // cal_LJ.cu:29
+    sg2[v] = sg * sg;
+    fs[v] = 12.0 * euv / sg;
+    fe[v] = eu > 0.0 ? 2.0 * euv / eu : 0.0;
+    ff[v] = 24.0 * euv;
     qc[v] = sv.q[v] * cc;
   }
   double acc[NOUT] = {0, 0, 0, 0, 0, 0};
@@ -245,21 +271,31 @@ k_adjoint_r(int nx, int ny, int nz, double drx, double dry, double drz,
       const double dx = p.x - X, dy = p.y - Y, dz = p.z - Z;
       const double r2 = dx * dx + dy * dy + dz * dz;
       const bool clamped = r2 < 1.0e-4;            // cal_LJ.cu:64
-      const double ir2 = clamped ? 1.0e4 : 1.0 / r2;
-      const double ri = r2 > 0.0 ? rsqrt(r2) : 0.0;
+      const double ri = r2 > 0.0 ? rsqrt_nr<2>(r2) : 0.0;
+      const double ir2 = clamped ? 1.0e4 : ri * ri;
       const double ra = r2 * ri;
       const bool coul = ra >= 1.0e-5;              // cal_Coulomb.cu:114
       double wq = 0.0, fr = 0.0;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         const double w = pw[v][i];
-        const double s2 = sg2[v] * ir2;
-        const double s6 = s2 * s2 * s2, s12 = s6 * s6;
         // w = 0 in the solute core, where g and zeta underflow
         if (w != 0.0) {
-          acc[1] += w * 12.0 * euv[v] / sg[v] * (2.0 * s12 - s6);  // d/d sigma_u
-          acc[2] += w * 4.0 * (s12 - s6) * deps_fac[v];           // d/d eps_u
-          if (!clamped) fr += w * 24.0 * euv[v] * (2.0 * s12 - s6) * ir2;
+          double b12, b6;                          // 2 s^12 - s^6 and s^12 - s^6
+          if (MIX) {
+            const float s2 = (float)sg2[v] * (float)ir2;
+            const float s6 = s2 * s2 * s2, s12 = s6 * s6;
+            b12 = (double)(2.0f * s12 - s6);
+            b6 = (double)(s12 - s6);
+          } else {
+            const double s2 = sg2[v] * ir2;
+            const double s6 = s2 * s2 * s2, s12 = s6 * s6;
+            b12 = 2.0 * s12 - s6;
+            b6 = s12 - s6;
+          }
+          acc[1] += w * fs[v] * b12;               // d/d sigma_u
+          acc[2] += w * fe[v] * b6;                // d/d eps_u
+          if (!clamped) fr += w * ff[v] * b12 * ir2;
         }
         if (coul) wq += w * qc[v];
       }
@@ -268,7 +304,7 @@ k_adjoint_r(int nx, int ny, int nz, double drx, double dry, double drz,
       if (coul) {
         acc[0] += wq * ri;
         fr += wq * qu * ri * ri * ri;
-        const double em = exp(-ra);
+        const double em = ra < 40.0 ? exp(-ra) : 0.0;
         const double phi = (1.0 - em) * ri;
         const double dphi = (ra * em - (1.0 - em)) * ri * ri;      // d phi / d r
         acc[0] += om * phi;
@@ -453,80 +489,145 @@ void anderson_coefficients(const std::vector<double> &gram, int m, std::vector<d
   c.assign(x.begin(), x.begin() + m);
 }
 
-template <int V>
+// The transposed solve's operator in precision T: (L v)_a = F^-1[sum_b
+// X_ab F[v_b]] with the iteration's own k-space pass between the transforms.
+template <typename T> struct OzOp;
+
+template <> struct OzOp<double> {
+  Context &c;
+  double2 *buf;
+  explicit OzOp(Context &cc, double2 *b) : c(cc), buf(b) {}
+  int apply(int V, const double *v, double *out, const StageParams *sp, DevState *st) {
+    const int gb = blocks_for(c.n);
+    k_pack<<<gb, kThreads, 0, c.stream>>>(c.n, V, c.nx, c.ny, c.d_tw, v, buf);
+    if (cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)buf, (cufftDoubleComplex *)buf,
+                     CUFFT_FORWARD) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
+    int rc = launch_oz_kspace(c, buf, sp, st);
+    if (rc != RISM3D_OK) return rc;
+    if (cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)buf, (cufftDoubleComplex *)buf,
+                     CUFFT_INVERSE) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
+    k_unpack<<<gb, kThreads, 0, c.stream>>>(c.n, V, c.nx, c.ny, c.d_tw, 1.0 / c.vol, buf, out);
+    c.launches += 2;
+    return RISM3D_OK;
+  }
+};
+
+template <> struct OzOp<float> {
+  Context &c;
+  float2 *buf;
+  explicit OzOp(Context &cc, float2 *b) : c(cc), buf(b) {}
+  int apply(int V, const float *v, float *out, const StageParams *sp, DevState *st) {
+    const int gb = blocks_for(c.n);
+    k_pack32<<<gb, kThreads, 0, c.stream>>>(c.n, V, c.nx, c.ny, c.d_twf, v, buf);
+    if (cufftExecC2C(c.plan32, (cufftComplex *)buf, (cufftComplex *)buf, CUFFT_FORWARD) !=
+        CUFFT_SUCCESS)
+      return RISM3D_CUFFT_ERROR;
+    int rc = launch_oz_kspace32(c, buf, sp, st);
+    if (rc != RISM3D_OK) return rc;
+    if (cufftExecC2C(c.plan32, (cufftComplex *)buf, (cufftComplex *)buf, CUFFT_INVERSE) !=
+        CUFFT_SUCCESS)
+      return RISM3D_CUFFT_ERROR;
+    k_unpack32<<<gb, kThreads, 0, c.stream>>>(c.n, V, c.nx, c.ny, c.d_twf, (float)(1.0 / c.vol),
+                                              buf, out);
+    c.launches += 2;
+    return RISM3D_OK;
+  }
+};
+
+// Solve tolerance (relative residual) per precision: FP64 solves to 1e-10;
+// FP32 stores its residuals in FP32, whose rounding leaves a floor near
+// 1e-7 of |b|, so it stops at 2e-6 (or, stalled at its floor, within 10x
+// of that).
+template <typename T> struct SolveTol;
+template <> struct SolveTol<double> { static constexpr double tol = 1.0e-10; };
+template <> struct SolveTol<float> { static constexpr double tol = 2.0e-6; };
+
+// T: arithmetic and storage of the transposed-Jacobian solve (double: the
+// FP64 adjoint; float: the FP32 variant, with FP64 dot products, mixing
+// coefficients and sums).  The right-hand side w = L delta and the mismatch
+// delta are formed in FP64 in both.
+template <int V, typename T>
 int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
   const long long n = c.n, tot = (long long)V * n;
   const int P = (V + 1) / 2, gb = blocks_for(n), gt = blocks_for(tot);
   const int A = c.natom;
+  constexpr bool F32 = sizeof(T) == 4;
   Scratch S(c);
-  double *G = S.get<double>(tot), *w = S.get<double>(tot), *xi = S.get<double>(tot);
-  double *Lxi = S.get<double>(tot), *tmp = S.get<double>(tot), *Om = S.get<double>(n);
-  double *ys = S.get<double>((size_t)kDepth * tot), *rs = S.get<double>((size_t)kDepth * tot);
+  double *w64 = S.get<double>(tot), *tmp = S.get<double>(tot), *Om = S.get<double>(n);
+  T *G = S.get<T>(tot), *xi = S.get<T>(tot), *Lxi = S.get<T>(tot);
+  T *w = F32 ? S.get<T>(tot) : (T *)w64;
+  T *ys = S.get<T>((size_t)kDepth * tot), *rs = S.get<T>((size_t)kDepth * tot);
   double *dpart = S.get<double>((size_t)(kDepth + 1) * kDotBlocks);
   double *dsum = S.get<double>(kDepth + 1);
-  double **hist = S.get<double *>(kDepth);
+  T **hist = S.get<T *>(kDepth);
   StageParams *sp0 = S.get<StageParams>(1), *spq = S.get<StageParams>(1);
   DevState *st0 = S.get<DevState>(1);
   double2 *buf = c.d_buf;                       // the solve is finished: reuse
-  if (!G || !w || !xi || !Lxi || !tmp || !Om || !ys || !rs || !dpart || !dsum || !hist ||
-      !sp0 || !spq || !st0) {
+  typedef typename std::conditional<F32, float2, double2>::type CT;
+  CT *bufT = F32 ? (CT *)c.f_buf : (CT *)buf;
+  if (F32 && !bufT) bufT = (CT *)S.get<float2>((size_t)P * n);
+  if (!G || !w || !w64 || !xi || !Lxi || !tmp || !Om || !ys || !rs || !dpart || !dsum ||
+      !hist || !sp0 || !spq || !st0 || !bufT) {
     c.err = "adjoint: out of device memory";
     return RISM3D_CUDA_ERROR;
+  }
+  if (F32 && !c.plan32) {                       // FP64 context: the FP32 plan, made once
+    int dims[3] = {c.nz, c.ny, c.nx};
+    if (!cufft_ok(c, cufftPlanMany(&c.plan32, 3, dims, nullptr, 1, (int)n, nullptr, 1, (int)n,
+                                   CUFFT_C2C, P), "cufftPlanMany C2C"))
+      return RISM3D_CUFFT_ERROR;
   }
   StageParams zero{}, q{};
   for (int v = 0; v < V; ++v) q.qcf[v] = c.qv[v] * c.cf_final;
   DevState run{};
-  std::vector<const double *> hp(kDepth);
+  std::vector<T *> hp(kDepth);
   for (int i = 0; i < kDepth; ++i) hp[i] = rs + (size_t)i * tot;
   if (!cuda_ok(c, cudaMemcpyAsync(sp0, &zero, sizeof(zero), cudaMemcpyHostToDevice, c.stream), "adjoint") ||
       !cuda_ok(c, cudaMemcpyAsync(spq, &q, sizeof(q), cudaMemcpyHostToDevice, c.stream), "adjoint") ||
       !cuda_ok(c, cudaMemcpyAsync(st0, &run, sizeof(run), cudaMemcpyHostToDevice, c.stream), "adjoint") ||
-      !cuda_ok(c, cudaMemcpyAsync(hist, hp.data(), sizeof(double *) * kDepth,
+      !cuda_ok(c, cudaMemcpyAsync(hist, hp.data(), sizeof(T *) * kDepth,
                                   cudaMemcpyHostToDevice, c.stream), "adjoint") ||
       !cuda_ok(c, cudaStreamSynchronize(c.stream), "adjoint"))
     return RISM3D_CUDA_ERROR;
   if (!cufft_ok(c, cufftSetStream(c.plan64, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
-  auto fft = [&](int dir) {
-    return cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)buf, (cufftDoubleComplex *)buf, dir);
-  };
-  // (L v)_a = F^-1[sum_b X_ab F[v_b]]
-  auto applyL = [&](const double *v, double *out) -> int {
-    k_pack<<<gb, kThreads, 0, c.stream>>>(n, V, c.nx, c.ny, c.d_tw, v, buf);
-    if (fft(CUFFT_FORWARD) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
-    int rc = launch_oz_kspace(c, buf, sp0, st0);
-    if (rc != RISM3D_OK) return rc;
-    if (fft(CUFFT_INVERSE) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
-    k_unpack<<<gb, kThreads, 0, c.stream>>>(n, V, c.nx, c.ny, c.d_tw, 1.0 / c.vol, buf, out);
-    c.launches += 2;
-    return RISM3D_OK;
-  };
-  // delta = q (fr - F^-1 fk) (into tmp), w = L delta
+  if (F32 && !cufft_ok(c, cufftSetStream(c.plan32, c.stream), "cufftSetStream"))
+    return RISM3D_CUFFT_ERROR;
+  OzOp<double> L64(c, buf);
+  OzOp<T> LT(c, bufT);
+  // delta = q (fr - F^-1 fk) (into tmp), w = L delta (FP64)
   cudaMemsetAsync(buf, 0, sizeof(double2) * P * n, c.stream);
   k_fk_to_buf<<<gb, kThreads, 0, c.stream>>>(n, c.nx, c.ny, c.d_fkh, buf);
-  if (fft(CUFFT_INVERSE) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
+  if (cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)buf, (cufftDoubleComplex *)buf,
+                   CUFFT_INVERSE) != CUFFT_SUCCESS)
+    return RISM3D_CUFFT_ERROR;
   k_unpack<<<gb, kThreads, 0, c.stream>>>(n, 1, c.nx, c.ny, c.d_tw, 1.0 / c.vol, buf, Om);
   k_delta<<<gb, kThreads, 0, c.stream>>>(n, V, c.d_fr, Om, spq, tmp);
   c.launches += 3;
-  int rc = applyL(tmp, w);
+  int rc = L64.apply(V, tmp, w64, sp0, st0);
   if (rc != RISM3D_OK) return rc;
-  k_gprime<<<gt, kThreads, 0, c.stream>>>(tot, c.prm.closure, c.d_t, c.d_U, G);
+  if (F32) {
+    k_cast<double, T><<<gt, kThreads, 0, c.stream>>>(tot, w64, w);
+    c.launches += 1;
+  }
+  k_gprime<T><<<gt, kThreads, 0, c.stream>>>(tot, c.prm.closure, c.d_t, c.d_U, G);
   c.launches += 1;
   static const bool trace = getenv("RISM3D_TRACE") && getenv("RISM3D_TRACE")[0] == '1';
   const auto w0 = std::chrono::steady_clock::now();
   // Anderson-accelerated solve of G xi - (G - 1) L xi = (G - 1) w from xi = 0
-  cudaMemsetAsync(xi, 0, sizeof(double) * tot, c.stream);
-  cudaMemsetAsync(ys, 0, sizeof(double) * kDepth * tot, c.stream);
-  cudaMemsetAsync(rs, 0, sizeof(double) * kDepth * tot, c.stream);
+  cudaMemsetAsync(xi, 0, sizeof(T) * tot, c.stream);
+  cudaMemsetAsync(ys, 0, sizeof(T) * kDepth * tot, c.stream);
+  cudaMemsetAsync(rs, 0, sizeof(T) * kDepth * tot, c.stream);
   std::vector<double> gram((size_t)kDepth * kDepth, 0.0), coef;
-  double bnorm = -1.0;
-  int ns = 0, slot = 0, it = 0;
-  const double eta = 0.5, tol = 1.0e-10;
+  double bnorm = -1.0, best = 1e300;
+  int ns = 0, slot = 0, it = 0, since_best = 0;
+  const double eta = 0.5, tol = SolveTol<T>::tol;
   const int maxit = 3000;
+  bool stalled = false;
   for (; it < maxit; ++it) {
-    rc = applyL(xi, Lxi);
+    rc = LT.apply(V, xi, Lxi, sp0, st0);
     if (rc != RISM3D_OK) return rc;
     const int nd = ns < kDepth ? ns + 1 : kDepth;      // filled slots incl. this one
-    k_residual_dots<<<kDotBlocks, kThreads, 0, c.stream>>>(
+    k_residual_dots<T><<<kDotBlocks, kThreads, 0, c.stream>>>(
         tot, G, w, Lxi, xi, eta, hist, slot, nd, ys + (size_t)slot * tot, dpart);
     k_sum_rows<<<kDepth + 1, kThreads, 0, c.stream>>>(dpart, kDotBlocks, dsum);
     c.launches += 2;
@@ -535,32 +636,37 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
         !cuda_ok(c, cudaStreamSynchronize(c.stream), "adjoint"))
       return RISM3D_CUDA_ERROR;
     if (!std::isfinite(d[kDepth])) { c.err = "adjoint solve diverged"; return RISM3D_DIVERGED; }
-    if (bnorm < 0) bnorm = sqrt(d[kDepth]);            // xi = 0: r = (G - 1) w
-    if (sqrt(d[kDepth]) <= tol * bnorm) break;
+    const double rn = sqrt(d[kDepth]);
+    if (bnorm < 0) bnorm = rn;                         // xi = 0: r = (G - 1) w
+    if (rn <= tol * bnorm) break;
+    // FP32: 200 steps without a 1 % gain end the solve at its rounding
+    // floor when that is within 10x of the target
+    if (rn < 0.99 * best) { best = rn; since_best = 0; }
+    else if (F32 && ++since_best > 200 && rn <= 10.0 * tol * bnorm) { stalled = true; break; }
     for (int i = 0; i < kDepth; ++i)
       gram[(size_t)slot * kDepth + i] = gram[(size_t)i * kDepth + slot] = d[i];
     gram[(size_t)slot * kDepth + slot] = d[kDepth];
     ns = nd;
     anderson_coefficients(gram, ns, coef);
-    Mix mx{};
+    Mix<T> mx{};
     mx.ns = ns;
     for (int a = 0; a < ns; ++a) {
       mx.ys[a] = ys + (size_t)a * tot;
       mx.c[a] = coef[a];
     }
-    k_combine<<<gt, kThreads, 0, c.stream>>>(tot, mx, xi);
+    k_combine<T><<<gt, kThreads, 0, c.stream>>>(tot, mx, xi);
     c.launches += 1;
     slot = (slot + 1) % kDepth;
   }
   if (it == maxit) { c.err = "adjoint solve did not converge"; return RISM3D_NOT_CONVERGED; }
   const auto w1 = std::chrono::steady_clock::now();
   // weights from zeta; L xi is current (the loop leaves right after applyL)
-  double *W = ys;                               // history no longer needed
+  double *W = tmp;                              // delta no longer needed
   SiteW sv{};
   for (int v = 0; v < V; ++v) {
     sv.sig[v] = c.sigv[v]; sv.eps[v] = c.epsv[v]; sv.q[v] = c.qv[v] * c.cf_final; sv.rho[v] = c.rho[v];
   }
-  k_weights<<<gb, kThreads, 0, c.stream>>>(n, V, c.d_g, c.d_h, G, xi, Lxi, w, sv, W, Om);
+  k_weights<T><<<gb, kThreads, 0, c.stream>>>(n, V, c.d_g, c.d_h, G, xi, Lxi, w64, sv, W, Om);
   c.launches += 1;
   const double cc = kHartree * kBohr * kAvogadro;      // N_A kB T x ubeta
   // real-space part: atoms in tiles of 128, grid points split in chunks
@@ -577,13 +683,15 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
   double2 *ph = S.get<double2>((size_t)A * (c.nx + c.ny + c.nz));
   double2 *omh = S.get<double2>(n / 2);
   if (!part_r || !part_k || !ph || !omh) { c.err = "adjoint: out of device memory"; return RISM3D_CUDA_ERROR; }
-  k_adjoint_r<V><<<dim3(tiles, nchunk), kAtomsPerBlock, 0, c.stream>>>(
+  k_adjoint_r<V, F32><<<dim3(tiles, nchunk), kAtomsPerBlock, 0, c.stream>>>(
       c.nx, c.ny, c.nz, c.dr[0], c.dr[1], c.dr[2], W, Om, c.d_atoms, A, sv, cc, chunk, part_r);
   double *sum_r = part_r + (size_t)nchunk * A * NOUT;
   k_sum_chunks<<<(A * NOUT + 255) / 256, 256, 0, c.stream>>>(part_r, nchunk, A, NOUT, sum_r);
   // k-space part: Omega^ = F[Omega]; -cc/2 (1/V) sum over all k = -cc/V Re over the owner half
   k_pack<<<gb, kThreads, 0, c.stream>>>(n, 1, c.nx, c.ny, c.d_tw, Om, buf);
-  if (fft(CUFFT_FORWARD) != CUFFT_SUCCESS) return RISM3D_CUFFT_ERROR;
+  if (cufftExecZ2Z(c.plan64, (cufftDoubleComplex *)buf, (cufftDoubleComplex *)buf,
+                   CUFFT_FORWARD) != CUFFT_SUCCESS)
+    return RISM3D_CUFFT_ERROR;
   k_forward_post<<<gb, kThreads, 0, c.stream>>>(n, c.nx, c.ny, c.dv, buf, omh);
   const long long L3 = (long long)A * (c.nx + c.ny + c.nz);
   k_phase_rows_adj<<<(unsigned)((L3 + 255) / 256), 256, 0, c.stream>>>(
@@ -600,11 +708,15 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
       !cuda_ok(c, cudaMemcpyAsync(hk.data(), sum_k, sizeof(double) * hk.size(), cudaMemcpyDeviceToHost, c.stream), "adjoint") ||
       !cuda_ok(c, cudaStreamSynchronize(c.stream), "adjoint"))
     return RISM3D_CUDA_ERROR;
+  c.adj_steps = it;
+  c.adj_stalled = stalled;
   if (trace) {
     const auto w2 = std::chrono::steady_clock::now();
-    fprintf(stderr, "[rism3d] adjoint: %d Anderson steps %.1f ms, back-projection %.1f ms\n", it,
+    fprintf(stderr, "[rism3d] adjoint (%s): %d Anderson steps %.1f ms, back-projection %.1f ms%s\n",
+            F32 ? "fp32" : "fp64", it,
             std::chrono::duration<double, std::milli>(w1 - w0).count(),
-            std::chrono::duration<double, std::milli>(w2 - w1).count());
+            std::chrono::duration<double, std::milli>(w2 - w1).count(),
+            stalled ? " (stopped at the FP32 floor)" : "");
   }
   // the charge-up factor of the last stage is already in the site charges
   for (int u = 0; u < A; ++u) {
@@ -618,19 +730,26 @@ int adjoint_v(Context &c, double *dq, double *dsig, double *deps, double *dR) {
   return RISM3D_OK;
 }
 
+template <int V>
+int adjoint_p(Context &c, int precision, double *dq, double *dsig, double *deps, double *dR) {
+  return precision == RISM3D_MIXED ? adjoint_v<V, float>(c, dq, dsig, deps, dR)
+                                   : adjoint_v<V, double>(c, dq, dsig, deps, dR);
+}
+
 }  // namespace
 
-int compute_adjoint(Context &c, double *dq, double *dsig, double *deps, double *dR) {
+int compute_adjoint(Context &c, int precision, double *dq, double *dsig, double *deps,
+                    double *dR) {
   if (c.nb != 1) { c.err = "gradients are for single-solute contexts"; return RISM3D_BAD_STATE; }
   switch (c.natv) {
-    case 1: return adjoint_v<1>(c, dq, dsig, deps, dR);
-    case 2: return adjoint_v<2>(c, dq, dsig, deps, dR);
-    case 3: return adjoint_v<3>(c, dq, dsig, deps, dR);
-    case 4: return adjoint_v<4>(c, dq, dsig, deps, dR);
-    case 5: return adjoint_v<5>(c, dq, dsig, deps, dR);
-    case 6: return adjoint_v<6>(c, dq, dsig, deps, dR);
-    case 7: return adjoint_v<7>(c, dq, dsig, deps, dR);
-    case 8: return adjoint_v<8>(c, dq, dsig, deps, dR);
+    case 1: return adjoint_p<1>(c, precision, dq, dsig, deps, dR);
+    case 2: return adjoint_p<2>(c, precision, dq, dsig, deps, dR);
+    case 3: return adjoint_p<3>(c, precision, dq, dsig, deps, dR);
+    case 4: return adjoint_p<4>(c, precision, dq, dsig, deps, dR);
+    case 5: return adjoint_p<5>(c, precision, dq, dsig, deps, dR);
+    case 6: return adjoint_p<6>(c, precision, dq, dsig, deps, dR);
+    case 7: return adjoint_p<7>(c, precision, dq, dsig, deps, dR);
+    case 8: return adjoint_p<8>(c, precision, dq, dsig, deps, dR);
   }
   return RISM3D_UNSUPPORTED_SHAPE;
 }

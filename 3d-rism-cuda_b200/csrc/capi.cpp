@@ -577,7 +577,24 @@ int rism3d_grad(rism3d_ctx *x, double *dq, double *dsig, double *deps, double *d
     c.err = "gradients are not defined with an ESP cube potential (it does not follow the solute)";
     return RISM3D_BAD_STATE;
   }
-  return compute_adjoint(c, dq, dsig, deps, dR);
+  return compute_adjoint(c, RISM3D_FP64, dq, dsig, deps, dR);
+}
+
+int rism3d_grad_precision(rism3d_ctx *x, int precision, double *dq, double *dsig, double *deps,
+                          double *dR) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &c = x->c;
+  cudaSetDevice(c.dev);
+  if (precision != RISM3D_FP64 && precision != RISM3D_MIXED) {
+    c.err = "precision must be RISM3D_FP64 or RISM3D_MIXED";
+    return RISM3D_BAD_INPUT;
+  }
+  if (!c.solved) { c.err = "no solution yet"; return RISM3D_BAD_STATE; }
+  if (c.d_esp) {
+    c.err = "gradients are not defined with an ESP cube potential (it does not follow the solute)";
+    return RISM3D_BAD_STATE;
+  }
+  return compute_adjoint(c, precision, dq, dsig, deps, dR);
 }
 
 int rism3d_set_esp(rism3d_ctx *x, const double *esp) {

@@ -215,6 +215,8 @@ struct Context {
   std::vector<double> euv;       // [2][V][A] (x dv)
   std::vector<double> dulj, due; // [A][3] (x dv)
   bool have_forces = false;
+  int adj_steps = 0;             // Anderson steps of the last adjoint solve
+  bool adj_stalled = false;      // FP32 adjoint stopped at its rounding floor
 
   // file-driven mode (rism3d_initialize)
   std::string outlist, fname, fsolvent, control_dir;
@@ -251,10 +253,14 @@ int compute_observables(Context &c);              // observe.cu
 int compute_atom_integrals(Context &c, bool forces);  // observe.cu
 int compute_se_from_grids(Context &c);            // observe.cu: SE totals, one solute
 int device_grid(Context &c, int which, double *out);  // observe.cu: rism3d_get_grid_device
-int compute_adjoint(Context &c, double *dq, double *dsig, double *deps,
+// precision RISM3D_FP64: FP64 throughout; RISM3D_MIXED: FP32 transposed
+// solve and FP32 LJ pair factors of the back-projection, FP64 accumulation
+int compute_adjoint(Context &c, int precision, double *dq, double *dsig, double *deps,
                     double *dR);                  // adjoint.cu
 // FP64 OZ k-space pass on a packed buffer (adjoint solve)
 int launch_oz_kspace(Context &c, double2 *buf, const StageParams *sp, DevState *st);
+// the same pass in FP32 (the adjoint's FP32 variant)
+int launch_oz_kspace32(Context &c, float2 *buf, const StageParams *sp, DevState *st);
 int fetch_grid(Context &c, int which, double *host);
 int time_kernel(Context &c, int which, int reps, double *ms);   // solver.cu
 void free_device(Context &c);

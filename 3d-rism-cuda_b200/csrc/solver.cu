@@ -1519,6 +1519,31 @@ int oz_kspace_v(Context &c, double2 *buf, const StageParams *sp, DevState *st) {
   return cuda_ok(c, cudaGetLastError(), "oz k-space") ? RISM3D_OK : RISM3D_CUDA_ERROR;
 }
 
+// The same OZ pass in FP32 (the adjoint's FP32 operator)
+template <int V>
+int oz_kspace32_v(Context &c, float2 *buf, const StageParams *sp, DevState *st) {
+  IterArgs<float> a = make_args<float>(c, false);
+  a.buf = buf; a.sp = sp; a.st = st;
+  k_kspace<float, V><<<dim3(wave_blocks(k_kspace<float, V>, c.n / 2, 1), 1), kThreads, 0,
+                       c.stream>>>(a);
+  c.launches += 1;
+  return cuda_ok(c, cudaGetLastError(), "oz k-space") ? RISM3D_OK : RISM3D_CUDA_ERROR;
+}
+
+int launch_oz_kspace32(Context &c, float2 *buf, const StageParams *sp, DevState *st) {
+  switch (c.natv) {
+    case 1: return oz_kspace32_v<1>(c, buf, sp, st);
+    case 2: return oz_kspace32_v<2>(c, buf, sp, st);
+    case 3: return oz_kspace32_v<3>(c, buf, sp, st);
+    case 4: return oz_kspace32_v<4>(c, buf, sp, st);
+    case 5: return oz_kspace32_v<5>(c, buf, sp, st);
+    case 6: return oz_kspace32_v<6>(c, buf, sp, st);
+    case 7: return oz_kspace32_v<7>(c, buf, sp, st);
+    case 8: return oz_kspace32_v<8>(c, buf, sp, st);
+  }
+  return RISM3D_UNSUPPORTED_SHAPE;
+}
+
 int launch_oz_kspace(Context &c, double2 *buf, const StageParams *sp, DevState *st) {
   switch (c.natv) {
     case 1: return oz_kspace_v<1>(c, buf, sp, st);

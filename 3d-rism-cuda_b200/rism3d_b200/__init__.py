@@ -22,7 +22,7 @@ FP64, MIXED = 0, 1
 GRID_G, GRID_H, GRID_C, GRID_T, GRID_U, GRID_E, GRID_FR, GRID_QV = range(8)
 
 EXPORTS = ["rism3d_create", "rism3d_set_solvent", "rism3d_set_solute", "rism3d_set_tuv",
-           "rism3d_solve", "rism3d_euv", "rism3d_forces", "rism3d_grad", "rism3d_get_grid",
+           "rism3d_solve", "rism3d_euv", "rism3d_forces", "rism3d_grad", "rism3d_grad_precision", "rism3d_get_grid",
            "rism3d_solve_batch", "rism3d_destroy", "rism3d_last_error",
            "rism3d_initialize", "rism3d_iterate", "rism3d_output",
            "rism3d_refresh_potentials", "rism3d_kernel_launches", "rism3d_time_kernel",
@@ -86,6 +86,7 @@ def lib():
         L.rism3d_euv.argtypes = [vp, d]
         L.rism3d_forces.argtypes = [vp, d, d]
         L.rism3d_grad.argtypes = [vp, d, d, d, d]
+        L.rism3d_grad_precision.argtypes = [vp, C.c_int, d, d, d, d]
         L.rism3d_get_grid.argtypes = [vp, C.c_int, d]
         L.rism3d_solve_batch.argtypes = [vp, C.c_int, i, i, d, d, d, d, d, C.POINTER(Result)]
         L.rism3d_destroy.argtypes = [vp]
@@ -215,10 +216,17 @@ class Solver:
         self._check(lib().rism3d_forces(self.h, _dp(a), _dp(b)))
         return a, b
 
-    def grad(self):
+    def grad(self, precision=FP64):
+        """d(SFE_SC)/d(q, sigma, eps, xyz) of every atom (J/mol per unit):
+        rism3d_grad (FP64), or with precision=MIXED the FP32 variant
+        (rism3d_grad_precision)."""
         dq = np.zeros(self.natom); ds = np.zeros(self.natom); de = np.zeros(self.natom)
         dR = np.zeros((self.natom, 3))
-        self._check(lib().rism3d_grad(self.h, _dp(dq), _dp(ds), _dp(de), _dp(dR)))
+        if precision == FP64:
+            self._check(lib().rism3d_grad(self.h, _dp(dq), _dp(ds), _dp(de), _dp(dR)))
+        else:
+            self._check(lib().rism3d_grad_precision(self.h, precision, _dp(dq), _dp(ds),
+                                                    _dp(de), _dp(dR)))
         return dq, ds, de, dR
 
     def solve_batch(self, mols):

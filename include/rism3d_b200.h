@@ -156,6 +156,17 @@ int rism3d_forces(rism3d_ctx *ctx, double *dulj, double *due);
 int rism3d_grad(rism3d_ctx *ctx, double *dmu_dq, double *dmu_dsig,
                 double *dmu_deps, double *dmu_dR);
 
+/* The same gradients in a chosen arithmetic.  RISM3D_FP64 is rism3d_grad
+ * (transposed-Jacobian solve to 1e-10 relative).  RISM3D_MIXED solves the
+ * transposed system in FP32 (FP32 operator and storage, FP64 dot products,
+ * mixing coefficients and sums) to 2e-6 relative and evaluates the LJ pair
+ * factors of the back-projection in FP32; the Coulomb and long-range terms
+ * and every accumulation stay FP64.  Works on FP64 and MIXED contexts (an
+ * FP64 context makes its FP32 transform plan on the first call).  No
+ * counterpart in the reference, which has only the cal_grad forces. */
+int rism3d_grad_precision(rism3d_ctx *ctx, int precision, double *dmu_dq,
+                          double *dmu_dsig, double *dmu_deps, double *dmu_dR);
+
 /* ESP cube potential (cal_Coulomb.cu:41-96, the reference's -e input):
  * esp[N] in Hartree/e on the cell grid, x fastest, replaces the point-charge
  * Coulomb potential e that enters the closure (e = esp hartree / (kB T));

@@ -17,7 +17,7 @@ def declared_symbols():
 def test_header_declares_reference_interface():
     syms = declared_symbols()
     for s in ("rism3d_initialize", "rism3d_iterate", "rism3d_output", "rism3d_create",
-              "rism3d_solve", "rism3d_grad", "rism3d_solve_batch", "rism3d_destroy"):
+              "rism3d_solve", "rism3d_grad", "rism3d_grad_precision", "rism3d_solve_batch", "rism3d_destroy"):
         assert s in syms
 
 

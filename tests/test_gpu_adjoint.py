@@ -119,35 +119,86 @@ def test_autograd_function_routes_backward_through_the_adjoint(tight):
     assert np.allclose(args[3].grad.numpy(), 2 * dR)
 
 
-def test_protein_scale_gradients_match_central_differences():
-    """The 846-atom solute at 256^3 (KH), solves converged to 1e-11: adjoint
-    d mu/dq of three seeded atoms against central differences (step 1e-4 e)
-    to 1e-5 relative; d mu/dx against central differences extrapolated to a
-    zero step.  The KH closure switches from e^x to 1 + x at x = 0, so mu is
-    only once differentiable in the positions and the position differences
-    carry an error linear in the step (measured ~5x larger at 5e-3 A than at
-    1e-3 A); 2 D(h) - D(2h) removes it, leaving 2e-4.  Every atom's position
-    gradient is also checked against cal_grad forces (1%: the long-range
-    mismatch term)."""
+def _fd_check(fd, ad, rel, scale):
+    """|fd - ad| <= rel * max(|fd|, scale) per entry (scale keeps a
+    component that happens to be near zero from demanding more than the
+    difference quotient can resolve)."""
+    fd, ad = np.asarray(fd), np.asarray(ad)
+    bound = rel * np.maximum(np.abs(fd), scale)
+    bad = np.abs(fd - ad) > bound
+    assert not bad.any(), (np.flatnonzero(bad), fd[bad], ad[bad])
+
+
+def test_config4_gradients_on_32_atoms_match_central_differences():
+    """Config 4: the 846-atom solute at 256^3 (KH).  The adjoint gradients of
+    all atoms in FP64 and in the FP32 variant (FP32 transposed solve and LJ
+    pair factors, FP64 sums) agree with each other; on 32 seeded atoms they
+    agree with central finite differences of the solve: charges (step 1e-4 e)
+    to 1e-4 relative, all three position components (step 1e-3 A) to 2e-4.
+    The KH closure switches from e^x to 1 + x at x = 0, so mu is only once
+    differentiable in the positions and a central difference carries an
+    error linear in the step (measured ~5x larger at 5e-3 A than at 1e-3 A);
+    the extrapolation 2 D(h) - D(2h) removes it.  LJ sigma and epsilon are
+    checked on 4 of the atoms.  The differences re-solve to a 1e-11 residual
+    in mixed precision (its FP32 refinement reaches the FP64 tolerance and
+    the last cycle is FP64), each started from the unperturbed solution.
+    Every atom's position gradient is also checked against cal_grad forces
+    (1 %: the long-range mismatch term)."""
+    import rism3d_b200 as R
     case, _, _ = load_case("cfg2_protein846_kh", conv=1e-11)
     s = _solver(case)
     s.solve()
-    dq, _, _, dR = s.grad()
+    dq, dsig, deps, dR = s.grad()
+    dq32, dsig32, deps32, dR32 = s.grad(precision=R.MIXED)
+    for a64, a32 in ((dq, dq32), (dsig, dsig32), (deps, deps32), (dR, dR32)):
+        assert np.abs(a32 - a64).max() <= 1e-4 * np.abs(a64).max(), np.abs(a32 - a64).max()
     dulj, due = s.forces()
     assert np.abs(dulj + due - dR).max() <= 1e-2 * np.abs(dR).max()
+    t0 = s.grid_array(R.GRID_T)
+    s.close()
+    fdsolver = product_solver(case, precision=R.MIXED)
+    fdsolver.set_tuv(t0)
     rng = np.random.default_rng(4)
-    atoms = rng.choice(len(case.q), 3, replace=False)
+    atoms = rng.choice(len(case.q), 32, replace=False)
 
-    def dx(u, h):
+    def mu(**kw):
+        return _mu(fdsolver, case, **kw)
+
+    def dpos(u, k, h):
         xp, xm = case.xyz.copy(), case.xyz.copy()
-        xp[u, 0] += h; xm[u, 0] -= h
-        return (_mu(s, case, xyz=xp) - _mu(s, case, xyz=xm)) / (2 * h)
+        xp[u, k] += h; xm[u, k] -= h
+        return (mu(xyz=xp) - mu(xyz=xm)) / (2 * h)
 
+    fdq, fdR = [], []
     for u in atoms:
         qp, qm = case.q.copy(), case.q.copy()
         qp[u] += 1e-4; qm[u] -= 1e-4
-        fdq = (_mu(s, case, q=qp) - _mu(s, case, q=qm)) / 2e-4
-        assert abs(fdq - dq[u]) <= 1e-5 * abs(fdq), (u, fdq, dq[u])
-        fdx = 2.0 * dx(u, 1e-3) - dx(u, 2e-3)
-        assert abs(fdx - dR[u, 0]) <= 2e-4 * abs(fdx), (u, fdx, dR[u, 0])
-    s.close()
+        fdq.append((mu(q=qp) - mu(q=qm)) / 2e-4)
+        fdR.append([2.0 * dpos(u, k, 1e-3) - dpos(u, k, 2e-3) for k in range(3)])
+    _fd_check(fdq, dq[atoms], 1e-4, 1e-2 * np.abs(dq).max())
+    _fd_check(np.array(fdR), dR[atoms], 2e-4, 1e-2 * np.abs(dR).max())
+    fds, fde = [], []
+    for u in atoms[:4]:
+        sp, sm = case.sig.copy(), case.sig.copy()
+        sp[u] += 1e-4; sm[u] -= 1e-4
+        fds.append((mu(sig=sp) - mu(sig=sm)) / 2e-4)
+        he = 1e-4 * case.eps[u]
+        ep, em = case.eps.copy(), case.eps.copy()
+        ep[u] += he; em[u] -= he
+        fde.append((mu(eps=ep) - mu(eps=em)) / (2 * he))
+    _fd_check(fds, dsig[atoms[:4]], 1e-4, 1e-2 * np.abs(dsig).max())
+    _fd_check(fde, deps[atoms[:4]], 1e-4, 1e-2 * np.abs(deps).max())
+    fdsolver.close()
+
+
+def test_fp32_adjoint_variant_matches_fp64_on_the_small_chain(tight):
+    """The FP32 variant of the adjoint (rism3d_grad_precision, MIXED) on the
+    12-atom chain agrees with the FP64 adjoint (and so with the finite
+    differences above) to 1e-5 of each gradient's largest entry."""
+    import rism3d_b200 as R
+    case, s, g64 = tight
+    s.set_solute(case.sig, case.eps, case.q, case.xyz)
+    s.solve()
+    g32 = s.grad(precision=R.MIXED)
+    for a64, a32 in zip(g64, g32):
+        assert np.abs(a32 - a64).max() <= 1e-5 * np.abs(a64).max()
