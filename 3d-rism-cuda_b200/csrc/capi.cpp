@@ -97,6 +97,11 @@ void free_device(Context &c) {
   c.hist_cap = 0;
   if (c.d_count) cudaFree(c.d_count);
   c.d_count = nullptr;
+  if (c.plan32z) cufftDestroy(c.plan32z);
+  c.plan32z = 0;
+  c.xfused = false;
+  if (c.d_xroots) cudaFree(c.d_xroots);
+  c.d_xroots = nullptr;
   if (c.plan64) cufftDestroy(c.plan64);
   if (c.plan32) cufftDestroy(c.plan32);
   if (c.plan1) cufftDestroy(c.plan1);
@@ -189,6 +194,10 @@ static int alloc_state(Context &c) {
   if (mixed && !cufft_ok(c, cufftPlanMany(&c.plan32, 3, dims, nullptr, 1, np, nullptr, 1,
                                           np, CUFFT_C2C, nbat), "cufftPlanMany C2C"))
     return RISM3D_CUFFT_ERROR;
+  if (mixed) {
+    const int rc = setup_fused_axes(c);
+    if (rc != RISM3D_OK) return rc;
+  }
   c.plans_ok = true;
   return RISM3D_OK;
 }

@@ -44,6 +44,7 @@
 #include <cstring>
 
 #include "rism3d_impl.h"
+#include "xfft.cuh"
 
 namespace rism3d {
 
@@ -80,6 +81,7 @@ struct IterArgs {
   double *hist;             // per-iteration rms (single solves, verbose) or null
   int hist_cap;
   int nofk;                 // refinement: q cf fk cancels, fk is not read
+  const float2 *xroots;     // fused-axis passes: W_nx^m, m < nx (nx == ny)
 };
 
 // Batched solves: blockIdx.y selects the solute; every per-solute array is
@@ -620,6 +622,294 @@ __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a0) {
   if (threadIdx.x == 0) *a.count = 0u;
 }
 
+// --------------------------------------------- passes with a fused axis
+// FP32 single-solute solves on grids with nx = ny = E^2 (E = 8 or 16) fold
+// two axes of each 3D transform into the streaming passes, so that cuFFT
+// only transforms along z (one strided pass per direction, c.plan32z):
+//   k_pass_ax  inverse x-DFT of the last OZ result + pass A + forward x-DFT
+//   cuFFT z    forward
+//   k_kspace_y forward y-DFT + pass K + inverse y-DFT (owner/mirror tiles)
+//   cuFFT z    inverse
+//   k_pass_rx  inverse x-DFT + pass R (residual sums, finalize)
+// DFTs along different axes commute, so passes K and R see the same values
+// as on the 3D cuFFT path.  An x line of E^2 points is held by a group of E
+// consecutive lanes, E points each (xfft.cuh); the half-shift twiddles are
+// applied per point as in the unfused passes.
+constexpr int kXThreads = 256;
+
+template <int V, int CLOS, bool REF, int E>
+__global__ void __launch_bounds__(kXThreads) k_pass_ax(IterArgs<float> a) {
+  constexpr int NX = E * E, LPB = kXThreads / E, P = (V + 1) / 2;
+  __shared__ float2 scr[LPB][(E + 1) * E];
+  const DevState *st = a.st;
+  const int done = st->done, mode = st->mode, slot = st->upd_slot;
+  if (done && st->after_done != 0) return;      // past the snapshot: idle
+  const float s1 = (float)st->s1, s2 = (float)st->s2, m = (float)st->m;
+  const long long n = a.n;
+  const int g = threadIdx.x / E, t = threadIdx.x % E;
+  const unsigned mask = (E == 16) ? (0xffffu << (threadIdx.x & 16)) : (0xffu << (threadIdx.x & 24));
+  const int lines = a.ny * a.nz;
+  const float2 *tw = a.tw;
+  const float iv = (float)a.invvol;
+  const bool need_h = done || mode != 0;
+  for (int line = blockIdx.x * LPB + g; line < lines; line += gridDim.x * LPB) {
+    const int iy = line % a.ny, iz = line / a.ny;
+    const size_t base = (size_t)line * NX;
+    const float2 twyz = cmul(tw[NX + iy], tw[NX + a.ny + iz]);
+    const int dyz = (iy + iz) & 1;
+#pragma unroll 1
+    for (int p = 0; p < P; ++p) {
+      float2 z[E];
+      if (need_h) {
+#pragma unroll
+        for (int j = 0; j < E; ++j) z[j] = a.buf[(size_t)p * n + base + t + E * j];
+        xfft::line_dft<E, true>(z, t, scr[g], a.xroots, mask);   // z[k] at ix = t + E k
+      }
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        const int ix = t + E * k;
+        const size_t j = base + ix;
+        const float dir = ((ix & 1) ^ dyz) ? -1.0f : 1.0f;
+        const float2 dkf = cmul(tw[ix], twyz);
+        float h[2] = {0.0f, 0.0f};
+        if (need_h) {
+          // inverse post-twiddle (timekb, fft3d.cu:52-60): (1/V) dir conj(dkf)
+          const float sc = iv * dir;
+          const float2 zz = cmul(z[k], make_float2(dkf.x * sc, -dkf.y * sc));
+          h[0] = zz.x;
+          h[1] = zz.y;
+        }
+        float cv[2] = {0.0f, 0.0f};
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int v = 2 * p + q;
+          if (v >= V) break;
+          const size_t i2 = (size_t)v * n + j;
+          const float tv = a.t[i2], Uv = a.U[i2];
+          if (done) {                           // pass_a_final, fused form
+            if (!REF && a.hout) {
+              a.hout[i2] = (double)h[q];
+              a.gout[i2] = (double)closure<CLOS>(tv - Uv);
+            }
+            if (done == 3 && mode != 0) {
+              const float r0 = REF ? a.R0[i2] : 0.0f;
+              const float R = residual<CLOS, REF>(h[q], tv, Uv, r0);
+              const float y = tv + m * R;
+              float tn = tv + R;
+              if (mode == 2) tn = y + s1 * (a.Y[i2] - y) + s2 * (a.Y[(size_t)V * n + i2] - y);
+              a.Y[(size_t)slot * V * n + i2] = y;
+              a.RP[(size_t)slot * V * n + i2] = R;
+              a.t[i2] = tn;
+            }
+            continue;
+          }
+          float tn = tv;
+          if (mode != 0) {
+            const float r0 = REF ? a.R0[i2] : 0.0f;
+            const float R = residual<CLOS, REF>(h[q], tv, Uv, r0);   // tr
+            const float y = tv + m * R;
+            if (mode == 1) tn = tv + R;                              // newdt0 (Picard)
+            else tn = y + s1 * (a.Y[i2] - y) + s2 * (a.Y[(size_t)V * n + i2] - y);  // newdt (AN2)
+            a.Y[(size_t)slot * V * n + i2] = y;
+            a.RP[(size_t)slot * V * n + i2] = R;
+            a.t[i2] = tn;
+          }
+          cv[q] = cfun<CLOS, REF>(tn, Uv);
+        }
+        // forward pre-twiddle (timekf, fft3d.cu:41-49): dir dkf (c_a + i c_b)
+        z[k] = cmul(make_float2(cv[0], cv[1]), make_float2(dkf.x * dir, dkf.y * dir));
+      }
+      if (done) continue;
+      xfft::line_dft<E, false>(z, t, scr[g], a.xroots, mask);    // z[k] at kx = t + E k
+#pragma unroll
+      for (int k = 0; k < E; ++k) a.buf[(size_t)p * n + base + t + E * k] = z[k];
+    }
+  }
+}
+
+template <int V, int CLOS, bool REF, int E>
+__global__ void __launch_bounds__(kXThreads) k_pass_rx(IterArgs<float> a) {
+  constexpr int NX = E * E, LPB = kXThreads / E, P = (V + 1) / 2;
+  __shared__ float2 scr[LPB][(E + 1) * E];
+  __shared__ double red[kXThreads / 32][6];
+  __shared__ bool last;
+  DevState *st = a.st;
+  if (st->done) {                                // loop stopped: count idle cycles
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->after_done += 1;
+    return;
+  }
+  const bool gram = st->count <= 0;
+  const long long n = a.n;
+  const int g = threadIdx.x / E, t = threadIdx.x % E;
+  const unsigned mask = (E == 16) ? (0xffffu << (threadIdx.x & 16)) : (0xffu << (threadIdx.x & 24));
+  const int lines = a.ny * a.nz;
+  const float2 *tw = a.tw;
+  const float iv = (float)a.invvol;
+  double w8[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) w8[v] = a.sp->irho[v];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int line = blockIdx.x * LPB + g; line < lines; line += gridDim.x * LPB) {
+    const int iy = line % a.ny, iz = line / a.ny;
+    const size_t base = (size_t)line * NX;
+    const float2 twyz = cmul(tw[NX + iy], tw[NX + a.ny + iz]);
+    const int dyz = (iy + iz) & 1;
+#pragma unroll 1
+    for (int p = 0; p < P; ++p) {
+      float2 z[E];
+#pragma unroll
+      for (int j = 0; j < E; ++j) z[j] = a.buf[(size_t)p * n + base + t + E * j];
+      xfft::line_dft<E, true>(z, t, scr[g], a.xroots, mask);
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        const int ix = t + E * k;
+        const size_t j = base + ix;
+        const float dir = ((ix & 1) ^ dyz) ? -1.0f : 1.0f;
+        const float2 dkf = cmul(tw[ix], twyz);
+        const float sc = iv * dir;
+        const float2 zz = cmul(z[k], make_float2(dkf.x * sc, -dkf.y * sc));
+        const float h[2] = {zz.x, zz.y};
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int v = 2 * p + q;
+          if (v >= V) break;
+          const size_t i2 = (size_t)v * n + j;
+          const float rb = REF ? a.R0[i2] : 0.0f;
+          const double R = (double)residual<CLOS, REF>(h[q], a.t[i2], a.U[i2], rb);
+          acc[0] += R * R;                          // cal_rms.cu:18
+          if (gram) {                               // theta30, anderson_cuda.cu:33-39
+            const double d0 = R - (double)a.RP[i2];
+            const double d1 = R - (double)a.RP[(size_t)V * n + i2];
+            acc[1] += w8[v] * R * d0;
+            acc[2] += w8[v] * R * d1;
+            acc[3] += w8[v] * d0 * d0;
+            acc[4] += w8[v] * d0 * d1;
+            acc[5] += w8[v] * d1 * d1;
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[k] = v;
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k) red[wid][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double s = 0.0;
+    for (int w = 0; w < kXThreads / 32; ++w) s += red[w][threadIdx.x];
+    a.part[(size_t)threadIdx.x * a.nblocks + blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(a.count, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_block(st, a.part, a.nblocks, (double)n * V, a.hist, a.hist_cap);
+  if (threadIdx.x == 0) *a.count = 0u;
+}
+
+// Pass K with the y-axis DFTs folded in (one site pair, P = 1).  A block
+// owns the tile of kW consecutive kx columns at one kz < nz/2 and the mirror
+// tile (columns nx - c0 - kW .. nx - c0 - 1 at nz - 1 - kz), so that every
+// owner point k and its mirror -k meet in the block: forward y-DFT of both
+// tiles into shared memory, the OZ pair product of kspace_pair on every
+// owner point, inverse y-DFT, with the buffer read and written once.  Thread
+// (col, t) moves the points y = t + E j of column col of each tile; a
+// column's E threads sit kW apart in the block, so the transposes of the
+// y-DFT go through shared memory behind block-wide barriers.
+constexpr int kW = 16;
+
+template <int E>
+struct KYLayout {
+  static constexpr int NY = E * E;
+  static constexpr int SCOL = (E + 1) * E + 1;   // transpose scratch per column
+  static constexpr int MROW = NY + 1;            // one tile column of ky values
+  static constexpr size_t bytes() {
+    return sizeof(float2) * ((size_t)kW * SCOL + (size_t)2 * kW * MROW);
+  }
+};
+
+// y-DFT of one tile column group: v in (points y = t + E j), out to the tile
+// array T[col][ky] (ky = t + E k).
+template <int E, bool INV>
+__device__ __forceinline__ void col_dft_to(float2 (&v)[E], int col, int t, float2 *scr,
+                                          float2 *T, const float2 *__restrict__ roots) {
+  using L = KYLayout<E>;
+  xfft::stage1<E, INV>(v, t, roots);
+  __syncthreads();                               // scratch free
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) scr[col * L::SCOL + k1 * (E + 1) + t] = v[k1];
+  __syncthreads();
+#pragma unroll
+  for (int s = 0; s < E; ++s) v[s] = scr[col * L::SCOL + t * (E + 1) + s];
+  xfft::dft_small<E, INV>(v);
+  if (T)
+#pragma unroll
+    for (int k = 0; k < E; ++k) T[col * L::MROW + t + E * k] = v[k];
+}
+
+template <int V, int E>
+__global__ void __launch_bounds__(kW * E, 2) k_kspace_y(IterArgs<float> a) {
+  using L = KYLayout<E>;
+  constexpr int NY = L::NY;
+  extern __shared__ float2 ksm[];
+  float2 *scr = ksm;                             // [kW][SCOL]
+  float2 *O = ksm + (size_t)kW * L::SCOL;        // owner tile [kW][MROW]
+  float2 *M = O + (size_t)kW * L::MROW;          // mirror tile [kW][MROW]
+  if (a.st->done) return;
+  const int nx = a.nx, nz = a.nz;
+  const int col = threadIdx.x % kW, t = threadIdx.x / kW;
+  const int cblocks = nx / kW, tiles = cblocks * (nz / 2);
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int cb = tile % cblocks, kz = tile / cblocks, kzm = nz - 1 - kz;
+    const int kx = cb * kW + col, kxm = nx - cb * kW - kW + col;
+    float2 v[E], vm[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int y = t + E * j;
+      v[j] = a.buf[((size_t)kz * NY + y) * nx + kx];
+      vm[j] = a.buf[((size_t)kzm * NY + y) * nx + kxm];
+    }
+    col_dft_to<E, false>(v, col, t, scr, O, a.xroots);
+    col_dft_to<E, false>(vm, col, t, scr, M, a.xroots);
+    __syncthreads();
+    // owner point (kx, ky, kz) and its mirror (nx-1-kx, ny-1-ky, nz-1-kz),
+    // which is column kW-1-col, row NY-1-ky of the mirror tile
+#pragma unroll 2
+    for (int k = 0; k < E; ++k) {
+      const int ky = t + E * k;
+      const long long j = (long long)kx + (long long)nx * (ky + (long long)NY * kz);
+      float2 y[1] = {O[col * L::MROW + ky]};
+      float2 ym[1] = {M[(kW - 1 - col) * L::MROW + (NY - 1 - ky)]};
+      float2 o[1], om[1];
+      kspace_pair<float, V>(a, j, kx, ky, kz, y, ym, o, om);
+      O[col * L::MROW + ky] = o[0];
+      M[(kW - 1 - col) * L::MROW + (NY - 1 - ky)] = om[0];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      v[j] = O[col * L::MROW + t + E * j];
+      vm[j] = M[col * L::MROW + t + E * j];
+    }
+    col_dft_to<E, true>(v, col, t, scr, nullptr, a.xroots);
+    col_dft_to<E, true>(vm, col, t, scr, nullptr, a.xroots);
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int y = t + E * j;
+      a.buf[((size_t)kz * NY + y) * nx + kx] = v[j];
+      a.buf[((size_t)kzm * NY + y) * nx + kxm] = vm[j];
+    }
+  }
+}
+
 // ------------------------------------------------------------- finalize
 // Run by the last block of pass R to finish: fixed-order reduction of the
 // block sums, then the host logic of iterate.cu:52-62 and AN2::calculate
@@ -817,8 +1107,55 @@ int wave_blocks(K kernel, long long work, int nb) {
   return (int)std::max(1LL, std::min(need, wave));
 }
 
+// Blocks for a grid-stride launch of `kernel` with `threads` threads and
+// `smem` dynamic shared memory: the work's blocks, at most one full wave.
+template <typename K>
+int wave_blocks_smem(K kernel, int threads, size_t smem, long long need) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+      sms < 1 || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+    sms = 148;
+  }
+  return (int)std::max(1LL, std::min(need, (long long)sms * per_sm));
+}
+
+template <int V, int CLOS, bool REF, int E>
+int grid_ax(const Context &c) {
+  const long long lines = (long long)c.ny * c.nz;
+  return wave_blocks_smem(k_pass_ax<V, CLOS, REF, E>, kXThreads, 0,
+                          (lines * E + kXThreads - 1) / kXThreads);
+}
+
+template <int V, int E>
+int grid_ky(const Context &c) {
+  return wave_blocks_smem(k_kspace_y<V, E>, kW * E, KYLayout<E>::bytes(),
+                          (long long)(c.nx / kW) * (c.nz / 2));
+}
+
+// One FP32 iteration with the x and y axes of the transforms folded into the
+// passes (single solute, V <= 2, nx = ny = E^2): cuFFT transforms along z.
+template <int V, int CLOS, bool REF, int E>
+void launch_iteration_x(Context &c, const IterArgs<float> &a) {
+  k_pass_ax<V, CLOS, REF, E><<<grid_ax<V, CLOS, REF, E>(c), kXThreads, 0, c.stream>>>(a);
+  cufftExecC2C(c.plan32z, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_FORWARD);
+  k_kspace_y<V, E><<<grid_ky<V, E>(c), kW * E, KYLayout<E>::bytes(), c.stream>>>(a);
+  cufftExecC2C(c.plan32z, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
+  k_pass_rx<V, CLOS, REF, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a);
+}
+
 template <typename T, int V, int CLOS, bool REF>
 void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
+  if constexpr (sizeof(T) == 4 && V <= 2) {
+    if (c.xfused) {
+      if (c.nx == 256) launch_iteration_x<V, CLOS, REF, 16>(c, a);
+      else launch_iteration_x<V, CLOS, REF, 8>(c, a);
+      return;
+    }
+  }
   const dim3 ba(wave_blocks(k_pass_a<T, V, CLOS, REF>, a.n, c.nb), c.nb),
       bk(wave_blocks(k_kspace<T, V>, a.n / 2, c.nb), c.nb), br(a.nblocks, c.nb);
   k_pass_a<T, V, CLOS, REF><<<ba, kThreads, 0, c.stream>>>(a);
@@ -850,6 +1187,7 @@ IterArgs<T> make_args(Context &c, bool fp64) {
   a.st = c.d_state; a.sp = c.d_stage; a.part = c.d_part; a.nblocks = c.nred_blocks;
   a.count = c.d_count;
   a.hist = c.nb == 1 ? c.d_hist : nullptr;
+  a.xroots = c.d_xroots;
   a.hist_cap = c.hist_cap;
   (void)fp64;
   return a;
@@ -1020,6 +1358,8 @@ int run_phase(Context &c, cufftHandle plan, T *t, T *U, T *Y, T *RP,
                                          watch ? 1 : 0, c.prm.an2_count);
   c.launches += 1;
   if (!cufft_ok(c, cufftSetStream(plan, c.stream), "cufftSetStream")) return RISM3D_CUFFT_ERROR;
+  if (c.plan32z && !cufft_ok(c, cufftSetStream(c.plan32z, c.stream), "cufftSetStream"))
+    return RISM3D_CUFFT_ERROR;
   int status = RISM3D_OK;
   static const bool trace = getenv("RISM3D_TRACE") && getenv("RISM3D_TRACE")[0] == '1';
   cudaGraphExec_t &lx = REF ? c.loop32r : (sizeof(T) == 8) ? c.loop64 : c.loop32;
@@ -1282,6 +1622,22 @@ int solve_v(Context &c, int chargeup) {
   return (status == RISM3D_CUDA_ERROR || status == RISM3D_CUFFT_ERROR) ? status : RISM3D_OK;
 }
 
+template <int V, int CLOS, int E>
+void time_fused(Context &c, const IterArgs<float> &a, int which, int reps) {
+  for (int r = 0; r < reps; ++r) {
+    switch (which) {
+      case 10: k_pass_ax<V, CLOS, false, E><<<grid_ax<V, CLOS, false, E>(c), kXThreads, 0,
+                                                c.stream>>>(a); break;
+      case 13: k_pass_ax<V, CLOS, true, E><<<grid_ax<V, CLOS, true, E>(c), kXThreads, 0,
+                                               c.stream>>>(a); break;
+      case 11: k_kspace_y<V, E><<<grid_ky<V, E>(c), kW * E, KYLayout<E>::bytes(),
+                                  c.stream>>>(a); break;
+      case 15: k_pass_rx<V, CLOS, true, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a); break;
+      default: k_pass_rx<V, CLOS, false, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a); break;
+    }
+  }
+}
+
 template <typename T, int V, int CLOS>
 int time_kernel_t(Context &c, int which, int reps, double *ms) {
   const bool fp64 = sizeof(T) == 8;
@@ -1312,7 +1668,24 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
             bar = wave_blocks(k_pass_a<T, V, CLOS, true>, a.n, 1),
             bk = wave_blocks(k_kspace<T, V>, a.n / 2, 1);
   cudaEventRecord(e0, c.stream);
-  for (int r = 0; r < reps; ++r) {
+  bool fused_done = false;
+  if constexpr (sizeof(T) == 4 && V <= 2) {
+    // the fused-axis passes the FP32 solve runs (ids as below; 14: one
+    // cuFFT transform along z)
+    if (c.xfused && which != 14) {
+      if (c.nx == 256) time_fused<V, CLOS, 16>(c, a, which, reps);
+      else time_fused<V, CLOS, 8>(c, a, which, reps);
+      fused_done = true;
+    }
+  }
+  if (which == 14) {
+    if (!c.plan32z) { c.err = "no z-axis plan (fused-axis passes are off)"; return RISM3D_BAD_STATE; }
+    cufftSetStream(c.plan32z, c.stream);
+    for (int r = 0; r < reps; ++r)
+      cufftExecC2C(c.plan32z, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_FORWARD);
+    fused_done = true;
+  }
+  for (int r = 0; r < reps && !fused_done; ++r) {
     switch (which) {
       case 0: case 10: k_pass_a<T, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a); break;
       case 13: k_pass_a<T, V, CLOS, true><<<bar, kThreads, 0, c.stream>>>(a); break;
@@ -1351,6 +1724,45 @@ int solve_c(Context &c, int cu) {
 }
 
 }  // namespace
+
+int setup_fused_axes(Context &c) {
+  c.xfused = false;
+  const char *off = getenv("RISM3D_NO_XFFT");
+  if (off && off[0] == '1') return RISM3D_OK;
+  if (c.prm.precision != RISM3D_MIXED || c.nb != 1 || c.natv < 1 || c.natv > 2 ||
+      c.nx != c.ny || (c.nx != 256 && c.nx != 64) || c.nz % 2 != 0)
+    return RISM3D_OK;
+  cudaError_t e = cudaSuccess;
+  if (c.nx == 256) {
+    const int ks = (int)KYLayout<16>::bytes();
+    e = cudaFuncSetAttribute(k_kspace_y<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ks);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_kspace_y<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ks);
+  } else {
+    const int ks = (int)KYLayout<8>::bytes();
+    e = cudaFuncSetAttribute(k_kspace_y<1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ks);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_kspace_y<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ks);
+  }
+  if (!cuda_ok(c, e, "fused-axis kernel attributes")) return RISM3D_CUDA_ERROR;
+  std::vector<float2> roots(c.nx);
+  for (int m = 0; m < c.nx; ++m) {
+    const double ang = 2.0 * kPi * m / c.nx;
+    roots[m] = make_float2((float)cos(ang), (float)-sin(ang));
+  }
+  if (!cuda_ok(c, cudaMalloc(&c.d_xroots, sizeof(float2) * c.nx), "alloc roots") ||
+      !cuda_ok(c, cudaMemcpy(c.d_xroots, roots.data(), sizeof(float2) * c.nx, cudaMemcpyHostToDevice),
+               "copy roots"))
+    return RISM3D_CUDA_ERROR;
+  // transforms along z: one per (x, y) column, stride nx ny, columns adjacent
+  int nz = c.nz, emb = c.nz;
+  const int nxy = c.nx * c.ny;
+  if (!cufft_ok(c, cufftPlanMany(&c.plan32z, 1, &nz, &emb, nxy, 1, &emb, nxy, 1, CUFFT_C2C, nxy),
+                "cufftPlanMany z"))
+    return RISM3D_CUFFT_ERROR;
+  c.xfused = true;
+  return RISM3D_OK;
+}
 
 int build_twiddles(Context &c) {
   std::vector<double2> tw(c.nx + c.ny + c.nz);
@@ -1489,7 +1901,7 @@ int time_kernel(Context &c, int which, int reps, double *ms) {
     *ms = t / reps;
     return RISM3D_OK;
   }
-  if (!(which >= 0 && which <= 2) && !(which >= 10 && which <= 13) && which != 15) {
+  if (!(which >= 0 && which <= 2) && !(which >= 10 && which <= 15)) {
     c.err = "unknown kernel id";
     return RISM3D_BAD_INPUT;
   }
