@@ -9,6 +9,7 @@
 // from its own host thread, so a sub-batch that has converged stops paying
 // for the transforms of the others.
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 #include <thread>
 #include <vector>
@@ -59,6 +60,7 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
       groups[{kv.first, (int)((long long)i * parts / total)}].push_back(kv.second[i]);
   }
   // one child context per group, each on its own stream
+  const long long call = ++p.batch_calls;
   std::vector<std::pair<Context *, const std::vector<int> *>> work;
   for (auto &kv : groups) {
     const int grid = kv.first.first.first;
@@ -69,9 +71,11 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
       if (!ch && cc.grid == grid && cc.box == box && cc.nb == nb) {
         bool taken = false;
         for (const auto &wk : work) taken = taken || wk.first == cc.ctx;
-        if (!taken) ch = cc.ctx;
+        if (!taken) { ch = cc.ctx; cc.last_call = call; }
       }
     if (!ch) {
+      size_t free0 = 0, free1 = 0, total = 0;
+      cudaMemGetInfo(&free0, &total);
       rism3d_params cp = p.prm;
       cp.grid[0] = cp.grid[1] = cp.grid[2] = grid;
       cp.box[0] = cp.box[1] = cp.box[2] = box;
@@ -89,9 +93,37 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
         delete ch;
         return rc;
       }
-      p.children.push_back({grid, nb, box, ch});
+      cudaMemGetInfo(&free1, &total);
+      Context::Child cc;
+      cc.grid = grid; cc.nb = nb; cc.box = box; cc.ctx = ch;
+      cc.last_call = call;
+      cc.bytes = free0 > free1 ? free0 - free1 : 0;
+      p.children.push_back(cc);
     }
     work.push_back({ch, &kv.second});
+  }
+  // Children not used by this call stay cached for later calls with the
+  // same shapes, up to a byte budget (RISM3D_BATCH_CACHE_BYTES, default
+  // 4 GiB); beyond it the least recently used ones are freed, so callers
+  // whose batch composition changes from call to call do not accumulate
+  // one context per composition.
+  {
+    size_t budget = 4ull << 30;
+    if (const char *e = getenv("RISM3D_BATCH_CACHE_BYTES")) budget = (size_t)strtoull(e, nullptr, 10);
+    for (;;) {
+      size_t idle = 0;
+      int lru = -1;
+      for (size_t i = 0; i < p.children.size(); ++i) {
+        const Context::Child &cc = p.children[i];
+        if (cc.last_call == call) continue;
+        idle += cc.bytes;
+        if (lru < 0 || cc.last_call < p.children[lru].last_call) lru = (int)i;
+      }
+      if (idle <= budget || lru < 0) break;
+      context_release(*p.children[lru].ctx);
+      delete p.children[lru].ctx;
+      p.children.erase(p.children.begin() + lru);
+    }
   }
   // work queued on the caller's stream before this call comes first
   cudaEvent_t start = nullptr;

@@ -239,8 +239,11 @@ struct Context {
     int grid = 0, nb = 0;
     double box = 0;
     Context *ctx = nullptr;
+    long long last_call = 0;   // batch call that last used it
+    size_t bytes = 0;          // device memory it holds (measured at creation)
   };
   std::vector<Child> children;
+  long long batch_calls = 0;
 };
 
 // ---- kernels/launchers (implemented in the .cu files) ----

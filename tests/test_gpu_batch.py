@@ -114,3 +114,37 @@ def test_batch_config3_shapes_match_oracle():
         assert abs(res[i]["sfe_sc"] - o["sfe_sc"]) < MU_TOL, (g, res[i]["sfe_sc"], o["sfe_sc"])
         assert abs(res[i]["sfe_gf"] - o["sfe_gf"]) < MU_TOL, g
         assert abs(res[i]["pmv"] - o["pmv"] * 1000) < 1e-4, g
+
+
+def test_batch_child_cache_stays_within_its_budget():
+    """Batch calls whose composition changes every call (as in a training
+    loop with random batches) each need new sub-batch contexts; the idle
+    ones are freed least recently used first once they hold more than
+    RISM3D_BATCH_CACHE_BYTES, so device memory stops growing, and results
+    stay those of fresh contexts."""
+    import torch
+    import rism3d_b200 as R
+    sv = F.read_xvk(os.path.join(GOLDEN, "h2o_vv.xvk"))
+    mols = _mols()
+    small = [m for m in mols if m[4] == 32]
+    os.environ["RISM3D_BATCH_CACHE_BYTES"] = str(64 << 20)
+    try:
+        parent = R.Solver((32, 32, 32), (16.0, 16.0, 16.0), batch_chunk_points=1 << 30)
+        parent.set_solvent_obj(sv)
+        ref = parent.solve_batch(small[:1])
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        used = []
+        for k in range(1, 25):
+            # k copies of the 32^3 solutes: a new composition every call
+            batch = (small * k)[:k + 1]
+            res = parent.solve_batch(batch)
+            assert abs(res[0]["sfe_sc"] - ref[0]["sfe_sc"]) < 1e-6 * abs(ref[0]["sfe_sc"]) + 1e-6
+            torch.cuda.synchronize()
+            used.append(free0 - torch.cuda.mem_get_info()[0])
+        parent.close()
+    finally:
+        del os.environ["RISM3D_BATCH_CACHE_BYTES"]
+    # the last calls hold their own child plus at most the budget of idle ones
+    per_solute = used[0] / 2.0
+    assert used[-1] <= (64 << 20) + 30 * per_solute + (256 << 20), (used[-1], per_solute)
