@@ -139,9 +139,10 @@ def test_config4_gradients_on_32_atoms_match_central_differences():
     differentiable in the positions and a central difference carries an
     error linear in the step (measured ~5x larger at 5e-3 A than at 1e-3 A);
     the extrapolation 2 D(h) - D(2h) removes it.  LJ sigma and epsilon are
-    checked on 4 of the atoms.  The differences re-solve to a 1e-11 residual
-    in mixed precision (its FP32 refinement reaches the FP64 tolerance and
-    the last cycle is FP64), each started from the unperturbed solution.
+    checked on 4 of the atoms.  The differences re-solve in FP64 to a 1e-11
+    residual, each started from the unperturbed solution (a mixed-precision
+    context evaluates the LJ grid in FP32, whose rounding moves mu by more
+    than the 1e-3 A position steps resolve).
     Every atom's position gradient is also checked against cal_grad forces
     (1 %: the long-range mismatch term)."""
     import rism3d_b200 as R
@@ -156,7 +157,7 @@ def test_config4_gradients_on_32_atoms_match_central_differences():
     assert np.abs(dulj + due - dR).max() <= 1e-2 * np.abs(dR).max()
     t0 = s.grid_array(R.GRID_T)
     s.close()
-    fdsolver = product_solver(case, precision=R.MIXED)
+    fdsolver = product_solver(case)
     fdsolver.set_tuv(t0)
     rng = np.random.default_rng(4)
     atoms = rng.choice(len(case.q), 32, replace=False)
