@@ -1727,8 +1727,9 @@ int solve_c(Context &c, int cu) {
 
 int setup_fused_axes(Context &c) {
   c.xfused = false;
-  const char *off = getenv("RISM3D_NO_XFFT");
-  if (off && off[0] == '1') return RISM3D_OK;
+  // opt-in (RISM3D_XFFT=1) until the fused passes beat the 3D cuFFT path
+  const char *on = getenv("RISM3D_XFFT");
+  if (!on || on[0] != '1') return RISM3D_OK;
   if (c.prm.precision != RISM3D_MIXED || c.nb != 1 || c.natv < 1 || c.natv > 2 ||
       c.nx != c.ny || (c.nx != 256 && c.nx != 64) || c.nz % 2 != 0)
     return RISM3D_OK;

