@@ -660,12 +660,19 @@ __global__ void __launch_bounds__(kXThreads) k_pass_ax(IterArgs<float> a) {
 #pragma unroll 1
     for (int p = 0; p < P; ++p) {
       float2 z[E];
+      float2 *zs = scr[g];                    // the line, point ix = t + E k at zs[k E + t]
       if (need_h) {
 #pragma unroll
         for (int j = 0; j < E; ++j) z[j] = a.buf[(size_t)p * n + base + t + E * j];
         xfft::line_dft<E, true>(z, t, scr[g], a.xroots, mask);   // z[k] at ix = t + E k
       }
+      __syncwarp(mask);                       // the transpose's reads are done
+      if (need_h)
 #pragma unroll
+        for (int k = 0; k < E; ++k) zs[k * E + t] = z[k];
+      // per point: one copy of the body (the refinement closure inlined for
+      // every point of an unrolled loop overflowed the instruction cache)
+#pragma unroll 1
       for (int k = 0; k < E; ++k) {
         const int ix = t + E * k;
         const size_t j = base + ix;
@@ -675,7 +682,7 @@ __global__ void __launch_bounds__(kXThreads) k_pass_ax(IterArgs<float> a) {
         if (need_h) {
           // inverse post-twiddle (timekb, fft3d.cu:52-60): (1/V) dir conj(dkf)
           const float sc = iv * dir;
-          const float2 zz = cmul(z[k], make_float2(dkf.x * sc, -dkf.y * sc));
+          const float2 zz = cmul(zs[k * E + t], make_float2(dkf.x * sc, -dkf.y * sc));
           h[0] = zz.x;
           h[1] = zz.y;
         }
@@ -717,8 +724,10 @@ __global__ void __launch_bounds__(kXThreads) k_pass_ax(IterArgs<float> a) {
           cv[q] = cfun<CLOS, REF>(tn, Uv);
         }
         // forward pre-twiddle (timekf, fft3d.cu:41-49): dir dkf (c_a + i c_b)
-        z[k] = cmul(make_float2(cv[0], cv[1]), make_float2(dkf.x * dir, dkf.y * dir));
+        zs[k * E + t] = cmul(make_float2(cv[0], cv[1]), make_float2(dkf.x * dir, dkf.y * dir));
       }
+#pragma unroll
+      for (int k = 0; k < E; ++k) z[k] = zs[k * E + t];
       if (done) continue;
       xfft::line_dft<E, false>(z, t, scr[g], a.xroots, mask);    // z[k] at kx = t + E k
 #pragma unroll
@@ -757,17 +766,21 @@ __global__ void __launch_bounds__(kXThreads) k_pass_rx(IterArgs<float> a) {
 #pragma unroll 1
     for (int p = 0; p < P; ++p) {
       float2 z[E];
+      float2 *zs = scr[g];
 #pragma unroll
       for (int j = 0; j < E; ++j) z[j] = a.buf[(size_t)p * n + base + t + E * j];
       xfft::line_dft<E, true>(z, t, scr[g], a.xroots, mask);
+      __syncwarp(mask);
 #pragma unroll
+      for (int k = 0; k < E; ++k) zs[k * E + t] = z[k];
+#pragma unroll 2
       for (int k = 0; k < E; ++k) {
         const int ix = t + E * k;
         const size_t j = base + ix;
         const float dir = ((ix & 1) ^ dyz) ? -1.0f : 1.0f;
         const float2 dkf = cmul(tw[ix], twyz);
         const float sc = iv * dir;
-        const float2 zz = cmul(z[k], make_float2(dkf.x * sc, -dkf.y * sc));
+        const float2 zz = cmul(zs[k * E + t], make_float2(dkf.x * sc, -dkf.y * sc));
         const float h[2] = {zz.x, zz.y};
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -832,12 +845,12 @@ struct KYLayout {
   static constexpr int SCOL = (E + 1) * E + 1;   // transpose scratch per column
   static constexpr int MROW = NY + 1;            // one tile column of ky values
   static constexpr size_t bytes() {
-    return sizeof(float2) * ((size_t)kW * SCOL + (size_t)2 * kW * MROW);
+    return sizeof(float2) * ((size_t)kW * SCOL + (size_t)kW * MROW);
   }
 };
 
-// y-DFT of one tile column group: v in (points y = t + E j), out to the tile
-// array T[col][ky] (ky = t + E k).
+// y-DFT of one tile column group: v in (points y = t + E j) and out
+// (ky = t + E k), optionally also to the tile array T[col][ky].
 template <int E, bool INV>
 __device__ __forceinline__ void col_dft_to(float2 (&v)[E], int col, int t, float2 *scr,
                                           float2 *T, const float2 *__restrict__ roots) {
@@ -861,8 +874,7 @@ __global__ void __launch_bounds__(kW * E, 2) k_kspace_y(IterArgs<float> a) {
   constexpr int NY = L::NY;
   extern __shared__ float2 ksm[];
   float2 *scr = ksm;                             // [kW][SCOL]
-  float2 *O = ksm + (size_t)kW * L::SCOL;        // owner tile [kW][MROW]
-  float2 *M = O + (size_t)kW * L::MROW;          // mirror tile [kW][MROW]
+  float2 *M = ksm + (size_t)kW * L::SCOL;        // mirror tile [kW][MROW]
   if (a.st->done) return;
   const int nx = a.nx, nz = a.nz;
   const int col = threadIdx.x % kW, t = threadIdx.x / kW;
@@ -872,33 +884,27 @@ __global__ void __launch_bounds__(kW * E, 2) k_kspace_y(IterArgs<float> a) {
     const int kx = cb * kW + col, kxm = nx - cb * kW - kW + col;
     float2 v[E], vm[E];
 #pragma unroll
-    for (int j = 0; j < E; ++j) {
-      const int y = t + E * j;
-      v[j] = a.buf[((size_t)kz * NY + y) * nx + kx];
-      vm[j] = a.buf[((size_t)kzm * NY + y) * nx + kxm];
-    }
-    col_dft_to<E, false>(v, col, t, scr, O, a.xroots);
+    for (int j = 0; j < E; ++j) vm[j] = a.buf[((size_t)kzm * NY + t + E * j) * nx + kxm];
     col_dft_to<E, false>(vm, col, t, scr, M, a.xroots);
-    __syncthreads();
-    // owner point (kx, ky, kz) and its mirror (nx-1-kx, ny-1-ky, nz-1-kz),
-    // which is column kW-1-col, row NY-1-ky of the mirror tile
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = a.buf[((size_t)kz * NY + t + E * j) * nx + kx];
+    col_dft_to<E, false>(v, col, t, scr, nullptr, a.xroots);   // owner stays in registers
+    __syncthreads();                             // M complete
+    // owner point (kx, ky, kz), ky = t + E k, and its mirror (nx-1-kx,
+    // ny-1-ky, nz-1-kz): column kW-1-col, row NY-1-ky of the mirror tile
 #pragma unroll 2
     for (int k = 0; k < E; ++k) {
       const int ky = t + E * k;
       const long long j = (long long)kx + (long long)nx * (ky + (long long)NY * kz);
-      float2 y[1] = {O[col * L::MROW + ky]};
-      float2 ym[1] = {M[(kW - 1 - col) * L::MROW + (NY - 1 - ky)]};
-      float2 o[1], om[1];
+      float2 *mp = M + (kW - 1 - col) * L::MROW + (NY - 1 - ky);
+      float2 y[1] = {v[k]}, ym[1] = {*mp}, o[1], om[1];
       kspace_pair<float, V>(a, j, kx, ky, kz, y, ym, o, om);
-      O[col * L::MROW + ky] = o[0];
-      M[(kW - 1 - col) * L::MROW + (NY - 1 - ky)] = om[0];
+      v[k] = o[0];
+      *mp = om[0];
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < E; ++j) {
-      v[j] = O[col * L::MROW + t + E * j];
-      vm[j] = M[col * L::MROW + t + E * j];
-    }
+    for (int j = 0; j < E; ++j) vm[j] = M[col * L::MROW + t + E * j];
     col_dft_to<E, true>(v, col, t, scr, nullptr, a.xroots);
     col_dft_to<E, true>(vm, col, t, scr, nullptr, a.xroots);
 #pragma unroll
@@ -909,6 +915,8 @@ __global__ void __launch_bounds__(kW * E, 2) k_kspace_y(IterArgs<float> a) {
     }
   }
 }
+
+
 
 // ------------------------------------------------------------- finalize
 // Run by the last block of pass R to finish: fixed-order reduction of the
@@ -1681,8 +1689,10 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
   if (which == 14) {
     if (!c.plan32z) { c.err = "no z-axis plan (fused-axis passes are off)"; return RISM3D_BAD_STATE; }
     cufftSetStream(c.plan32z, c.stream);
-    for (int r = 0; r < reps; ++r)
-      cufftExecC2C(c.plan32z, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_FORWARD);
+    for (int r = 0; r < reps; ++r) {
+      if constexpr (sizeof(T) == 4)
+        cufftExecC2C(c.plan32z, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_FORWARD);
+    }
     fused_done = true;
   }
   for (int r = 0; r < reps && !fused_done; ++r) {
