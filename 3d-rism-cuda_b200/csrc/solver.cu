@@ -184,15 +184,24 @@ __device__ __forceinline__ double fexpm1(double x) { return expm1(x); }
 __device__ __forceinline__ float fexpm1(float x) { return expm1f(x); }
 
 // C(x0 + d) - C(x0) to the relative precision of the difference itself
-// (refinement form): e^x0 expm1(d) on the exponential branch, d on the
-// linear KH branch, and the two mixed cases where x0 and x0 + d straddle 0
-// (there |x0| <= |d|, so nothing large cancels).
+// (refinement form).  KH: C(x) - 1 = max(x, 0) + expm1(min(x, 0)), so with
+// a = min(x0 + d, 0), b = min(x0, 0)
+//   C(x0 + d) - C(x0) = [max(x0 + d, 0) - max(x0, 0)] + e^b expm1(a - b),
+// where the linear bracket is d itself when both arguments are >= 0 and
+// a - b is d itself when both are < 0: e^x0 expm1(d) on the exponential
+// branch, d on the linear one, and in the two mixed cases (|x0| <= |d|)
+// x - expm1(x0) and expm1(x) - x0.  One exp and one expm1 per call and no
+// branches, so the lanes of a warp never split over the four cases.
 template <int CLOS, typename T>
 __device__ __forceinline__ T closure_diff(T x0, T d) {
   if (CLOS == 1) return fexp(x0) * fexpm1(d);
   const T x = x0 + d;
-  if (x0 < T(0)) return x < T(0) ? fexp(x0) * fexpm1(d) : x - fexpm1(x0);
-  return x >= T(0) ? d : fexpm1(x) - x0;
+  const bool pos = x >= T(0), pos0 = x0 >= T(0);
+  const T zero = T(0);
+  const T lin = (pos && pos0) ? d : (fmax(x, zero) - fmax(x0, zero));
+  const T b = fmin(x0, zero);
+  const T da = (!pos && !pos0) ? d : (fmin(x, zero) - b);
+  return lin + fexp(b) * fexpm1(da);
 }
 
 // Residual of the cycle at the current state: plain h + 1 - C(t - U);
