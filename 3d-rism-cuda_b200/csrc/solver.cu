@@ -644,49 +644,12 @@ __global__ void __launch_bounds__(kThreads) k_pass_r(IterArgs<T> a0) {
 // as on the 3D cuFFT path.  An x line of E^2 points is held by a group of E
 // consecutive lanes, E points each (xfft.cuh); the half-shift twiddles are
 // applied per point as in the unfused passes.
-constexpr int kXThreads = 128;
-
-// Asynchronous 16-byte copies global -> shared (cp.async, no registers held
-// while in flight), committed as one group and waited for by the issuing
-// thread; the group's lanes then synchronise to see each other's copies.
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// Shared memory of a fused pass: per line group the DFT scratch and the
-// line's per-point arrays (kArr per site: for pass A t, U, Y0, Y1, R0; for
-// pass R t, U, RP0, RP1, R0), prefetched while the line's DFT runs.
-constexpr int kArr = 5;
-template <int V, int E>
-struct XLayout {
-  static constexpr int NX = E * E, LPB = kXThreads / E, SCR = (E + 1) * E;
-  static constexpr size_t bytes() {
-    return sizeof(float2) * (size_t)LPB * SCR + sizeof(float) * (size_t)LPB * V * kArr * NX;
-  }
-};
-
-// Copy the NX points of the arrays src[0..na) of one line into dst[i][NX]
-// (E lanes, 16 bytes each per copy).
-template <int E>
-__device__ __forceinline__ void prefetch_line(float *dst, const float *const *src, int na,
-                                              int t) {
-  constexpr int NX = E * E, C = NX / 4;
-  for (int i = 0; i < na; ++i)
-#pragma unroll 4
-    for (int c = t; c < C; c += E) cp_async16(dst + (size_t)i * NX + 4 * c, src[i] + 4 * c);
-}
+constexpr int kXThreads = 256;
 
 template <int V, int CLOS, bool REF, int E>
-__global__ void __launch_bounds__(kXThreads) k_pass_ax(IterArgs<float> a) {
-  static_assert(V <= 2, "one packed site pair");
-  using L = XLayout<V, E>;
-  constexpr int NX = L::NX, LPB = L::LPB;
-  extern __shared__ float4 xsm4[];
-  float2 *scr_all = reinterpret_cast<float2 *>(xsm4);
-  float *pre_all = reinterpret_cast<float *>(scr_all + (size_t)LPB * L::SCR);
+__global__ void __launch_bounds__(kXThreads, 4) k_pass_ax(IterArgs<float> a) {
+  constexpr int NX = E * E, LPB = kXThreads / E, P = (V + 1) / 2;
+  __shared__ float2 scr[LPB][(E + 1) * E];
   const DevState *st = a.st;
   const int done = st->done, mode = st->mode, slot = st->upd_slot;
   if (done && st->after_done != 0) return;      // past the snapshot: idle
@@ -694,114 +657,98 @@ __global__ void __launch_bounds__(kXThreads) k_pass_ax(IterArgs<float> a) {
   const long long n = a.n;
   const int g = threadIdx.x / E, t = threadIdx.x % E;
   const unsigned mask = (E == 16) ? (0xffffu << (threadIdx.x & 16)) : (0xffu << (threadIdx.x & 24));
-  float2 *zs = scr_all + (size_t)g * L::SCR;    // the line: point ix = t + E k at zs[k E + t]
-  float *pre = pre_all + (size_t)g * V * kArr * NX;   // [v][array][ix]
   const int lines = a.ny * a.nz;
   const float2 *tw = a.tw;
   const float iv = (float)a.invvol;
   const bool need_h = done || mode != 0;
-  const bool need_y = mode == 2, need_r0 = REF && (mode != 0);
   for (int line = blockIdx.x * LPB + g; line < lines; line += gridDim.x * LPB) {
     const int iy = line % a.ny, iz = line / a.ny;
     const size_t base = (size_t)line * NX;
-    // per-point arrays of the line, in flight during the inverse x-DFT
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const float *src[kArr] = {a.t + (size_t)v * n + base, a.U + (size_t)v * n + base,
-                                a.Y + (size_t)v * n + base, a.Y + (size_t)(V + v) * n + base,
-                                REF ? a.R0 + (size_t)v * n + base : nullptr};
-      prefetch_line<E>(pre + (size_t)v * kArr * NX, src, 2, t);
-      if (need_y) prefetch_line<E>(pre + (size_t)v * kArr * NX + 2 * NX, src + 2, 2, t);
-      if (need_r0) prefetch_line<E>(pre + (size_t)v * kArr * NX + 4 * NX, src + 4, 1, t);
-    }
-    cp_async_commit();
     const float2 twyz = cmul(tw[NX + iy], tw[NX + a.ny + iz]);
     const int dyz = (iy + iz) & 1;
-    float2 z[E];
-    if (need_h) {
-#pragma unroll
-      for (int j = 0; j < E; ++j) z[j] = a.buf[base + t + E * j];
-      xfft::line_dft<E, true>(z, t, zs, a.xroots, mask);   // z[k] at ix = t + E k
-    }
-    __syncwarp(mask);                       // the transpose's reads are done
-    if (need_h)
-#pragma unroll
-      for (int k = 0; k < E; ++k) zs[k * E + t] = z[k];
-    cp_async_wait_all();
-    __syncwarp(mask);                       // every lane's copies have landed
-    // per point: one copy of the body (the refinement closure inlined for
-    // every point of an unrolled loop only grew the code)
 #pragma unroll 1
-    for (int k = 0; k < E; ++k) {
-      const int ix = t + E * k;
-      const size_t j = base + ix;
-      const float dir = ((ix & 1) ^ dyz) ? -1.0f : 1.0f;
-      const float2 dkf = cmul(tw[ix], twyz);
-      float h[2] = {0.0f, 0.0f};
+    for (int p = 0; p < P; ++p) {
+      float2 z[E];
+      float2 *zs = scr[g];                    // the line, point ix = t + E k at zs[k E + t]
       if (need_h) {
-        // inverse post-twiddle (timekb, fft3d.cu:52-60): (1/V) dir conj(dkf)
-        const float sc = iv * dir;
-        const float2 zz = cmul(zs[k * E + t], make_float2(dkf.x * sc, -dkf.y * sc));
-        h[0] = zz.x;
-        h[1] = zz.y;
-      }
-      float cv[2] = {0.0f, 0.0f};
 #pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const size_t i2 = (size_t)v * n + j;
-        const float *pv = pre + (size_t)v * kArr * NX + ix;
-        const float tv = pv[0], Uv = pv[NX];
-        if (done) {                           // pass_a_final, fused form
-          if (!REF && a.hout) {
-            a.hout[i2] = (double)h[v];
-            a.gout[i2] = (double)closure<CLOS>(tv - Uv);
+        for (int j = 0; j < E; ++j) z[j] = a.buf[(size_t)p * n + base + t + E * j];
+        xfft::line_dft<E, true>(z, t, scr[g], a.xroots, mask);   // z[k] at ix = t + E k
+      }
+      __syncwarp(mask);                       // the transpose's reads are done
+      if (need_h)
+#pragma unroll
+        for (int k = 0; k < E; ++k) zs[k * E + t] = z[k];
+      // per point: one copy of the body (the refinement closure inlined for
+      // every point of an unrolled loop overflowed the instruction cache)
+#pragma unroll 1
+      for (int k = 0; k < E; ++k) {
+        const int ix = t + E * k;
+        const size_t j = base + ix;
+        const float dir = ((ix & 1) ^ dyz) ? -1.0f : 1.0f;
+        const float2 dkf = cmul(tw[ix], twyz);
+        float h[2] = {0.0f, 0.0f};
+        if (need_h) {
+          // inverse post-twiddle (timekb, fft3d.cu:52-60): (1/V) dir conj(dkf)
+          const float sc = iv * dir;
+          const float2 zz = cmul(zs[k * E + t], make_float2(dkf.x * sc, -dkf.y * sc));
+          h[0] = zz.x;
+          h[1] = zz.y;
+        }
+        float cv[2] = {0.0f, 0.0f};
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int v = 2 * p + q;
+          if (v >= V) break;
+          const size_t i2 = (size_t)v * n + j;
+          const float tv = a.t[i2], Uv = a.U[i2];
+          if (done) {                           // pass_a_final, fused form
+            if (!REF && a.hout) {
+              a.hout[i2] = (double)h[q];
+              a.gout[i2] = (double)closure<CLOS>(tv - Uv);
+            }
+            if (done == 3 && mode != 0) {
+              const float r0 = REF ? a.R0[i2] : 0.0f;
+              const float R = residual<CLOS, REF>(h[q], tv, Uv, r0);
+              const float y = tv + m * R;
+              float tn = tv + R;
+              if (mode == 2) tn = y + s1 * (a.Y[i2] - y) + s2 * (a.Y[(size_t)V * n + i2] - y);
+              a.Y[(size_t)slot * V * n + i2] = y;
+              a.RP[(size_t)slot * V * n + i2] = R;
+              a.t[i2] = tn;
+            }
+            continue;
           }
-          if (done == 3 && mode != 0) {
-            const float r0 = REF ? pv[4 * NX] : 0.0f;
-            const float R = residual<CLOS, REF>(h[v], tv, Uv, r0);
+          float tn = tv;
+          if (mode != 0) {
+            const float r0 = REF ? a.R0[i2] : 0.0f;
+            const float R = residual<CLOS, REF>(h[q], tv, Uv, r0);   // tr
             const float y = tv + m * R;
-            float tn = tv + R;
-            if (mode == 2) tn = y + s1 * (pv[2 * NX] - y) + s2 * (pv[3 * NX] - y);
+            if (mode == 1) tn = tv + R;                              // newdt0 (Picard)
+            else tn = y + s1 * (a.Y[i2] - y) + s2 * (a.Y[(size_t)V * n + i2] - y);  // newdt (AN2)
             a.Y[(size_t)slot * V * n + i2] = y;
             a.RP[(size_t)slot * V * n + i2] = R;
             a.t[i2] = tn;
           }
-          continue;
+          cv[q] = cfun<CLOS, REF>(tn, Uv);
         }
-        float tn = tv;
-        if (mode != 0) {
-          const float r0 = REF ? pv[4 * NX] : 0.0f;
-          const float R = residual<CLOS, REF>(h[v], tv, Uv, r0);   // tr
-          const float y = tv + m * R;
-          if (mode == 1) tn = tv + R;                              // newdt0 (Picard)
-          else tn = y + s1 * (pv[2 * NX] - y) + s2 * (pv[3 * NX] - y);  // newdt (AN2)
-          a.Y[(size_t)slot * V * n + i2] = y;
-          a.RP[(size_t)slot * V * n + i2] = R;
-          a.t[i2] = tn;
-        }
-        cv[v] = cfun<CLOS, REF>(tn, Uv);
+        // forward pre-twiddle (timekf, fft3d.cu:41-49): dir dkf (c_a + i c_b)
+        zs[k * E + t] = cmul(make_float2(cv[0], cv[1]), make_float2(dkf.x * dir, dkf.y * dir));
       }
-      // forward pre-twiddle (timekf, fft3d.cu:41-49): dir dkf (c_a + i c_b)
-      zs[k * E + t] = cmul(make_float2(cv[0], cv[1]), make_float2(dkf.x * dir, dkf.y * dir));
+#pragma unroll
+      for (int k = 0; k < E; ++k) z[k] = zs[k * E + t];
+      if (done) continue;
+      xfft::line_dft<E, false>(z, t, scr[g], a.xroots, mask);    // z[k] at kx = t + E k
+#pragma unroll
+      for (int k = 0; k < E; ++k) a.buf[(size_t)p * n + base + t + E * k] = z[k];
     }
-    if (done) { __syncwarp(mask); continue; }
-#pragma unroll
-    for (int k = 0; k < E; ++k) z[k] = zs[k * E + t];
-    xfft::line_dft<E, false>(z, t, zs, a.xroots, mask);    // z[k] at kx = t + E k
-#pragma unroll
-    for (int k = 0; k < E; ++k) a.buf[base + t + E * k] = z[k];
-    __syncwarp(mask);                       // the next line reuses zs and pre
   }
 }
 
 template <int V, int CLOS, bool REF, int E>
-__global__ void __launch_bounds__(kXThreads) k_pass_rx(IterArgs<float> a) {
-  static_assert(V <= 2, "one packed site pair");
-  using L = XLayout<V, E>;
-  constexpr int NX = L::NX, LPB = L::LPB;
-  extern __shared__ float4 xsm4[];
-  float2 *scr_all = reinterpret_cast<float2 *>(xsm4);
-  float *pre_all = reinterpret_cast<float *>(scr_all + (size_t)LPB * L::SCR);
+__global__ void __launch_bounds__(kXThreads, 3) k_pass_rx(IterArgs<float> a) {
+  constexpr int NX = E * E, LPB = kXThreads / E, P = (V + 1) / 2;
+  __shared__ float2 scr[LPB][(E + 1) * E];
   __shared__ double red[kXThreads / 32][6];
   __shared__ bool last;
   DevState *st = a.st;
@@ -813,8 +760,6 @@ __global__ void __launch_bounds__(kXThreads) k_pass_rx(IterArgs<float> a) {
   const long long n = a.n;
   const int g = threadIdx.x / E, t = threadIdx.x % E;
   const unsigned mask = (E == 16) ? (0xffffu << (threadIdx.x & 16)) : (0xffu << (threadIdx.x & 24));
-  float2 *zs = scr_all + (size_t)g * L::SCR;
-  float *pre = pre_all + (size_t)g * V * kArr * NX;   // [v][t U RP0 RP1 R0][ix]
   const int lines = a.ny * a.nz;
   const float2 *tw = a.tw;
   const float iv = (float)a.invvol;
@@ -825,53 +770,47 @@ __global__ void __launch_bounds__(kXThreads) k_pass_rx(IterArgs<float> a) {
   for (int line = blockIdx.x * LPB + g; line < lines; line += gridDim.x * LPB) {
     const int iy = line % a.ny, iz = line / a.ny;
     const size_t base = (size_t)line * NX;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const float *src[kArr] = {a.t + (size_t)v * n + base, a.U + (size_t)v * n + base,
-                                a.RP + (size_t)v * n + base, a.RP + (size_t)(V + v) * n + base,
-                                REF ? a.R0 + (size_t)v * n + base : nullptr};
-      prefetch_line<E>(pre + (size_t)v * kArr * NX, src, 2, t);
-      if (gram) prefetch_line<E>(pre + (size_t)v * kArr * NX + 2 * NX, src + 2, 2, t);
-      if (REF) prefetch_line<E>(pre + (size_t)v * kArr * NX + 4 * NX, src + 4, 1, t);
-    }
-    cp_async_commit();
     const float2 twyz = cmul(tw[NX + iy], tw[NX + a.ny + iz]);
     const int dyz = (iy + iz) & 1;
-    float2 z[E];
+#pragma unroll 1
+    for (int p = 0; p < P; ++p) {
+      float2 z[E];
+      float2 *zs = scr[g];
 #pragma unroll
-    for (int j = 0; j < E; ++j) z[j] = a.buf[base + t + E * j];
-    xfft::line_dft<E, true>(z, t, zs, a.xroots, mask);
-    __syncwarp(mask);
+      for (int j = 0; j < E; ++j) z[j] = a.buf[(size_t)p * n + base + t + E * j];
+      xfft::line_dft<E, true>(z, t, scr[g], a.xroots, mask);
+      __syncwarp(mask);
 #pragma unroll
-    for (int k = 0; k < E; ++k) zs[k * E + t] = z[k];
-    cp_async_wait_all();
-    __syncwarp(mask);
+      for (int k = 0; k < E; ++k) zs[k * E + t] = z[k];
 #pragma unroll 2
-    for (int k = 0; k < E; ++k) {
-      const int ix = t + E * k;
-      const float dir = ((ix & 1) ^ dyz) ? -1.0f : 1.0f;
-      const float2 dkf = cmul(tw[ix], twyz);
-      const float sc = iv * dir;
-      const float2 zz = cmul(zs[k * E + t], make_float2(dkf.x * sc, -dkf.y * sc));
-      const float h[2] = {zz.x, zz.y};
+      for (int k = 0; k < E; ++k) {
+        const int ix = t + E * k;
+        const size_t j = base + ix;
+        const float dir = ((ix & 1) ^ dyz) ? -1.0f : 1.0f;
+        const float2 dkf = cmul(tw[ix], twyz);
+        const float sc = iv * dir;
+        const float2 zz = cmul(zs[k * E + t], make_float2(dkf.x * sc, -dkf.y * sc));
+        const float h[2] = {zz.x, zz.y};
 #pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const float *pv = pre + (size_t)v * kArr * NX + ix;
-        const float rb = REF ? pv[4 * NX] : 0.0f;
-        const double R = (double)residual<CLOS, REF>(h[v], pv[0], pv[NX], rb);
-        acc[0] += R * R;                          // cal_rms.cu:18
-        if (gram) {                               // theta30, anderson_cuda.cu:33-39
-          const double d0 = R - (double)pv[2 * NX];
-          const double d1 = R - (double)pv[3 * NX];
-          acc[1] += w8[v] * R * d0;
-          acc[2] += w8[v] * R * d1;
-          acc[3] += w8[v] * d0 * d0;
-          acc[4] += w8[v] * d0 * d1;
-          acc[5] += w8[v] * d1 * d1;
+        for (int q = 0; q < 2; ++q) {
+          const int v = 2 * p + q;
+          if (v >= V) break;
+          const size_t i2 = (size_t)v * n + j;
+          const float rb = REF ? a.R0[i2] : 0.0f;
+          const double R = (double)residual<CLOS, REF>(h[q], a.t[i2], a.U[i2], rb);
+          acc[0] += R * R;                          // cal_rms.cu:18
+          if (gram) {                               // theta30, anderson_cuda.cu:33-39
+            const double d0 = R - (double)a.RP[i2];
+            const double d1 = R - (double)a.RP[(size_t)V * n + i2];
+            acc[1] += w8[v] * R * d0;
+            acc[2] += w8[v] * R * d1;
+            acc[3] += w8[v] * d0 * d0;
+            acc[4] += w8[v] * d0 * d1;
+            acc[5] += w8[v] * d1 * d1;
+          }
         }
       }
     }
-    __syncwarp(mask);                             // the next line reuses zs and pre
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
@@ -1204,33 +1143,8 @@ int wave_blocks_smem(K kernel, int threads, size_t smem, long long need) {
 template <int V, int CLOS, bool REF, int E>
 int grid_ax(const Context &c) {
   const long long lines = (long long)c.ny * c.nz;
-  return wave_blocks_smem(k_pass_ax<V, CLOS, REF, E>, kXThreads, XLayout<V, E>::bytes(),
+  return wave_blocks_smem(k_pass_ax<V, CLOS, REF, E>, kXThreads, 0,
                           (lines * E + kXThreads - 1) / kXThreads);
-}
-
-// Dynamic shared-memory limits of the fused kernels of one line size.
-template <int V, int CLOS, int E>
-cudaError_t fused_attrs_vc() {
-  const int b = (int)XLayout<V, E>::bytes();
-  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(k_pass_ax<V, CLOS, false, E>, at, b);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_ax<V, CLOS, true, E>, at, b);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_rx<V, CLOS, false, E>, at, b);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_rx<V, CLOS, true, E>, at, b);
-  return e;
-}
-
-template <int E>
-cudaError_t fused_attrs() {
-  const int ks = (int)KYLayout<E>::bytes();
-  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(k_kspace_y<1, E>, at, ks);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_kspace_y<2, E>, at, ks);
-  if (e == cudaSuccess) e = fused_attrs_vc<1, 0, E>();
-  if (e == cudaSuccess) e = fused_attrs_vc<1, 1, E>();
-  if (e == cudaSuccess) e = fused_attrs_vc<2, 0, E>();
-  if (e == cudaSuccess) e = fused_attrs_vc<2, 1, E>();
-  return e;
 }
 
 template <int V, int E>
@@ -1243,12 +1157,11 @@ int grid_ky(const Context &c) {
 // passes (single solute, V <= 2, nx = ny = E^2): cuFFT transforms along z.
 template <int V, int CLOS, bool REF, int E>
 void launch_iteration_x(Context &c, const IterArgs<float> &a) {
-  k_pass_ax<V, CLOS, REF, E><<<grid_ax<V, CLOS, REF, E>(c), kXThreads, XLayout<V, E>::bytes(),
-                               c.stream>>>(a);
+  k_pass_ax<V, CLOS, REF, E><<<grid_ax<V, CLOS, REF, E>(c), kXThreads, 0, c.stream>>>(a);
   cufftExecC2C(c.plan32z, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_FORWARD);
   k_kspace_y<V, E><<<grid_ky<V, E>(c), kW * E, KYLayout<E>::bytes(), c.stream>>>(a);
   cufftExecC2C(c.plan32z, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
-  k_pass_rx<V, CLOS, REF, E><<<a.nblocks, kXThreads, XLayout<V, E>::bytes(), c.stream>>>(a);
+  k_pass_rx<V, CLOS, REF, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a);
 }
 
 template <typename T, int V, int CLOS, bool REF>
@@ -1730,16 +1643,14 @@ template <int V, int CLOS, int E>
 void time_fused(Context &c, const IterArgs<float> &a, int which, int reps) {
   for (int r = 0; r < reps; ++r) {
     switch (which) {
-      case 10: k_pass_ax<V, CLOS, false, E><<<grid_ax<V, CLOS, false, E>(c), kXThreads,
-                                                XLayout<V, E>::bytes(), c.stream>>>(a); break;
-      case 13: k_pass_ax<V, CLOS, true, E><<<grid_ax<V, CLOS, true, E>(c), kXThreads,
-                                               XLayout<V, E>::bytes(), c.stream>>>(a); break;
+      case 10: k_pass_ax<V, CLOS, false, E><<<grid_ax<V, CLOS, false, E>(c), kXThreads, 0,
+                                                c.stream>>>(a); break;
+      case 13: k_pass_ax<V, CLOS, true, E><<<grid_ax<V, CLOS, true, E>(c), kXThreads, 0,
+                                               c.stream>>>(a); break;
       case 11: k_kspace_y<V, E><<<grid_ky<V, E>(c), kW * E, KYLayout<E>::bytes(),
                                   c.stream>>>(a); break;
-      case 15: k_pass_rx<V, CLOS, true, E><<<a.nblocks, kXThreads, XLayout<V, E>::bytes(),
-                                              c.stream>>>(a); break;
-      default: k_pass_rx<V, CLOS, false, E><<<a.nblocks, kXThreads, XLayout<V, E>::bytes(),
-                                               c.stream>>>(a); break;
+      case 15: k_pass_rx<V, CLOS, true, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a); break;
+      default: k_pass_rx<V, CLOS, false, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a); break;
     }
   }
 }
@@ -1841,7 +1752,18 @@ int setup_fused_axes(Context &c) {
   if (c.prm.precision != RISM3D_MIXED || c.nb != 1 || c.natv < 1 || c.natv > 2 ||
       c.nx != c.ny || (c.nx != 256 && c.nx != 64) || c.nz % 2 != 0)
     return RISM3D_OK;
-  const cudaError_t e = c.nx == 256 ? fused_attrs<16>() : fused_attrs<8>();
+  cudaError_t e = cudaSuccess;
+  if (c.nx == 256) {
+    const int ks = (int)KYLayout<16>::bytes();
+    e = cudaFuncSetAttribute(k_kspace_y<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ks);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_kspace_y<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ks);
+  } else {
+    const int ks = (int)KYLayout<8>::bytes();
+    e = cudaFuncSetAttribute(k_kspace_y<1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ks);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_kspace_y<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ks);
+  }
   if (!cuda_ok(c, e, "fused-axis kernel attributes")) return RISM3D_CUDA_ERROR;
   std::vector<float2> roots(c.nx);
   for (int m = 0; m < c.nx; ++m) {
