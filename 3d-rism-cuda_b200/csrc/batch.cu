@@ -9,8 +9,10 @@
 // from its own host thread, so a sub-batch that has converged stops paying
 // for the transforms of the others.
 #include <algorithm>
+#include <chrono>
 #include <cstdlib>
 #include <map>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -22,33 +24,19 @@ struct rism3d_ctx {
   Context c;
 };
 
-extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, const int *grids,
-                                  const double *boxes, const double *sig, const double *eps,
-                                  const double *q, const double *xyz, rism3d_result *results) {
-  if (!x) return RISM3D_BAD_INPUT;
-  Context &p = x->c;
-  cudaSetDevice(p.dev);
-  if (!p.have_solvent) { p.err = "set the solvent first"; return RISM3D_BAD_STATE; }
-  if (nmol < 1 || !natoms || !grids || !boxes || !sig || !eps || !q || !xyz || !results) {
-    p.err = "bad batch arguments";
-    return RISM3D_BAD_INPUT;
-  }
-  std::vector<long long> off(nmol + 1, 0);
-  for (int m = 0; m < nmol; ++m) {
-    if (natoms[m] < 1 || grids[m] < 4 || !(boxes[m] > 0)) {
-      p.err = "bad batch entry " + std::to_string(m);
-      return RISM3D_BAD_INPUT;
-    }
-    off[m + 1] = off[m] + natoms[m];
-  }
+namespace {
+
+// One batched solve with sub-batches of about kChunkPoints grid points.
+int solve_batch_chunked(Context &p, int nmol, const int *natoms, const int *grids,
+                        const double *boxes, const double *sig, const double *eps,
+                        const double *q, const double *xyz, rism3d_result *results,
+                        const std::vector<long long> &off, long long kChunkPoints) {
   // group by cell; a group larger than kChunkPoints grid points in all is
   // split into sub-batches that converge and finish on their own (a batch
   // moves in lock-step: its transforms run for every solute until the last
   // one converges) and run concurrently, each on its own stream.  For 256
   // solutes on 48^3 / 64^3 / 96^3 cells: one batch per cell 67 solves/s,
   // sub-batches of 2^25 / 2^22 / 2^20 / 2^18 points 72 / 79 / 86 / 84.
-  const long long kChunkPoints = p.prm.batch_chunk_points > 0 ? p.prm.batch_chunk_points
-                                                               : (1LL << 20);
   std::map<std::pair<int, double>, std::vector<int>> cells;
   for (int m = 0; m < nmol; ++m) cells[{grids[m], boxes[m]}].push_back(m);
   std::map<std::pair<std::pair<int, double>, int>, std::vector<int>> groups;
@@ -62,51 +50,24 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
   // one child context per group, each on its own stream
   const long long call = ++p.batch_calls;
   std::vector<std::pair<Context *, const std::vector<int> *>> work;
+  // 1. cached children with the shapes of this call's groups
   for (auto &kv : groups) {
     const int grid = kv.first.first.first;
     const double box = kv.first.first.second;
     const int nb = (int)kv.second.size();
     Context *ch = nullptr;                 // a cached child not yet taken by this call
     for (Context::Child &cc : p.children)
-      if (!ch && cc.grid == grid && cc.box == box && cc.nb == nb) {
-        bool taken = false;
-        for (const auto &wk : work) taken = taken || wk.first == cc.ctx;
-        if (!taken) { ch = cc.ctx; cc.last_call = call; }
+      if (!ch && cc.grid == grid && cc.box == box && cc.nb == nb && cc.last_call != call) {
+        ch = cc.ctx;
+        cc.last_call = call;
       }
-    if (!ch) {
-      size_t free0 = 0, free1 = 0, total = 0;
-      cudaMemGetInfo(&free0, &total);
-      rism3d_params cp = p.prm;
-      cp.grid[0] = cp.grid[1] = cp.grid[2] = grid;
-      cp.box[0] = cp.box[1] = cp.box[2] = box;
-      cp.stream = nullptr;           // its own stream: groups run concurrently
-      cp.verbose = 0;
-      ch = new Context;
-      std::string err;
-      int rc = context_init(*ch, &cp, nb, err);
-      if (rc == RISM3D_OK)
-        rc = context_set_solvent(*ch, p.natv, p.rho, p.qv, p.sigv, p.epsv, p.temper, p.xt,
-                                 p.ntab, p.xdr, p.xvv_host.data());
-      if (rc != RISM3D_OK) {
-        p.err = err.empty() ? ch->err : err;
-        context_release(*ch);
-        delete ch;
-        return rc;
-      }
-      cudaMemGetInfo(&free1, &total);
-      Context::Child cc;
-      cc.grid = grid; cc.nb = nb; cc.box = box; cc.ctx = ch;
-      cc.last_call = call;
-      cc.bytes = free0 > free1 ? free0 - free1 : 0;
-      p.children.push_back(cc);
-    }
     work.push_back({ch, &kv.second});
   }
-  // Children not used by this call stay cached for later calls with the
+  // 2. Children not used by this call stay cached for later calls with the
   // same shapes, up to a byte budget (RISM3D_BATCH_CACHE_BYTES, default
-  // 4 GiB); beyond it the least recently used ones are freed, so callers
-  // whose batch composition changes from call to call do not accumulate
-  // one context per composition.
+  // 4 GiB); beyond it the least recently used ones are freed -- before
+  // this call allocates its new ones -- so callers whose batch composition
+  // changes from call to call do not accumulate one context per composition.
   {
     size_t budget = 4ull << 30;
     if (const char *e = getenv("RISM3D_BATCH_CACHE_BYTES")) budget = (size_t)strtoull(e, nullptr, 10);
@@ -124,6 +85,40 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
       delete p.children[lru].ctx;
       p.children.erase(p.children.begin() + lru);
     }
+  }
+  // 3. new children for the groups without one
+  for (auto &wk : work) {
+    if (wk.first) continue;
+    const int m0 = (*wk.second)[0];
+    const int grid = grids[m0];
+    const double box = boxes[m0];
+    const int nb = (int)wk.second->size();
+    size_t free0 = 0, free1 = 0, total = 0;
+    cudaMemGetInfo(&free0, &total);
+    rism3d_params cp = p.prm;
+    cp.grid[0] = cp.grid[1] = cp.grid[2] = grid;
+    cp.box[0] = cp.box[1] = cp.box[2] = box;
+    cp.stream = nullptr;           // its own stream: groups run concurrently
+    cp.verbose = 0;
+    Context *ch = new Context;
+    std::string err;
+    int rc = context_init(*ch, &cp, nb, err);
+    if (rc == RISM3D_OK)
+      rc = context_set_solvent(*ch, p.natv, p.rho, p.qv, p.sigv, p.epsv, p.temper, p.xt,
+                               p.ntab, p.xdr, p.xvv_host.data());
+    if (rc != RISM3D_OK) {
+      p.err = err.empty() ? ch->err : err;
+      context_release(*ch);
+      delete ch;
+      return rc;
+    }
+    cudaMemGetInfo(&free1, &total);
+    Context::Child cc;
+    cc.grid = grid; cc.nb = nb; cc.box = box; cc.ctx = ch;
+    cc.last_call = call;
+    cc.bytes = free0 > free1 ? free0 - free1 : 0;
+    p.children.push_back(cc);
+    wk.first = ch;
   }
   // work queued on the caller's stream before this call comes first
   cudaEvent_t start = nullptr;
@@ -201,4 +196,65 @@ extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, co
     ch->launches = 0;
   }
   return worst;
+}
+
+}  // namespace
+
+extern "C" int rism3d_solve_batch(rism3d_ctx *x, int nmol, const int *natoms, const int *grids,
+                                  const double *boxes, const double *sig, const double *eps,
+                                  const double *q, const double *xyz, rism3d_result *results) {
+  if (!x) return RISM3D_BAD_INPUT;
+  Context &p = x->c;
+  cudaSetDevice(p.dev);
+  if (!p.have_solvent) { p.err = "set the solvent first"; return RISM3D_BAD_STATE; }
+  if (nmol < 1 || !natoms || !grids || !boxes || !sig || !eps || !q || !xyz || !results) {
+    p.err = "bad batch arguments";
+    return RISM3D_BAD_INPUT;
+  }
+  std::vector<long long> off(nmol + 1, 0);
+  for (int m = 0; m < nmol; ++m) {
+    if (natoms[m] < 1 || grids[m] < 4 || !(boxes[m] > 0)) {
+      p.err = "bad batch entry " + std::to_string(m);
+      return RISM3D_BAD_INPUT;
+    }
+    off[m + 1] = off[m] + natoms[m];
+  }
+  if (p.prm.batch_chunk_points > 0)
+    return solve_batch_chunked(p, nmol, natoms, grids, boxes, sig, eps, q, xyz, results, off,
+                               p.prm.batch_chunk_points);
+  // Autotuned sub-batch size: the first call whose batch holds a given set
+  // of cells runs the whole batch once per candidate size (wall time from
+  // the call to the end of its last group), keeps the fastest for that set
+  // and returns the last run's results (the sub-batch size does not change
+  // any solute's equations, only which solutes share a launch).  Later calls
+  // with the same set of cells use the cached size.
+  std::string key;
+  {
+    std::map<std::pair<int, double>, int> cells;
+    for (int m = 0; m < nmol; ++m) cells[{grids[m], boxes[m]}] += 1;
+    for (auto &kv : cells)
+      key += std::to_string(kv.first.first) + "/" + std::to_string(kv.first.second) + ";";
+  }
+  auto it = p.batch_tuned.find(key);
+  if (it != p.batch_tuned.end())
+    return solve_batch_chunked(p, nmol, natoms, grids, boxes, sig, eps, q, xyz, results, off,
+                               it->second);
+  static const long long kCandidates[] = {1LL << 18, 1LL << 19, 1LL << 20, 1LL << 21, 1LL << 22};
+  long long best = 1LL << 20;
+  double best_ms = 1e300;
+  int rc = RISM3D_OK;
+  for (long long cand : kCandidates) {
+    if (!cuda_ok(p, cudaStreamSynchronize(p.stream), "batch tuning")) return RISM3D_CUDA_ERROR;
+    const auto t0 = std::chrono::steady_clock::now();
+    rc = solve_batch_chunked(p, nmol, natoms, grids, boxes, sig, eps, q, xyz, results, off, cand);
+    if (rc == RISM3D_CUDA_ERROR || rc == RISM3D_CUFFT_ERROR || rc == RISM3D_BAD_INPUT ||
+        rc == RISM3D_UNSUPPORTED_SHAPE || rc == RISM3D_BAD_STATE)
+      return rc;
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (ms < best_ms) { best_ms = ms; best = cand; }
+  }
+  p.batch_tuned[key] = best;
+  if (best != kCandidates[sizeof(kCandidates) / sizeof(kCandidates[0]) - 1])
+    rc = solve_batch_chunked(p, nmol, natoms, grids, boxes, sig, eps, q, xyz, results, off, best);
+  return rc;
 }

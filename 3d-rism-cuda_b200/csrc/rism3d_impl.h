@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -244,6 +245,8 @@ struct Context {
   };
   std::vector<Child> children;
   long long batch_calls = 0;
+  // autotuned sub-batch size (grid points) per set of cells in a batch
+  std::map<std::string, long long> batch_tuned;
 };
 
 // ---- kernels/launchers (implemented in the .cu files) ----

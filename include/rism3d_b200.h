@@ -75,7 +75,10 @@ typedef struct {
   long long batch_chunk_points; /* rism3d_solve_batch: solutes of one cell run
                              in sub-batches of about this many grid points in
                              all, which converge, finish and overlap on their
-                             own (0 = 2^20) */
+                             own.  0 = autotuned: the first batch with a given
+                             set of cells is solved once per candidate size
+                             (2^18 .. 2^22 points) and the fastest is kept for
+                             later batches with that set */
 } rism3d_params;
 
 typedef struct {
