@@ -198,6 +198,10 @@ static int alloc_state(Context &c) {
     const int rc = setup_fused_axes(c);
     if (rc != RISM3D_OK) return rc;
   }
+  {
+    const int rc = setup_pipe_r(c);
+    if (rc != RISM3D_OK) return rc;
+  }
   c.plans_ok = true;
   return RISM3D_OK;
 }

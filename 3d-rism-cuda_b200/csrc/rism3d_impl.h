@@ -196,6 +196,7 @@ struct Context {
   // FP32 passes with the x and y axes of the transforms folded in (single
   // solutes, natv <= 2, nx = ny = 64 or 256): cuFFT then transforms along z
   // only (plan32z), with the x-line roots of unity in d_xroots
+  bool pipe_r = false;       // pass R as the cp.async pipeline (natv <= 2)
   bool xfused = false;
   cufftHandle plan32z = 0;
   float2 *d_xroots = nullptr;
@@ -256,6 +257,7 @@ int launch_potential_r(Context &c);               // potential.cu (timing hook)
 int upload_chi(Context &c);                       // solver.cu
 // decide on and set up the fused-axis FP32 passes (plan, roots, limits)
 int setup_fused_axes(Context &c);                 // solver.cu
+int setup_pipe_r(Context &c);                     // solver.cu: pipelined pass R
 // spline.cc:4-43: natural cubic spline through (xp[k], yp[k]), k < np; writes
 // {y_k, b_k, c_k, d_k} (y + b t + c t^2 + d t^3 on interval k; zero
 // coefficients on the last knot) to out[k * stride + 0..3]

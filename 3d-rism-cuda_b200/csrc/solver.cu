@@ -927,6 +927,157 @@ __global__ void __launch_bounds__(kW * E, 2) k_kspace_y(IterArgs<float> a) {
 
 
 
+// Pass R as a software pipeline (V <= 2, one packed site pair): a block
+// walks chunks of kThreads * PTS consecutive points (PTS = 16 bytes of T),
+// and each thread copies its own 16-byte slice of every input of the NEXT
+// chunk into its private shared-memory slots with cp.async while it works
+// on the current one, two stages deep.  A thread reads back only what it
+// copied, so no block barrier is needed; the loads in flight per SM are
+// those of a whole chunk per resident block (the plain pass R holds only
+// what its registers can).
+constexpr int kPipeStages = 2;
+
+__device__ __forceinline__ void cp16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// slots of one thread in one stage (16-byte units): buf (2: PTS complex
+// points), t[V], U[V], RP0[V], RP1[V], R0[V]
+template <int V> struct PipeSlots {
+  static constexpr int BUF = 0, T = 2, U = 2 + V, RP0 = 2 + 2 * V, RP1 = 2 + 3 * V,
+                       R0 = 2 + 4 * V, N = 2 + 5 * V;
+};
+
+template <typename T, int V>
+constexpr size_t pass_r_pipe_smem() {
+  return (size_t)16 * PipeSlots<V>::N * kPipeStages * kThreads;
+}
+
+template <typename T, int V, int CLOS, bool REF>
+__global__ void __launch_bounds__(kThreads) k_pass_r_pipe(IterArgs<T> a0) {
+  static_assert(V <= 2, "one packed site pair");
+  const IterArgs<T> a = solute_view<T, V>(a0);
+  typedef typename Cx<T>::t C;
+  constexpr int PTS = 16 / sizeof(T);            // points per 16-byte slice
+  constexpr int CP = kThreads * PTS;             // points per chunk
+  using S = PipeSlots<V>;
+  extern __shared__ float4 pipe_sm[];
+  __shared__ double red[kThreads / 32][6];
+  __shared__ bool last;
+  DevState *st = a.st;
+  if (st->done) {                                // loop stopped: count idle cycles
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->after_done += 1;
+    return;
+  }
+  const bool gram = st->count <= 0;
+  const long long n = a.n;
+  const StageParams *sp = a.sp;
+  const C *tw = a.tw;
+  double w8[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) w8[v] = sp->irho[v];
+  // this thread's slots: [stage][slot], 16 bytes each, interleaved by thread
+  auto slot = [&](int stage, int k) -> float4 * {
+    return pipe_sm + ((size_t)(stage * S::N + k) * kThreads + threadIdx.x);
+  };
+  const long long nchunks = (n + CP - 1) / CP;
+  auto issue = [&](long long c, int stage) {
+    const long long j = c * CP + (long long)threadIdx.x * PTS;
+    if (c < nchunks && j < n) {
+      cp16(slot(stage, S::BUF), a.buf + j);
+      cp16(slot(stage, S::BUF + 1), a.buf + j + PTS / 2);
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        cp16(slot(stage, S::T + v), a.t + (size_t)v * n + j);
+        cp16(slot(stage, S::U + v), a.U + (size_t)v * n + j);
+        if (gram) {
+          cp16(slot(stage, S::RP0 + v), a.RP + (size_t)v * n + j);
+          cp16(slot(stage, S::RP1 + v), a.RP + (size_t)(V + v) * n + j);
+        }
+        if (REF) cp16(slot(stage, S::R0 + v), a.R0 + (size_t)v * n + j);
+      }
+    }
+    cp_commit();                                 // an empty group keeps the count
+  };
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  long long c = blockIdx.x;
+  issue(c, 0);
+  for (int stage = 0; c < nchunks; c += gridDim.x, stage ^= 1) {
+    issue(c + gridDim.x, stage ^ 1);             // the next chunk, in flight meanwhile
+    cp_wait<1>();                                // this chunk's slices have landed
+    const long long j = c * CP + (long long)threadIdx.x * PTS;
+    if (j >= n) continue;
+    // PTS complex points over two 16-byte slots (PTS / 2 in each)
+    const T *bz0 = reinterpret_cast<const T *>(slot(stage, S::BUF));
+    const T *bz1 = reinterpret_cast<const T *>(slot(stage, S::BUF + 1));
+    int ix, iy, iz, dir0;
+    C dkf[PTS];
+    point_phase(j, a.fdx, a.fdy, tw, ix, iy, iz, dir0, dkf[0]);
+    {
+      const C tyz = cmul(tw[a.nx + iy], tw[a.nx + a.ny + iz]);
+#pragma unroll
+      for (int k = 1; k < PTS; ++k) dkf[k] = cmul(tw[ix + k], tyz);
+    }
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) {
+      const int dir = (k & 1) ? -dir0 : dir0;
+      const T sc = (T)a.invvol * (T)dir;
+      const C w = mk<C>(dkf[k].x * sc, -dkf[k].y * sc);
+      const T *bz = k < PTS / 2 ? bz0 + 2 * k : bz1 + 2 * (k - PTS / 2);
+      C zz;
+      zz.x = bz[0];
+      zz.y = bz[1];
+      const C z = cmul(zz, w);
+      const T h[2] = {z.x, z.y};
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const T tv = reinterpret_cast<const T *>(slot(stage, S::T + v))[k];
+        const T Uv = reinterpret_cast<const T *>(slot(stage, S::U + v))[k];
+        const T rb = REF ? reinterpret_cast<const T *>(slot(stage, S::R0 + v))[k] : T(0);
+        const double R = (double)residual<CLOS, REF>(h[v], tv, Uv, rb);
+        acc[0] += R * R;                          // cal_rms.cu:18
+        if (gram) {                               // theta30, anderson_cuda.cu:33-39
+          const double d0 = R - (double)reinterpret_cast<const T *>(slot(stage, S::RP0 + v))[k];
+          const double d1 = R - (double)reinterpret_cast<const T *>(slot(stage, S::RP1 + v))[k];
+          acc[1] += w8[v] * R * d0;
+          acc[2] += w8[v] * R * d1;
+          acc[3] += w8[v] * d0 * d0;
+          acc[4] += w8[v] * d0 * d1;
+          acc[5] += w8[v] * d1 * d1;
+        }
+      }
+    }
+  }
+  cp_wait<0>();
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[k] = v;
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k) red[wid][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) s += red[w][threadIdx.x];
+    a.part[(size_t)threadIdx.x * a.nblocks + blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(a.count, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_block(st, a.part, a.nblocks, (double)n * V, a.hist, a.hist_cap);
+  if (threadIdx.x == 0) *a.count = 0u;
+}
+
 // ------------------------------------------------------------- finalize
 // Run by the last block of pass R to finish: fixed-order reduction of the
 // block sums, then the host logic of iterate.cu:52-62 and AN2::calculate
@@ -1164,6 +1315,15 @@ void launch_iteration_x(Context &c, const IterArgs<float> &a) {
   k_pass_rx<V, CLOS, REF, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a);
 }
 
+// Blocks of the pipelined pass R: one full wave (it walks the grid), at most
+// the partial-sum slots the context has.
+template <typename T, int V, int CLOS, bool REF>
+int pipe_r_blocks(const Context &c) {
+  const int w = wave_blocks_smem(k_pass_r_pipe<T, V, CLOS, REF>, kThreads,
+                                 pass_r_pipe_smem<T, V>(), c.nred_blocks);
+  return std::min(w, c.nred_blocks);
+}
+
 template <typename T, int V, int CLOS, bool REF>
 void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   if constexpr (sizeof(T) == 4 && V <= 2) {
@@ -1187,6 +1347,16 @@ void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
     cufftExecZ2Z(plan, (cufftDoubleComplex *)a.buf, (cufftDoubleComplex *)a.buf, CUFFT_INVERSE);
   } else {
     cufftExecC2C(plan, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
+  }
+  if constexpr (V <= 2) {
+    if (c.pipe_r) {
+      IterArgs<T> ar = a;
+      ar.nblocks = pipe_r_blocks<T, V, CLOS, REF>(c);
+      k_pass_r_pipe<T, V, CLOS, REF><<<dim3(ar.nblocks, c.nb), kThreads, pass_r_pipe_smem<T, V>(),
+                                       c.stream>>>(ar);
+      (void)sizeof(C);
+      return;
+    }
   }
   k_pass_r<T, V, CLOS, REF><<<br, kThreads, 0, c.stream>>>(a);
   (void)sizeof(C);
@@ -1709,8 +1879,30 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
       case 0: case 10: k_pass_a<T, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a); break;
       case 13: k_pass_a<T, V, CLOS, true><<<bar, kThreads, 0, c.stream>>>(a); break;
       case 1: case 11: k_kspace<T, V><<<bk, kThreads, 0, c.stream>>>(a); break;
-      case 15: k_pass_r<T, V, CLOS, true><<<a.nblocks, kThreads, 0, c.stream>>>(a); break;
-      default: k_pass_r<T, V, CLOS, false><<<a.nblocks, kThreads, 0, c.stream>>>(a); break;
+      case 15:
+        if constexpr (V <= 2) {
+          if (c.pipe_r) {
+            IterArgs<T> ar = a;
+            ar.nblocks = pipe_r_blocks<T, V, CLOS, true>(c);
+            k_pass_r_pipe<T, V, CLOS, true><<<ar.nblocks, kThreads, pass_r_pipe_smem<T, V>(),
+                                              c.stream>>>(ar);
+            break;
+          }
+        }
+        k_pass_r<T, V, CLOS, true><<<a.nblocks, kThreads, 0, c.stream>>>(a);
+        break;
+      default:
+        if constexpr (V <= 2) {
+          if (c.pipe_r) {
+            IterArgs<T> ar = a;
+            ar.nblocks = pipe_r_blocks<T, V, CLOS, false>(c);
+            k_pass_r_pipe<T, V, CLOS, false><<<ar.nblocks, kThreads, pass_r_pipe_smem<T, V>(),
+                                               c.stream>>>(ar);
+            break;
+          }
+        }
+        k_pass_r<T, V, CLOS, false><<<a.nblocks, kThreads, 0, c.stream>>>(a);
+        break;
     }
   }
   cudaEventRecord(e1, c.stream);
@@ -1743,6 +1935,28 @@ int solve_c(Context &c, int cu) {
 }
 
 }  // namespace
+
+template <typename T, int V>
+cudaError_t pipe_r_attrs() {
+  const int b = (int)pass_r_pipe_smem<T, V>();
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(k_pass_r_pipe<T, V, 0, false>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_r_pipe<T, V, 1, false>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_r_pipe<T, V, 0, true>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_r_pipe<T, V, 1, true>, at, b);
+  return e;
+}
+
+int setup_pipe_r(Context &c) {
+  c.pipe_r = false;
+  const char *off = getenv("RISM3D_NO_PIPE_R");
+  if ((off && off[0] == '1') || c.natv > 2) return RISM3D_OK;
+  cudaError_t e = c.natv == 1 ? pipe_r_attrs<double, 1>() : pipe_r_attrs<double, 2>();
+  if (e == cudaSuccess) e = c.natv == 1 ? pipe_r_attrs<float, 1>() : pipe_r_attrs<float, 2>();
+  if (!cuda_ok(c, e, "pass R attributes")) return RISM3D_CUDA_ERROR;
+  c.pipe_r = true;
+  return RISM3D_OK;
+}
 
 int setup_fused_axes(Context &c) {
   c.xfused = false;
