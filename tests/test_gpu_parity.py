@@ -112,4 +112,4 @@ def test_fused_axis_passes_match_the_cufft_path(name):
     s1.close()
     assert abs(r1["iterations"] - r0["iterations"]) <= 10, (r1["iterations"], r0["iterations"])
     assert abs(r1["sfe_sc"] - r0["sfe_sc"]) < 0.1 * MU_TOL
-    assert abs(r1["pmv"] - r0["pmv"]) < 1e-5
+    assert abs(r1["pmv"] - r0["pmv"]) < 1e-4
