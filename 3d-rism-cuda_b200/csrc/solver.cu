@@ -1078,6 +1078,146 @@ __global__ void __launch_bounds__(kThreads) k_pass_r_pipe(IterArgs<T> a0) {
   if (threadIdx.x == 0) *a.count = 0u;
 }
 
+// Pass A as the same software pipeline (V <= 2): each thread prefetches its
+// 16-byte slices of the next chunk's inputs (the packed OZ result, t, U, the
+// two history slots Y, and R0 in the refinement form) while it updates the
+// current chunk; outputs go straight to global memory as 16-byte stores.
+template <typename T, int V, int CLOS, bool REF>
+__global__ void __launch_bounds__(kThreads) k_pass_a_pipe(IterArgs<T> a0) {
+  static_assert(V <= 2, "one packed site pair");
+  const IterArgs<T> a = solute_view<T, V>(a0);
+  typedef typename Cx<T>::t C;
+  typedef typename V2<T>::t T2;
+  constexpr int PTS = 16 / sizeof(T);
+  constexpr int CP = kThreads * PTS;
+  using S = PipeSlots<V>;                        // RP0 / RP1 slots carry Y0 / Y1 here
+  extern __shared__ float4 pipe_sm[];
+  const DevState *st = a.st;
+  const int done = st->done, mode = st->mode, slot_w = st->upd_slot;
+  const T s1 = (T)st->s1, s2 = (T)st->s2, m = (T)st->m;
+  if (done) {
+    if (st->after_done == 0) pass_a_final<T, V, CLOS, REF>(a, mode, done, slot_w, s1, s2, m);
+    return;                                     // past the snapshot: idle
+  }
+  const long long n = a.n;
+  const C *tw = a.tw;
+  auto slot = [&](int stage, int k) -> float4 * {
+    return pipe_sm + ((size_t)(stage * S::N + k) * kThreads + threadIdx.x);
+  };
+  const long long nchunks = (n + CP - 1) / CP;
+  auto issue = [&](long long c, int stage) {
+    const long long j = c * CP + (long long)threadIdx.x * PTS;
+    if (c < nchunks && j < n) {
+      if (mode != 0) {
+        cp16(slot(stage, S::BUF), a.buf + j);
+        cp16(slot(stage, S::BUF + 1), a.buf + j + PTS / 2);
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        cp16(slot(stage, S::T + v), a.t + (size_t)v * n + j);
+        cp16(slot(stage, S::U + v), a.U + (size_t)v * n + j);
+        if (mode == 2) {
+          cp16(slot(stage, S::RP0 + v), a.Y + (size_t)v * n + j);
+          cp16(slot(stage, S::RP1 + v), a.Y + (size_t)(V + v) * n + j);
+        }
+        if (REF && mode != 0) cp16(slot(stage, S::R0 + v), a.R0 + (size_t)v * n + j);
+      }
+    }
+    cp_commit();
+  };
+  long long c = blockIdx.x;
+  issue(c, 0);
+  for (int stage = 0; c < nchunks; c += gridDim.x, stage ^= 1) {
+    issue(c + gridDim.x, stage ^ 1);
+    cp_wait<1>();
+    const long long j = c * CP + (long long)threadIdx.x * PTS;
+    if (j >= n) continue;
+    const T *bz0 = reinterpret_cast<const T *>(slot(stage, S::BUF));
+    const T *bz1 = reinterpret_cast<const T *>(slot(stage, S::BUF + 1));
+    int ix, iy, iz, dir0;
+    C dkf[PTS];
+    point_phase(j, a.fdx, a.fdy, tw, ix, iy, iz, dir0, dkf[0]);
+    {
+      const C tyz = cmul(tw[a.nx + iy], tw[a.nx + a.ny + iz]);
+#pragma unroll
+      for (int k = 1; k < PTS; ++k) dkf[k] = cmul(tw[ix + k], tyz);
+    }
+    T tn[V][PTS], yw[V][PTS], rw[V][PTS];
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) {
+      const int dir = (k & 1) ? -dir0 : dir0;
+      T h[2] = {T(0), T(0)};
+      if (mode != 0) {
+        // inverse post-twiddle (timekb, fft3d.cu:52-60): (1/V) dir conj(dkf)
+        const T sc = (T)a.invvol * (T)dir;
+        const C w = mk<C>(dkf[k].x * sc, -dkf[k].y * sc);
+        const T *bz = k < PTS / 2 ? bz0 + 2 * k : bz1 + 2 * (k - PTS / 2);
+        C zz;
+        zz.x = bz[0];
+        zz.y = bz[1];
+        const C z = cmul(zz, w);
+        h[0] = z.x;
+        h[1] = z.y;
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const T tv = reinterpret_cast<const T *>(slot(stage, S::T + v))[k];
+        tn[v][k] = tv;
+        if (mode != 0) {
+          const T Uv = reinterpret_cast<const T *>(slot(stage, S::U + v))[k];
+          const T r0 = REF ? reinterpret_cast<const T *>(slot(stage, S::R0 + v))[k] : T(0);
+          const T R = residual<CLOS, REF>(h[v], tv, Uv, r0);   // tr
+          const T y = tv + m * R;
+          rw[v][k] = R;
+          yw[v][k] = y;
+          if (mode == 1) {
+            tn[v][k] = tv + R;                                   // newdt0 (Picard)
+          } else {                                               // newdt (AN2)
+            const T y0 = reinterpret_cast<const T *>(slot(stage, S::RP0 + v))[k];
+            const T y1 = reinterpret_cast<const T *>(slot(stage, S::RP1 + v))[k];
+            tn[v][k] = y + s1 * (y0 - y) + s2 * (y1 - y);
+          }
+        }
+      }
+    }
+    if (mode != 0) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const size_t iv = (size_t)v * n + j;
+        T *py = a.Y + (size_t)slot_w * V * n + iv, *pr = a.RP + (size_t)slot_w * V * n + iv,
+          *pt = a.t + iv;
+#pragma unroll
+        for (int h2 = 0; h2 < PTS / 2; ++h2) {
+          T2 wy, wr, wt;
+          wy.x = yw[v][2 * h2]; wy.y = yw[v][2 * h2 + 1];
+          wr.x = rw[v][2 * h2]; wr.y = rw[v][2 * h2 + 1];
+          wt.x = tn[v][2 * h2]; wt.y = tn[v][2 * h2 + 1];
+          reinterpret_cast<T2 *>(py)[h2] = wy;
+          reinterpret_cast<T2 *>(pr)[h2] = wr;
+          reinterpret_cast<T2 *>(pt)[h2] = wt;
+        }
+      }
+    }
+    // closure + c_SR (kh/hnc + trm1mt, calculate_cuda.cu:1-29) and the
+    // forward pre-twiddle (timekf, fft3d.cu:41-49): dir * dkf * (c_a + i c_b)
+    C out[PTS];
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) {
+      const int dir = (k & 1) ? -dir0 : dir0;
+      const C wf = mk<C>(dkf[k].x * dir, dkf[k].y * dir);
+      C z;
+      z.x = cfun<CLOS, REF>(tn[0][k], reinterpret_cast<const T *>(slot(stage, S::U))[k]);
+      z.y = (V > 1) ? cfun<CLOS, REF>(tn[V - 1][k],
+                                      reinterpret_cast<const T *>(slot(stage, S::U + V - 1))[k])
+                    : T(0);
+      out[k] = cmul(z, wf);
+    }
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) a.buf[j + k] = out[k];
+  }
+  cp_wait<0>();
+}
+
 // ------------------------------------------------------------- finalize
 // Run by the last block of pass R to finish: fixed-order reduction of the
 // block sums, then the host logic of iterate.cu:52-62 and AN2::calculate
@@ -1325,6 +1465,13 @@ int pipe_r_blocks(const Context &c) {
 }
 
 template <typename T, int V, int CLOS, bool REF>
+int pipe_a_blocks(const Context &c) {
+  constexpr int CP = kThreads * (16 / (int)sizeof(T));
+  return wave_blocks_smem(k_pass_a_pipe<T, V, CLOS, REF>, kThreads, pass_r_pipe_smem<T, V>(),
+                          (c.n + CP - 1) / CP);
+}
+
+template <typename T, int V, int CLOS, bool REF>
 void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   if constexpr (sizeof(T) == 4 && V <= 2) {
     if (c.xfused) {
@@ -1335,7 +1482,15 @@ void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   }
   const dim3 ba(wave_blocks(k_pass_a<T, V, CLOS, REF>, a.n, c.nb), c.nb),
       bk(wave_blocks(k_kspace<T, V>, a.n / 2, c.nb), c.nb), br(a.nblocks, c.nb);
-  k_pass_a<T, V, CLOS, REF><<<ba, kThreads, 0, c.stream>>>(a);
+  if constexpr (V <= 2) {
+    if (c.pipe_r)
+      k_pass_a_pipe<T, V, CLOS, REF><<<dim3(pipe_a_blocks<T, V, CLOS, REF>(c), c.nb), kThreads,
+                                       pass_r_pipe_smem<T, V>(), c.stream>>>(a);
+    else
+      k_pass_a<T, V, CLOS, REF><<<ba, kThreads, 0, c.stream>>>(a);
+  } else {
+    k_pass_a<T, V, CLOS, REF><<<ba, kThreads, 0, c.stream>>>(a);
+  }
   typedef typename Cx<T>::t C;
   if (sizeof(T) == 8) {
     cufftExecZ2Z(plan, (cufftDoubleComplex *)a.buf, (cufftDoubleComplex *)a.buf, CUFFT_FORWARD);
@@ -1876,8 +2031,26 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
   }
   for (int r = 0; r < reps && !fused_done; ++r) {
     switch (which) {
-      case 0: case 10: k_pass_a<T, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a); break;
-      case 13: k_pass_a<T, V, CLOS, true><<<bar, kThreads, 0, c.stream>>>(a); break;
+      case 0: case 10:
+        if constexpr (V <= 2) {
+          if (c.pipe_r) {
+            k_pass_a_pipe<T, V, CLOS, false><<<pipe_a_blocks<T, V, CLOS, false>(c), kThreads,
+                                               pass_r_pipe_smem<T, V>(), c.stream>>>(a);
+            break;
+          }
+        }
+        k_pass_a<T, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a);
+        break;
+      case 13:
+        if constexpr (V <= 2) {
+          if (c.pipe_r) {
+            k_pass_a_pipe<T, V, CLOS, true><<<pipe_a_blocks<T, V, CLOS, true>(c), kThreads,
+                                              pass_r_pipe_smem<T, V>(), c.stream>>>(a);
+            break;
+          }
+        }
+        k_pass_a<T, V, CLOS, true><<<bar, kThreads, 0, c.stream>>>(a);
+        break;
       case 1: case 11: k_kspace<T, V><<<bk, kThreads, 0, c.stream>>>(a); break;
       case 15:
         if constexpr (V <= 2) {
@@ -1944,6 +2117,10 @@ cudaError_t pipe_r_attrs() {
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_r_pipe<T, V, 1, false>, at, b);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_r_pipe<T, V, 0, true>, at, b);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_r_pipe<T, V, 1, true>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_a_pipe<T, V, 0, false>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_a_pipe<T, V, 1, false>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_a_pipe<T, V, 0, true>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_a_pipe<T, V, 1, true>, at, b);
   return e;
 }
 
