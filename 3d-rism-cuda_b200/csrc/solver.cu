@@ -1078,10 +1078,11 @@ __global__ void __launch_bounds__(kThreads) k_pass_r_pipe(IterArgs<T> a0) {
   if (threadIdx.x == 0) *a.count = 0u;
 }
 
-// Pass A as the same software pipeline (V <= 2): each thread prefetches its
-// 16-byte slices of the next chunk's inputs (the packed OZ result, t, U, the
-// two history slots Y, and R0 in the refinement form) while it updates the
-// current chunk; outputs go straight to global memory as 16-byte stores.
+// Pass A as the same software pipeline (V <= 2), used for the refinement
+// form (which reads R0 as well): each thread prefetches its 16-byte slices
+// of the next chunk's inputs (the packed OZ result, t, U, the two history
+// slots Y, R0) while it updates the current chunk; outputs go straight to
+// global memory.
 template <typename T, int V, int CLOS, bool REF>
 __global__ void __launch_bounds__(kThreads) k_pass_a_pipe(IterArgs<T> a0) {
   static_assert(V <= 2, "one packed site pair");
@@ -1482,7 +1483,9 @@ void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   }
   const dim3 ba(wave_blocks(k_pass_a<T, V, CLOS, REF>, a.n, c.nb), c.nb),
       bk(wave_blocks(k_kspace<T, V>, a.n / 2, c.nb), c.nb), br(a.nblocks, c.nb);
-  if constexpr (V <= 2) {
+  // the pipelined pass A pays for the refinement form (it reads R0 too);
+  // the plain form already streams near bandwidth from registers
+  if constexpr (V <= 2 && REF) {
     if (c.pipe_r)
       k_pass_a_pipe<T, V, CLOS, REF><<<dim3(pipe_a_blocks<T, V, CLOS, REF>(c), c.nb), kThreads,
                                        pass_r_pipe_smem<T, V>(), c.stream>>>(a);
@@ -2031,16 +2034,7 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
   }
   for (int r = 0; r < reps && !fused_done; ++r) {
     switch (which) {
-      case 0: case 10:
-        if constexpr (V <= 2) {
-          if (c.pipe_r) {
-            k_pass_a_pipe<T, V, CLOS, false><<<pipe_a_blocks<T, V, CLOS, false>(c), kThreads,
-                                               pass_r_pipe_smem<T, V>(), c.stream>>>(a);
-            break;
-          }
-        }
-        k_pass_a<T, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a);
-        break;
+      case 0: case 10: k_pass_a<T, V, CLOS, false><<<ba, kThreads, 0, c.stream>>>(a); break;
       case 13:
         if constexpr (V <= 2) {
           if (c.pipe_r) {
