@@ -503,6 +503,28 @@ __global__ void __launch_bounds__(kThreads) k_kspace(IterArgs<T> a0) {
   if (a.st->done) return;
   const long long n = a.n, nh = n / 2;
   C *__restrict__ buf = a.buf;
+  if constexpr (sizeof(T) == 4 && P == 1) {
+    // FP32, one site pair: two neighbouring owner points j, j + 1 (j even,
+    // same x row) and their mirrors jm - 1, jm per thread, each pair of
+    // complex values one 16-byte access, so twice the bytes are in flight
+    for (long long j = 2 * ((long long)blockIdx.x * blockDim.x + threadIdx.x); j < nh;
+         j += 2 * (long long)gridDim.x * blockDim.x) {
+      const long long jm = n - 1 - j;           // k(jm) = -k(j); jm - 1 mirrors j + 1
+      const float4 w = *reinterpret_cast<const float4 *>(buf + j);
+      const float4 wm = *reinterpret_cast<const float4 *>(buf + jm - 1);
+      int ix, iy, iz;
+      split_index(j, a.fdx, a.fdy, ix, iy, iz);
+      C y0[1] = {make_float2(w.x, w.y)}, y1[1] = {make_float2(w.z, w.w)};
+      C ym0[1] = {make_float2(wm.z, wm.w)}, ym1[1] = {make_float2(wm.x, wm.y)};
+      C o0[1], om0[1], o1[1], om1[1];
+      kspace_pair<T, V>(a, j, ix, iy, iz, y0, ym0, o0, om0);
+      kspace_pair<T, V>(a, j + 1, ix + 1, iy, iz, y1, ym1, o1, om1);
+      *reinterpret_cast<float4 *>(buf + j) = make_float4(o0[0].x, o0[0].y, o1[0].x, o1[0].y);
+      *reinterpret_cast<float4 *>(buf + jm - 1) =
+          make_float4(om1[0].x, om1[0].y, om0[0].x, om0[0].y);
+    }
+    return;
+  }
   for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nh;
        j += (long long)gridDim.x * blockDim.x) {
     const long long jm = n - 1 - j;             // k(jm) = -k(j)
