@@ -355,7 +355,7 @@ def run_batch(args, dev, stream, rank=0, world=1, dist=False):
     in the reference's 3-site water + 0.1 M NaCl table (4 site types; the
     5-site water of the config needs the project's 1D XRISM tables).  Reports
     solves/s of one rism3d_solve_batch call and of a per-solute loop that
-    reuses one context per grid size (timed on a sample of the molecules).
+    reuses one context per grid size (timed on every molecule).
     Under N ranks the molecules are split by estimated cost (grid points);
     solves/s is all ranks' molecules over the slowest rank's time."""
     import torch
@@ -386,14 +386,14 @@ def run_batch(args, dev, stream, rank=0, world=1, dist=False):
     torch.cuda.synchronize()
     s_batch = e0.elapsed_time(e1) / 1e3
     parent.close()
-    # per-solute loop on a sample, one context per grid size (warm)
+    # per-solute loop over the same molecules, one context per grid size (warm)
     ctxs = {}
     for g in sorted({m[4] for m in mols}):
         L = [m[5] for m in mols if m[4] == g][0]
         c = R.Solver((g, g, g), (L, L, L), precision=R.MIXED, device=dev, stream=stream.cuda_stream)
         c.set_solvent_obj(sv)
         ctxs[g] = c
-    sample = mols[: max(8, len(mols) // 8)]
+    sample = mols                                 # every molecule of the batch
     for m in sample[:3]:
         ctxs[m[4]].set_solute(*m[:4]); ctxs[m[4]].solve()
     torch.cuda.synchronize()
