@@ -271,6 +271,10 @@ def run_ours(args, rank, world, dist):
     t1 = time.perf_counter()
     mixed.grad()
     adjoint_s = time.perf_counter() - t1
+    mixed.grad(precision=R.MIXED)                 # the FP32 adjoint variant (own scratch)
+    t1 = time.perf_counter()
+    mixed.grad(precision=R.MIXED)
+    adjoint32_s = time.perf_counter() - t1
     mixed.close(); fp64.close()
     batch = run_batch(args, dev, stream, rank, world, dist) if args.batch_mols > 0 else None
     cli = None
@@ -325,7 +329,8 @@ def run_ours(args, rank, world, dist):
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
         "batch": batch,
         "cli": cli,
-        "adjoint": {"s_per_gradient": adjoint_s, "timing": "second call (the first allocates scratch)",
+        "adjoint": {"s_per_gradient": adjoint_s, "s_per_gradient_fp32": adjoint32_s,
+                    "timing": "second call (the first allocates scratch)",
                     "outputs": "d mu/d(q, sigma, eps, xyz) of all "
                     "%d atoms" % len(sol.q)},
         "kernels": kern,
