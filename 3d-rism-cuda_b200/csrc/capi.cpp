@@ -102,6 +102,10 @@ void free_device(Context &c) {
   c.xfused = false;
   if (c.d_xroots) cudaFree(c.d_xroots);
   c.d_xroots = nullptr;
+  if (c.d_fkt) cudaFree(c.d_fkt);
+  c.d_fkt = nullptr;
+  delete c.ky_map;
+  c.ky_map = nullptr;
   if (c.plan64) cufftDestroy(c.plan64);
   if (c.plan32) cufftDestroy(c.plan32);
   if (c.plan1) cufftDestroy(c.plan1);

@@ -334,6 +334,10 @@ int compute_potentials(Context &c) {
   cudaFreeAsync(ph, c.stream);
   if (!cuda_ok(c, cudaGetLastError(), "k_potential_k")) return RISM3D_CUDA_ERROR;
   c.launches += 3;
+  if (c.d_fkt) {                                  // the TMA fused pass K reads fk by columns
+    const int rc = fused_fk_columns(c);
+    if (rc != RISM3D_OK) return rc;
+  }
   if (c.d_esp && c.nb == 1) {
     const long long eb = std::min<long long>((c.n + kThreads - 1) / kThreads, 148 * 16);
     k_esp_esr<<<(unsigned)eb, kThreads, 0, c.stream>>>(

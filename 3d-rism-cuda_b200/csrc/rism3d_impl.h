@@ -1,6 +1,7 @@
 // Internal declarations of the B200 3D-RISM solver (not part of the ABI).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -45,6 +46,8 @@ struct DevState {
   int total32;     // of which FP32
   int fallback;    // (solute 0) the FP32 bulk diverged: stage restarts in FP64
   int restart_next;  // (solute 0) FP64 phase starts a fresh AN2 history
+  int fault;       // a device-side wait gave up (a bulk or tile copy never
+                   // arrived): the loop was stopped and the solve reports it
   double best;     // best rms of this run (stagnation watch)
   double conv;
   double m, mp;    // AN2 mixing factor and bias
@@ -197,9 +200,14 @@ struct Context {
   // solutes, natv <= 2, nx = ny = 64 or 256): cuFFT then transforms along z
   // only (plan32z), with the x-line roots of unity in d_xroots
   bool pipe_r = false;       // pass R as the cp.async pipeline (natv <= 2)
+  bool bulk_r = false;       // pass R as the bulk-copy (cp.async.bulk) stream
   bool xfused = false;
   cufftHandle plan32z = 0;
   float2 *d_xroots = nullptr;
+  // TMA form of the fused pass K (nx = ny = 256): tensor map over f_buf and
+  // beta fk in FP32 laid out [nz/2][nx][ny]
+  CUtensorMap *ky_map = nullptr;
+  float2 *d_fkt = nullptr;
   cufftHandle plan1 = 0;     // one Z2Z transform of the cell (RMDFT), made on first use
   bool plans_ok = false;
   // one captured iteration per precision, reused by every solve
@@ -257,6 +265,8 @@ int launch_potential_r(Context &c);               // potential.cu (timing hook)
 int upload_chi(Context &c);                       // solver.cu
 // decide on and set up the fused-axis FP32 passes (plan, roots, limits)
 int setup_fused_axes(Context &c);                 // solver.cu
+int setup_kspace_tma(Context &c);                 // solver.cu: TMA fused pass K
+int fused_fk_columns(Context &c);                 // solver.cu: fk copy for it
 int setup_pipe_r(Context &c);                     // solver.cu: pipelined pass R
 // spline.cc:4-43: natural cubic spline through (xp[k], yp[k]), k < np; writes
 // {y_k, b_k, c_k, d_k} (y + b t + c t^2 + d t^3 on interval k; zero

@@ -44,6 +44,7 @@
 #include <cstring>
 
 #include "rism3d_impl.h"
+#include "tma.cuh"
 #include "xfft.cuh"
 
 namespace rism3d {
@@ -82,6 +83,7 @@ struct IterArgs {
   int hist_cap;
   int nofk;                 // refinement: q cf fk cancels, fk is not read
   const float2 *xroots;     // fused-axis passes: W_nx^m, m < nx (nx == ny)
+  const float2 *fkt;        // fused-axis pass K (nx = 256): beta fk as [nz/2][nx][ny]
 };
 
 // Batched solves: blockIdx.y selects the solute; every per-solute array is
@@ -415,16 +417,16 @@ __global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a0) {
 // and jm = N-1-j with k(jm) = -k(j).  y/ym are the forward-transformed
 // packed site pairs at j and jm; out/outm receive the OZ result repacked
 // for the inverse transform.
+// fk is beta fk at the owner point (zero when a.nofk).
 template <typename T, int V>
-__device__ __forceinline__ void kspace_pair(const IterArgs<T> &a, long long j, int ix, int iy,
-                                            int iz, const typename Cx<T>::t *y,
-                                            const typename Cx<T>::t *ym,
-                                            typename Cx<T>::t *out, typename Cx<T>::t *outm) {
+__device__ __forceinline__ void kspace_pair_fk(const IterArgs<T> &a, double2 fk, int ix, int iy,
+                                               int iz, const typename Cx<T>::t *y,
+                                               const typename Cx<T>::t *ym,
+                                               typename Cx<T>::t *out, typename Cx<T>::t *outm) {
   typedef typename Cx<T>::t C;
   constexpr int P = (V + 1) / 2;
   const StageParams *sp = a.sp;
   const int dir = ((ix + iy + iz) & 1) ? -1 : 1;
-  const double2 fk = a.nofk ? make_double2(0.0, 0.0) : a.fkh[j];
   // unpack the site pairs and finish the forward transform
   // (timeirvol * dv, fft3d.cu:32) and subtract q cf fk (mqvfk)
   C F[V];
@@ -493,6 +495,15 @@ __device__ __forceinline__ void kspace_pair(const IterArgs<T> &a, long long j, i
     out[p] = mk<C>(d * (ha.x - hb.y), d * (ha.y + hb.x));
     outm[p] = mk<C>(-d * (ha.x + hb.y), -d * (hb.x - ha.y));
   }
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void kspace_pair(const IterArgs<T> &a, long long j, int ix, int iy,
+                                            int iz, const typename Cx<T>::t *y,
+                                            const typename Cx<T>::t *ym,
+                                            typename Cx<T>::t *out, typename Cx<T>::t *outm) {
+  const double2 fk = a.nofk ? make_double2(0.0, 0.0) : a.fkh[j];
+  kspace_pair_fk<T, V>(a, fk, ix, iy, iz, y, ym, out, outm);
 }
 
 template <typename T, int V>
@@ -949,6 +960,186 @@ __global__ void __launch_bounds__(kW * E, 2) k_kspace_y(IterArgs<float> a) {
 
 
 
+// Pass K with the y-axis DFTs folded in, TMA form (nx = ny = 256, one site
+// pair).  A tile is 16 consecutive kx columns x 256 ky rows at one kz < nz/2
+// (32 KB of FP32 complex values) together with its mirror tile (columns
+// nx - c0 - 16 .. nx - c0 - 1 at nz - 1 - kz).  The TMA unit fetches both
+// into one of three shared-memory stages (128-byte rows, 128B swizzle) two
+// tiles ahead of the one being transformed, and tile stores write the
+// results back from the same stage, so the block's threads never issue a
+// global load or store of the grid themselves.
+//
+// Warp w transforms owner column w (lanes 0-15) and mirror column 15 - w
+// (lanes 16-31).  Lane t holds the points y = t + 16 j of its column; the
+// transpose of each 256-point DFT runs in place in the column's own
+// shared-memory slots (skewed so that both of its sides are free of bank
+// conflicts) behind __syncwarp only.  After the forward DFT the mirror of
+// owner point ky = t + 16 k (-k: nx-1-kx, ny-1-ky, nz-1-kz) sits in lane
+// t ^ 31 at register 15 - k, so a lane takes half of its column's
+// owner/mirror pairs with one shuffle each way.  beta fk comes from an FP32
+// copy laid out [kz][kx][ky] (ky fastest): the pairs of one step of a warp
+// read two runs of 16 consecutive values.  (Only the plain FP32 bulk reads
+// fk: the refinement form cancels it and the FP64 cycles use the FP64 grid,
+// so its FP32 rounding stays below the bulk's own rounding floor.)
+constexpr int kKyThreads = 512;
+constexpr int kKyStages = 3;
+constexpr unsigned kKyTileBytes = 16u * 256u * (unsigned)sizeof(float2);
+constexpr size_t kKySmem = (size_t)kKyStages * 2 * kKyTileBytes + 1024;   // + alignment
+constexpr long long kKyWaitPolls = 1LL << 24;
+
+// byte offset of float2 (row r, column c) in a tile of 16-column rows
+// stored with the 128B swizzle (16-byte chunk index XOR row mod 8)
+__device__ __forceinline__ unsigned ky_swz(int r, int c) {
+  return (unsigned)r * 128u + ((((unsigned)c >> 1) ^ ((unsigned)r & 7u)) << 4) +
+         (((unsigned)c & 1u) << 3);
+}
+
+// 256-point DFT of one tile column held by 16 lanes (v[j] = x[t + 16 j] in,
+// v[k] = X[t + 16 k] out); the transpose goes through the column's slots:
+// A_t[k1] is stored at row 16 k1 + ((t + k1) mod 16).
+template <bool INV>
+__device__ __forceinline__ void ky_col_dft(float2 (&v)[16], int t, unsigned char *tile, int c,
+                                           const float2 *__restrict__ roots) {
+  xfft::stage1<16, INV>(v, t, roots);
+  __syncwarp();                                  // the column's inputs are all read
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1)
+    *reinterpret_cast<float2 *>(tile + ky_swz(16 * k1 + ((t + k1) & 15), c)) = v[k1];
+  __syncwarp();
+#pragma unroll
+  for (int s = 0; s < 16; ++s)
+    v[s] = *reinterpret_cast<const float2 *>(tile + ky_swz(16 * t + ((s + t) & 15), c));
+  xfft::dft_small<16, INV>(v);
+}
+
+template <int V>
+__global__ void __launch_bounds__(kKyThreads, 1)
+    k_kspace_yt(IterArgs<float> a, const __grid_constant__ CUtensorMap map) {
+  constexpr int NY = 256;
+  extern __shared__ unsigned char ky_raw[];
+  __shared__ __align__(8) uint64_t full[kKyStages];
+  DevState *st = a.st;
+  if (st->done) return;
+  unsigned char *sm =
+      reinterpret_cast<unsigned char *>(((uintptr_t)ky_raw + 1023) & ~(uintptr_t)1023);
+  const int nx = a.nx, nz = a.nz;
+  const int cblocks = nx / 16, tiles = cblocks * (nz / 2);
+  const int mine = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, t = lane & 15;
+  const bool own = lane < 16;
+  const int c = own ? w : 15 - w;                // this half-warp's column in its tile
+  const unsigned half = own ? 0u : kKyTileBytes;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kKyStages; ++s) tma::mbar_init(&full[s], 1);
+    tma::mbar_init_fence();
+  }
+  __syncthreads();
+  // thread 0: fetch this block's tile i (owner and mirror) into stage i mod 3
+  auto fetch = [&](int i) {
+    const int tile = (int)blockIdx.x + i * (int)gridDim.x;
+    const int cb = tile % cblocks, kz = tile / cblocks;
+    unsigned char *dst = sm + (size_t)(i % kKyStages) * 2 * kKyTileBytes;
+    uint64_t *bar = &full[i % kKyStages];
+    tma::mbar_arrive_expect_tx(bar, 2 * kKyTileBytes);
+    tma::load_2d(dst, &map, bar, 2 * 16 * cb, kz * NY);
+    tma::load_2d(dst + kKyTileBytes, &map, bar, 2 * (nx - 16 * cb - 16), (nz - 1 - kz) * NY);
+  };
+  int fetched = 0;
+  if (threadIdx.x == 0)
+    for (; fetched < 2 && fetched < mine; ++fetched) fetch(fetched);
+  int fault = 0, i = 0;
+  for (; i < mine; ++i) {
+    const int tile = (int)blockIdx.x + i * (int)gridDim.x;
+    const int cb = tile % cblocks, kz = tile / cblocks;
+    const int kx = 16 * cb + w;                  // the warp's owner column
+    // beta fk at the owner points of this lane's eight pairs, before the wait
+    float2 fk[8];
+    if (a.nofk) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) fk[k] = make_float2(0.0f, 0.0f);
+    } else {
+      const float2 *fc = a.fkt + ((size_t)kz * nx + kx) * NY;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) fk[k] = fc[own ? t + 16 * k : (15 - t) + 16 * (15 - k)];
+    }
+    // (warp-uniform, so that the shuffles below always run on full warps)
+    const bool ready = __all_sync(0xffffffffu, tma::mbar_wait_bounded(&full[i % kKyStages],
+                                                                      (unsigned)(i / kKyStages) & 1u,
+                                                                      kKyWaitPolls));
+    unsigned char *col = sm + (size_t)(i % kKyStages) * 2 * kKyTileBytes + half;
+    if (ready) {
+      float2 v[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[j] = *reinterpret_cast<const float2 *>(col + ky_swz(t + 16 * j, c));
+      ky_col_dft<false>(v, t, col, c, a.xroots);
+      // owner lane t: pairs k = 0..7 of its column; mirror lane t ^ 31:
+      // the owner registers 15..8 of lane t
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        float2 p;
+        p.x = __shfl_xor_sync(0xffffffffu, v[15 - k].x, 31);
+        p.y = __shfl_xor_sync(0xffffffffu, v[15 - k].y, 31);
+        const int ky = own ? t + 16 * k : (15 - t) + 16 * (15 - k);
+        float2 y[1] = {own ? v[k] : p}, ym[1] = {own ? p : v[k]}, o[1], om[1];
+        kspace_pair_fk<float, V>(a, make_double2(fk[k].x, fk[k].y), kx, ky, kz, y, ym, o, om);
+        v[k] = own ? o[0] : om[0];
+        const float2 back = own ? om[0] : o[0];
+        v[15 - k].x = __shfl_xor_sync(0xffffffffu, back.x, 31);
+        v[15 - k].y = __shfl_xor_sync(0xffffffffu, back.y, 31);
+      }
+      ky_col_dft<true>(v, t, col, c, a.xroots);
+      __syncwarp();                              // the transpose's reads are done
+#pragma unroll
+      for (int j = 0; j < 16; ++j) *reinterpret_cast<float2 *>(col + ky_swz(t + 16 * j, c)) = v[j];
+    }
+    tma::fence_proxy_async();                    // the stage's writes, before the TMA reads them
+    fault = __syncthreads_or(!ready);
+    if (fault) break;
+    if (threadIdx.x == 0) {
+      const unsigned char *src = sm + (size_t)(i % kKyStages) * 2 * kKyTileBytes;
+      tma::store_2d(&map, src, 2 * 16 * cb, kz * NY);
+      tma::store_2d(&map, src + kKyTileBytes, 2 * (nx - 16 * cb - 16), (nz - 1 - kz) * NY);
+      tma::bulk_commit();
+      if (fetched < mine) {
+        tma::bulk_wait_read<1>();                // that stage's previous tile is stored
+        fetch(fetched++);
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    if (fault) {
+      // a tile never arrived: wait (bounded) for every fetch still in flight
+      // before the block's shared memory goes away, then stop the loop
+      for (int f = i; f < fetched; ++f)
+        tma::mbar_wait_bounded(&full[f % kKyStages], (unsigned)(f / kKyStages) & 1u, kKyWaitPolls);
+      st->fault = 1;
+      st->done = 2;
+    }
+    tma::bulk_wait<0>();
+  }
+}
+
+// beta fk re-laid out for k_kspace_yt: each kz plane of the owner half
+// transposed from [ky][kx] to [kx][ky] and rounded to FP32, 32 x 32 tiles
+// through shared memory.
+__global__ void k_fk_columns(int nx, int ny, const double2 *__restrict__ fkh,
+                             float2 *__restrict__ fkt) {
+  __shared__ double2 tile[32][33];
+  const size_t plane = (size_t)blockIdx.z * nx * ny;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int x = x0 + threadIdx.x, y = y0 + r;
+    if (x < nx && y < ny) tile[r][threadIdx.x] = fkh[plane + (size_t)y * nx + x];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int x = x0 + r, y = y0 + threadIdx.x;
+    if (x < nx && y < ny)
+      fkt[plane + (size_t)x * ny + y] =
+          make_float2((float)tile[threadIdx.x][r].x, (float)tile[threadIdx.x][r].y);
+  }
+}
+
 // Pass R as a software pipeline (V <= 2, one packed site pair): a block
 // walks chunks of kThreads * PTS consecutive points (PTS = 16 bytes of T),
 // and each thread copies its own 16-byte slice of every input of the NEXT
@@ -1088,6 +1279,172 @@ __global__ void __launch_bounds__(kThreads) k_pass_r_pipe(IterArgs<T> a0) {
   if (threadIdx.x < 6) {
     double s = 0.0;
     for (int w = 0; w < kThreads / 32; ++w) s += red[w][threadIdx.x];
+    a.part[(size_t)threadIdx.x * a.nblocks + blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(a.count, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_block(st, a.part, a.nblocks, (double)n * V, a.hist, a.hist_cap);
+  if (threadIdx.x == 0) *a.count = 0u;
+}
+
+// Pass R as a bulk-copy stream (V <= 2, one packed site pair).  A chunk is
+// bulk_pts<T>() consecutive points; thread 0 copies every input stream of a
+// chunk (buf, t and U per site, the two RP history slots when the Gram sums
+// are due, R0 in the refinement form) into one of kBulkStages shared-memory
+// stages with cp.async.bulk, kBulkStages - 1 chunks ahead of the one being
+// reduced, the bytes counted on the stage's mbarrier.  The other threads
+// issue no global loads at all: they read their points from the stage.  One
+// block per SM keeps ~3 x 48 KB of reads in flight.
+constexpr int kBulkThreads = 512;
+constexpr int kBulkStages = 4;
+constexpr long long kBulkWaitPolls = 1LL << 24;
+template <typename T> __host__ __device__ constexpr int bulk_pts() {
+  return sizeof(T) == 4 ? 1024 : 512;
+}
+template <typename T, int V> __host__ __device__ constexpr size_t bulk_stage_bytes() {
+  return (size_t)bulk_pts<T>() * (2 * sizeof(T) + 5 * V * sizeof(T));   // buf; t U RP0 RP1 R0
+}
+template <typename T, int V> __host__ __device__ constexpr size_t bulk_smem() {
+  return (size_t)kBulkStages * bulk_stage_bytes<T, V>();
+}
+
+template <typename T, int V, int CLOS, bool REF>
+__global__ void __launch_bounds__(kBulkThreads, 1) k_pass_r_bulk(IterArgs<T> a0) {
+  static_assert(V <= 2, "one packed site pair");
+  static_assert(kBulkThreads % kThreads == 0, "finalize_block folds groups of kThreads");
+  const IterArgs<T> a = solute_view<T, V>(a0);
+  typedef typename Cx<T>::t C;
+  constexpr int CP = bulk_pts<T>(), PT = CP / kBulkThreads;
+  constexpr size_t SB = bulk_stage_bytes<T, V>();
+  extern __shared__ __align__(16) unsigned char bulk_sm[];
+  __shared__ __align__(8) uint64_t full[kBulkStages];
+  __shared__ double red[kBulkThreads / 32][6];
+  __shared__ bool last;
+  DevState *st = a.st;
+  if (st->done) {                                // loop stopped: count idle cycles
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->after_done += 1;
+    return;
+  }
+  const bool gram = st->count <= 0;
+  const long long n = a.n;
+  const C *tw = a.tw;
+  double w8[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) w8[v] = a.sp->irho[v];
+  const long long nchunks = (n + CP - 1) / CP;
+  const int mine = (long long)blockIdx.x < nchunks
+                       ? (int)((nchunks - 1 - blockIdx.x) / gridDim.x) + 1 : 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kBulkStages; ++s) tma::mbar_init(&full[s], 1);
+    tma::mbar_init_fence();
+  }
+  __syncthreads();
+  // thread 0: copy chunk i of this block into stage i mod kBulkStages; stage
+  // layout [CP] C buf, then [CP] T each: t[V], U[V], RP0[V], RP1[V], R0[V]
+  auto fetch = [&](int i) {
+    const long long j0 = ((long long)blockIdx.x + (long long)i * gridDim.x) * CP;
+    const unsigned np = (unsigned)min((long long)CP, n - j0);
+    unsigned char *sg = bulk_sm + (size_t)(i % kBulkStages) * SB;
+    T *sT = reinterpret_cast<T *>(sg + CP * sizeof(C));
+    uint64_t *bar = &full[i % kBulkStages];
+    const unsigned bt = np * (unsigned)sizeof(T);
+    const unsigned streams = 2 * V + (gram ? 2 * V : 0) + (REF ? V : 0);
+    tma::mbar_arrive_expect_tx(bar, np * (unsigned)sizeof(C) + streams * bt);
+    tma::bulk_load(sg, a.buf + j0, np * (unsigned)sizeof(C), bar);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      tma::bulk_load(sT + (size_t)v * CP, a.t + (size_t)v * n + j0, bt, bar);
+      tma::bulk_load(sT + (size_t)(V + v) * CP, a.U + (size_t)v * n + j0, bt, bar);
+      if (gram) {
+        tma::bulk_load(sT + (size_t)(2 * V + v) * CP, a.RP + (size_t)v * n + j0, bt, bar);
+        tma::bulk_load(sT + (size_t)(3 * V + v) * CP, a.RP + (size_t)(V + v) * n + j0, bt, bar);
+      }
+      if (REF) tma::bulk_load(sT + (size_t)(4 * V + v) * CP, a.R0 + (size_t)v * n + j0, bt, bar);
+    }
+  };
+  int fetched = 0;
+  if (threadIdx.x == 0)
+    for (; fetched < kBulkStages - 1 && fetched < mine; ++fetched) fetch(fetched);
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  int fault = 0, i = 0;
+  for (; i < mine; ++i) {
+    // every thread is past chunk i - 1: its stage takes chunk i + kBulkStages - 1
+    if (__syncthreads_or(fault)) break;
+    if (threadIdx.x == 0 && fetched < mine) fetch(fetched++);
+    if (!tma::mbar_wait_bounded(&full[i % kBulkStages], (unsigned)(i / kBulkStages) & 1u,
+                                kBulkWaitPolls)) {
+      fault = 1;
+      continue;
+    }
+    const long long j0 = ((long long)blockIdx.x + (long long)i * gridDim.x) * CP;
+    const unsigned char *sg = bulk_sm + (size_t)(i % kBulkStages) * SB;
+    const C *sb = reinterpret_cast<const C *>(sg);
+    const T *sT = reinterpret_cast<const T *>(sg + CP * sizeof(C));
+    // PT consecutive points along x (j0 and PT are even, so they share a
+    // row and their twiddles differ only in the x factor)
+    const int q0 = threadIdx.x * PT;
+    if (j0 + q0 >= n) continue;
+    int ix, iy, iz, dir0;
+    C dkf0;
+    point_phase(j0 + q0, a.fdx, a.fdy, tw, ix, iy, iz, dir0, dkf0);
+    const C tyz = PT > 1 ? cmul(tw[a.nx + iy], tw[a.nx + a.ny + iz]) : dkf0;
+#pragma unroll
+    for (int k = 0; k < PT; ++k) {
+      const int q = q0 + k;
+      const C dkf = k == 0 ? dkf0 : cmul(tw[ix + k], tyz);
+      const T sc = (T)a.invvol * (T)((k & 1) ? -dir0 : dir0);
+      const C z = cmul(sb[q], mk<C>(dkf.x * sc, -dkf.y * sc));
+      const T h[2] = {z.x, z.y};
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const T rb = REF ? sT[(size_t)(4 * V + v) * CP + q] : T(0);
+        const double R = (double)residual<CLOS, REF>(h[v], sT[(size_t)v * CP + q],
+                                                     sT[(size_t)(V + v) * CP + q], rb);
+        acc[0] += R * R;                          // cal_rms.cu:18
+        if (gram) {                               // theta30, anderson_cuda.cu:33-39
+          const double d0 = R - (double)sT[(size_t)(2 * V + v) * CP + q];
+          const double d1 = R - (double)sT[(size_t)(3 * V + v) * CP + q];
+          acc[1] += w8[v] * R * d0;
+          acc[2] += w8[v] * R * d1;
+          acc[3] += w8[v] * d0 * d0;
+          acc[4] += w8[v] * d0 * d1;
+          acc[5] += w8[v] * d1 * d1;
+        }
+      }
+    }
+  }
+  fault = __syncthreads_or(fault);
+  if (fault) {
+    // a chunk never arrived: wait (bounded) for the copies still in flight
+    // before the block's shared memory goes away (a chunk already consumed
+    // passes at once); the NaN sums make the finalize stop the loop as
+    // diverged, and the flag makes it an error
+    if (threadIdx.x == 0) {
+      for (int f = i > 0 ? i - 1 : 0; f < fetched; ++f)
+        tma::mbar_wait_bounded(&full[f % kBulkStages], (unsigned)(f / kBulkStages) & 1u,
+                               kBulkWaitPolls);
+      st->fault = 1;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] = __longlong_as_double(0x7ff8000000000000LL);
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[k] = v;
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k) red[wid][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double s = 0.0;
+    for (int w = 0; w < kBulkThreads / 32; ++w) s += red[w][threadIdx.x];
     a.part[(size_t)threadIdx.x * a.nblocks + blockIdx.x] = s;
   }
   __threadfence();
@@ -1247,15 +1604,24 @@ __global__ void __launch_bounds__(kThreads) k_pass_a_pipe(IterArgs<T> a0) {
 // (anderson.cu:35-63) on one thread -- no separate launch, no host sync.
 __device__ void finalize_block(DevState *st, const double *part, int nblocks,
                                double nv_points, double *hist, int hist_cap) {
+  // blocks of any multiple of kThreads threads: threads past the first
+  // kThreads fold their sums into those slots, one group at a time
   __shared__ double red[6][kThreads];
   double s[6] = {0, 0, 0, 0, 0, 0};
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
 #pragma unroll
     for (int k = 0; k < 6; ++k) s[k] += __ldcg(part + (size_t)k * nblocks + b);
+  if (threadIdx.x < kThreads)
 #pragma unroll
-  for (int k = 0; k < 6; ++k) red[k][threadIdx.x] = s[k];
+    for (int k = 0; k < 6; ++k) red[k][threadIdx.x] = s[k];
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+  for (int g = kThreads; g < (int)blockDim.x; g += kThreads) {
+    if ((int)threadIdx.x >= g && (int)threadIdx.x < g + kThreads)
+#pragma unroll
+      for (int k = 0; k < 6; ++k) red[k][threadIdx.x - g] += s[k];
+    __syncthreads();
+  }
+  for (int w = min((int)blockDim.x, kThreads) / 2; w > 0; w >>= 1) {
     if ((int)threadIdx.x < w)
 #pragma unroll
       for (int k = 0; k < 6; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
@@ -1467,13 +1833,29 @@ int grid_ky(const Context &c) {
                           (long long)(c.nx / kW) * (c.nz / 2));
 }
 
+// The fused pass K: the TMA form on 256-point lines when its tensor map
+// (bound to the context's FP32 transform buffer) exists, else the
+// register/shared-memory form.
+template <int V, int E>
+void launch_kspace_y(Context &c, const IterArgs<float> &a) {
+  if constexpr (E == 16) {
+    if (c.ky_map && (const void *)a.buf == (const void *)c.f_buf) {
+      const int tiles = (c.nx / 16) * (c.nz / 2);
+      const int g = wave_blocks_smem(k_kspace_yt<V>, kKyThreads, kKySmem, tiles);
+      k_kspace_yt<V><<<g, kKyThreads, kKySmem, c.stream>>>(a, *c.ky_map);
+      return;
+    }
+  }
+  k_kspace_y<V, E><<<grid_ky<V, E>(c), kW * E, KYLayout<E>::bytes(), c.stream>>>(a);
+}
+
 // One FP32 iteration with the x and y axes of the transforms folded into the
 // passes (single solute, V <= 2, nx = ny = E^2): cuFFT transforms along z.
 template <int V, int CLOS, bool REF, int E>
 void launch_iteration_x(Context &c, const IterArgs<float> &a) {
   k_pass_ax<V, CLOS, REF, E><<<grid_ax<V, CLOS, REF, E>(c), kXThreads, 0, c.stream>>>(a);
   cufftExecC2C(c.plan32z, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_FORWARD);
-  k_kspace_y<V, E><<<grid_ky<V, E>(c), kW * E, KYLayout<E>::bytes(), c.stream>>>(a);
+  launch_kspace_y<V, E>(c, a);
   cufftExecC2C(c.plan32z, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
   k_pass_rx<V, CLOS, REF, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a);
 }
@@ -1492,6 +1874,38 @@ int pipe_a_blocks(const Context &c) {
   constexpr int CP = kThreads * (16 / (int)sizeof(T));
   return wave_blocks_smem(k_pass_a_pipe<T, V, CLOS, REF>, kThreads, pass_r_pipe_smem<T, V>(),
                           (c.n + CP - 1) / CP);
+}
+
+// Blocks of the bulk-copy pass R: one per SM (its stages fill the shared
+// memory), at most the partial-sum slots the context has.
+template <typename T, int V, int CLOS, bool REF>
+int bulk_r_blocks(const Context &c) {
+  const int w = wave_blocks_smem(k_pass_r_bulk<T, V, CLOS, REF>, kBulkThreads, bulk_smem<T, V>(),
+                                 c.nred_blocks);
+  return std::min(w, c.nred_blocks);
+}
+
+// Pass R in the form the context chose: bulk-copy stream, cp.async
+// pipeline, or plain grid-stride.
+template <typename T, int V, int CLOS, bool REF>
+void launch_pass_r(Context &c, const IterArgs<T> &a) {
+  if constexpr (V <= 2) {
+    if (c.bulk_r) {
+      IterArgs<T> ar = a;
+      ar.nblocks = bulk_r_blocks<T, V, CLOS, REF>(c);
+      k_pass_r_bulk<T, V, CLOS, REF><<<dim3(ar.nblocks, c.nb), kBulkThreads, bulk_smem<T, V>(),
+                                       c.stream>>>(ar);
+      return;
+    }
+    if (c.pipe_r) {
+      IterArgs<T> ar = a;
+      ar.nblocks = pipe_r_blocks<T, V, CLOS, REF>(c);
+      k_pass_r_pipe<T, V, CLOS, REF><<<dim3(ar.nblocks, c.nb), kThreads, pass_r_pipe_smem<T, V>(),
+                                       c.stream>>>(ar);
+      return;
+    }
+  }
+  k_pass_r<T, V, CLOS, REF><<<dim3(a.nblocks, c.nb), kThreads, 0, c.stream>>>(a);
 }
 
 template <typename T, int V, int CLOS, bool REF>
@@ -1528,18 +1942,9 @@ void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
   } else {
     cufftExecC2C(plan, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
   }
-  if constexpr (V <= 2) {
-    if (c.pipe_r) {
-      IterArgs<T> ar = a;
-      ar.nblocks = pipe_r_blocks<T, V, CLOS, REF>(c);
-      k_pass_r_pipe<T, V, CLOS, REF><<<dim3(ar.nblocks, c.nb), kThreads, pass_r_pipe_smem<T, V>(),
-                                       c.stream>>>(ar);
-      (void)sizeof(C);
-      return;
-    }
-  }
-  k_pass_r<T, V, CLOS, REF><<<br, kThreads, 0, c.stream>>>(a);
+  launch_pass_r<T, V, CLOS, REF>(c, a);
   (void)sizeof(C);
+  (void)br;
 }
 
 template <typename T>
@@ -1555,6 +1960,7 @@ IterArgs<T> make_args(Context &c, bool fp64) {
   a.count = c.d_count;
   a.hist = c.nb == 1 ? c.d_hist : nullptr;
   a.xroots = c.d_xroots;
+  a.fkt = c.d_fkt;
   a.hist_cap = c.hist_cap;
   (void)fp64;
   return a;
@@ -1970,6 +2376,11 @@ int solve_v(Context &c, int chargeup) {
     total32 = std::max(total32, x.total32);
   }
   bodies = fs[0].bodies;
+  for (const DevState &x : fs)
+    if (x.fault) {
+      c.err = "a device-side wait gave up: a bulk or tile copy never arrived";
+      status = RISM3D_CUDA_ERROR;
+    }
   c.launches += 4 * bodies;
   c.res.rms = fs[0].rms;
   if (nb > 1) {
@@ -1997,8 +2408,7 @@ void time_fused(Context &c, const IterArgs<float> &a, int which, int reps) {
                                                 c.stream>>>(a); break;
       case 13: k_pass_ax<V, CLOS, true, E><<<grid_ax<V, CLOS, true, E>(c), kXThreads, 0,
                                                c.stream>>>(a); break;
-      case 11: k_kspace_y<V, E><<<grid_ky<V, E>(c), kW * E, KYLayout<E>::bytes(),
-                                  c.stream>>>(a); break;
+      case 11: launch_kspace_y<V, E>(c, a); break;
       case 15: k_pass_rx<V, CLOS, true, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a); break;
       default: k_pass_rx<V, CLOS, false, E><<<a.nblocks, kXThreads, 0, c.stream>>>(a); break;
     }
@@ -2068,30 +2478,8 @@ int time_kernel_t(Context &c, int which, int reps, double *ms) {
         k_pass_a<T, V, CLOS, true><<<bar, kThreads, 0, c.stream>>>(a);
         break;
       case 1: case 11: k_kspace<T, V><<<bk, kThreads, 0, c.stream>>>(a); break;
-      case 15:
-        if constexpr (V <= 2) {
-          if (c.pipe_r) {
-            IterArgs<T> ar = a;
-            ar.nblocks = pipe_r_blocks<T, V, CLOS, true>(c);
-            k_pass_r_pipe<T, V, CLOS, true><<<ar.nblocks, kThreads, pass_r_pipe_smem<T, V>(),
-                                              c.stream>>>(ar);
-            break;
-          }
-        }
-        k_pass_r<T, V, CLOS, true><<<a.nblocks, kThreads, 0, c.stream>>>(a);
-        break;
-      default:
-        if constexpr (V <= 2) {
-          if (c.pipe_r) {
-            IterArgs<T> ar = a;
-            ar.nblocks = pipe_r_blocks<T, V, CLOS, false>(c);
-            k_pass_r_pipe<T, V, CLOS, false><<<ar.nblocks, kThreads, pass_r_pipe_smem<T, V>(),
-                                               c.stream>>>(ar);
-            break;
-          }
-        }
-        k_pass_r<T, V, CLOS, false><<<a.nblocks, kThreads, 0, c.stream>>>(a);
-        break;
+      case 15: launch_pass_r<T, V, CLOS, true>(c, a); break;
+      default: launch_pass_r<T, V, CLOS, false>(c, a); break;
     }
   }
   cudaEventRecord(e1, c.stream);
@@ -2140,14 +2528,91 @@ cudaError_t pipe_r_attrs() {
   return e;
 }
 
+template <typename T, int V>
+cudaError_t bulk_r_attrs() {
+  const int b = (int)bulk_smem<T, V>();
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(k_pass_r_bulk<T, V, 0, false>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_r_bulk<T, V, 1, false>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_r_bulk<T, V, 0, true>, at, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pass_r_bulk<T, V, 1, true>, at, b);
+  return e;
+}
+
+// Pass R for natv <= 2: the cp.async pipeline, or with RISM3D_BULK_R=1 the
+// bulk-copy stream (every stream's chunk offset must be 16-byte aligned: N
+// a multiple of 4).  RISM3D_NO_PIPE_R=1 keeps the plain grid-stride pass.
 int setup_pipe_r(Context &c) {
   c.pipe_r = false;
+  c.bulk_r = false;
   const char *off = getenv("RISM3D_NO_PIPE_R");
   if ((off && off[0] == '1') || c.natv > 2) return RISM3D_OK;
   cudaError_t e = c.natv == 1 ? pipe_r_attrs<double, 1>() : pipe_r_attrs<double, 2>();
   if (e == cudaSuccess) e = c.natv == 1 ? pipe_r_attrs<float, 1>() : pipe_r_attrs<float, 2>();
   if (!cuda_ok(c, e, "pass R attributes")) return RISM3D_CUDA_ERROR;
   c.pipe_r = true;
+  const char *bulk = getenv("RISM3D_BULK_R");
+  if (!bulk || bulk[0] != '1' || c.n % 4 != 0) return RISM3D_OK;
+  e = c.natv == 1 ? bulk_r_attrs<double, 1>() : bulk_r_attrs<double, 2>();
+  if (e == cudaSuccess) e = c.natv == 1 ? bulk_r_attrs<float, 1>() : bulk_r_attrs<float, 2>();
+  if (!cuda_ok(c, e, "bulk pass R attributes")) return RISM3D_CUDA_ERROR;
+  c.bulk_r = true;
+  return RISM3D_OK;
+}
+
+// TMA form of the fused pass K (nx = ny = 256): a tensor map over the FP32
+// transform buffer seen as (2 nx floats) x (ny nz rows), boxes of 16
+// complex columns x 256 rows with the 128B swizzle, and the [kz][kx][ky]
+// FP32 copy of beta fk.  RISM3D_KY_TMA=0 keeps the register/shared-memory form.
+int setup_kspace_tma(Context &c) {
+  const char *off = getenv("RISM3D_KY_TMA");
+  if (off && off[0] == '0') return RISM3D_OK;
+  typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+  if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault,
+                                       &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn) {
+    cudaGetLastError();
+    return RISM3D_OK;                            // no TMA entry point: the other form
+  }
+  cudaError_t e = cudaFuncSetAttribute(k_kspace_yt<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kKySmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_kspace_yt<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kKySmem);
+  if (!cuda_ok(c, e, "TMA pass K attributes")) return RISM3D_CUDA_ERROR;
+  CUtensorMap *map = new CUtensorMap;
+  const cuuint64_t dims[2] = {(cuuint64_t)2 * c.nx, (cuuint64_t)c.ny * c.nz};
+  const cuuint64_t strides[1] = {(cuuint64_t)2 * c.nx * sizeof(float)};
+  const cuuint32_t box[2] = {32, 256}, estr[2] = {1, 1};
+  const CUresult r = ((EncodeTiled)fn)(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, c.f_buf, dims,
+                                       strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                       CU_TENSOR_MAP_SWIZZLE_128B,
+                                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    delete map;
+    c.err = "cuTensorMapEncodeTiled failed: " + std::to_string((int)r);
+    return RISM3D_CUDA_ERROR;
+  }
+  if (!cuda_ok(c, cudaMalloc(&c.d_fkt, sizeof(float2) * (size_t)(c.n / 2)), "alloc fk columns")) {
+    delete map;
+    return RISM3D_CUDA_ERROR;
+  }
+  c.ky_map = map;
+  return RISM3D_OK;
+}
+
+int fused_fk_columns(Context &c) {
+  if (!c.d_fkt) return RISM3D_OK;
+  k_fk_columns<<<dim3((unsigned)(c.nx + 31) / 32, (unsigned)(c.ny + 31) / 32, (unsigned)c.nz / 2),
+                 dim3(32, 8), 0, c.stream>>>(c.nx, c.ny, c.d_fkh, c.d_fkt);
+  if (!cuda_ok(c, cudaGetLastError(), "k_fk_columns")) return RISM3D_CUDA_ERROR;
+  c.launches += 1;
   return RISM3D_OK;
 }
 
@@ -2172,6 +2637,10 @@ int setup_fused_axes(Context &c) {
       e = cudaFuncSetAttribute(k_kspace_y<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ks);
   }
   if (!cuda_ok(c, e, "fused-axis kernel attributes")) return RISM3D_CUDA_ERROR;
+  if (c.nx == 256) {
+    const int rc = setup_kspace_tma(c);
+    if (rc != RISM3D_OK) return rc;
+  }
   std::vector<float2> roots(c.nx);
   for (int m = 0; m < c.nx; ++m) {
     const double ang = 2.0 * kPi * m / c.nx;

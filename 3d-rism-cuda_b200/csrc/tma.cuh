@@ -1,0 +1,117 @@
+// Tensor-memory-accelerator (TMA) copies and the shared-memory transaction
+// barriers that track them (sm_90+ PTX, used on sm_100a).
+//
+// A tile or bulk load is issued by one thread: it names the source (a tensor
+// map encoded on the host with the global array's shape, strides, box and
+// swizzle, or a plain 16-byte-aligned address and size), the destination in
+// shared memory and an mbarrier in shared memory that counts the bytes as
+// they land.  Consumers wait on the barrier's phase parity.  Tile stores read
+// shared memory asynchronously and are tracked by bulk groups (commit /
+// wait_group).  Shared-memory writes of ordinary threads become visible to
+// the TMA unit only after fence.proxy.async.
+//
+// No load here uses cluster multicast: every CTA fetches its own data.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rism3d {
+namespace tma {
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+
+// make the initialised barriers visible to the async proxy (TMA)
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// one arrival that also announces `bytes` of transactions for this phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n"
+      " .reg .pred p;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for the phase with the given parity to complete, at most `limit`
+// polls; false when the limit ran out (the caller reports it and stops).
+// A phase that completed earlier (the barrier has moved on) passes at once.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, long long limit) {
+  for (long long i = 0; i < limit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// 2D tile load global -> shared, completion counted on `bar`
+__device__ __forceinline__ void load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x,
+                                        int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];\n" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_addr(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// 1D bulk copy global -> shared: both addresses 16-byte aligned, `bytes` a
+// multiple of 16; completion counted on `bar`
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// 2D tile store shared -> global (bulk-group completion)
+__device__ __forceinline__ void store_2d(const CUtensorMap *map, const void *src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%2, %3}], [%1];\n" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(smem_addr(src)), "r"(x), "r"(y)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+
+// all but the newest N store groups have finished reading shared memory
+template <int N> __device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;\n" ::"n"(N) : "memory");
+}
+
+// all but the newest N store groups are complete (writes performed)
+template <int N> __device__ __forceinline__ void bulk_wait() {
+  asm volatile("cp.async.bulk.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// order this thread's generic-proxy shared-memory accesses before later
+// async-proxy (TMA) accesses
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+}  // namespace tma
+}  // namespace rism3d

@@ -94,9 +94,11 @@ def test_fused_axis_passes_match_the_cufft_path(name):
     """The FP32 phases of a mixed solve with the x and y axes of the
     transforms folded into the passes (RISM3D_XFFT=1: cuFFT along z only;
     64^3 and 256^3 cells) against the same solve through 3D cuFFT
-    transforms: mu_ex and PMV within rounding of FP32 transforms, step
-    counts within 10 (the different FP32 rounding moves the hand-over from
-    the FP32 bulk to the refinement by a few steps)."""
+    transforms: mu_ex and PMV within rounding of FP32 transforms.  The step
+    counts agree to 10 %: the FP32 rounding of the bulk (and the order of
+    its FP64 partial sums) moves where the bulk hands over to the
+    refinement, and the AN2 trajectory after that point by tens of steps
+    at 256^3, while the converged fixed point stays the same."""
     import os
     import rism3d_b200 as R
     case, _, _ = load_case(name)
@@ -110,6 +112,42 @@ def test_fused_axis_passes_match_the_cufft_path(name):
         del os.environ["RISM3D_XFFT"]
     r1 = s1.solve()
     s1.close()
-    assert abs(r1["iterations"] - r0["iterations"]) <= 10, (r1["iterations"], r0["iterations"])
     assert abs(r1["sfe_sc"] - r0["sfe_sc"]) < 0.1 * MU_TOL
     assert abs(r1["pmv"] - r0["pmv"]) < 1e-4
+    assert abs(r1["iterations"] - r0["iterations"]) <= max(10, 0.1 * r0["iterations"]), \
+        (r1["iterations"], r0["iterations"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pass_r_forms_agree(precision):
+    """Pass R (residual, rms and the AN2 Gram sums) in its three forms on the
+    same 64^3 solve: the plain grid-stride kernel (RISM3D_NO_PIPE_R=1), the
+    cp.async pipeline (RISM3D_BULK_R=0) and the bulk-copy stream
+    (RISM3D_BULK_R=1).  Only the order of the FP64 partial sums differs, so
+    FP64 solves take the same steps to the same mu_ex (1e-6 J/mol); the
+    mixed solves agree within the FP32 rounding of the bulk."""
+    import os
+    import rism3d_b200 as R
+    case, _, _ = load_case("cfg0_chain12")
+    prec = R.FP64 if precision == "fp64" else R.MIXED
+    out = []
+    for env in ({"RISM3D_NO_PIPE_R": "1"}, {"RISM3D_BULK_R": "0"}, {"RISM3D_BULK_R": "1"}):
+        old = {k: os.environ.get(k) for k in env}
+        os.environ.update(env)
+        try:
+            s = product_solver(case, precision=prec)
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    del os.environ[k]
+                else:
+                    os.environ[k] = v
+        out.append(s.solve())
+        s.close()
+    for r in out[1:]:
+        if precision == "fp64":
+            assert r["iterations"] == out[0]["iterations"]
+            assert abs(r["sfe_sc"] - out[0]["sfe_sc"]) < 1e-6
+        else:
+            assert abs(r["sfe_sc"] - out[0]["sfe_sc"]) < 0.1 * MU_TOL
+            assert abs(r["iterations"] - out[0]["iterations"]) <= max(10, 0.1 * out[0]["iterations"])
