@@ -81,6 +81,8 @@ void free_device(Context &c) {
   c.d_obs = nullptr;
   c.d_atom_part = nullptr; c.chi.d_coef = nullptr; c.natom_part_cap = 0;
   c.d_xs = nullptr; c.nxs = 0;
+  if (c.d_xs32) cudaFree(c.d_xs32);
+  c.d_xs32 = nullptr;
   c.d_atom_off = c.d_atom_cnt = nullptr;
   if (c.h_state) cudaFreeHost(c.h_state);
   c.h_state = nullptr;

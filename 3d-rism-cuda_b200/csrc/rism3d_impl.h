@@ -141,6 +141,7 @@ struct Context {
   // cubic cells: chi_ab tabulated per s = ox^2 + oy^2 + oz^2 (odd o_d), so
   // |k| = (pi/L) sqrt(s) and the table index is (s - 3) / 8
   double *d_xs = nullptr;    // [nidx][V*V] or null (general cells: spline)
+  float *d_xs32 = nullptr;   // the same in FP32 for the FP32 passes
   int nxs = 0;
   std::vector<double> xvv_host;
   int ntab = 0;

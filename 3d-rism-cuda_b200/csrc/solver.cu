@@ -63,6 +63,7 @@ struct IterArgs {
   int nx, ny, nz;
   FastDiv fdx, fdy;         // division by nx and ny
   const double *xs;         // chi table per odd-square sum (cubic cells) or null
+  const float *xs32;        // the same table in FP32 (read by the FP32 passes)
   typename Cx<T>::t *buf;   // [P][N]
   T *t, *U, *Y, *RP;        // t, U: [V][N]; Y, RP: [2][V][N]
   const T *R0;              // refinement: base residual [V][N] (t = d, U = x0)
@@ -429,31 +430,49 @@ __device__ __forceinline__ void kspace_pair_fk(const IterArgs<T> &a, double2 fk,
   const int dir = ((ix + iy + iz) & 1) ? -1 : 1;
   // unpack the site pairs and finish the forward transform
   // (timeirvol * dv, fft3d.cu:32) and subtract q cf fk (mqvfk)
+  // (in the working precision T: the FP32 passes round F to FP32 anyway)
   C F[V];
   const T sc = (T)(a.dv * 0.5 * dir);
+  const T fx = (T)fk.x, fy = (T)fk.y;
 #pragma unroll
   for (int p = 0; p < P; ++p) {
-    const double qa = sp->qcf[2 * p];
-    F[2 * p] = mk<C>(sc * (y[p].x - ym[p].x) - qa * fk.x, sc * (y[p].y + ym[p].y) - qa * fk.y);
+    const T qa = (T)sp->qcf[2 * p];
+    F[2 * p] = mk<C>(sc * (y[p].x - ym[p].x) - qa * fx, sc * (y[p].y + ym[p].y) - qa * fy);
     if (2 * p + 1 < V) {
-      const double qb = sp->qcf[2 * p + 1];
-      F[2 * p + 1] = mk<C>(sc * (y[p].y - ym[p].y) - qb * fk.x, -sc * (y[p].x + ym[p].x) - qb * fk.y);
+      const T qb = (T)sp->qcf[2 * p + 1];
+      F[2 * p + 1] = mk<C>(sc * (y[p].y - ym[p].y) - qb * fx, -sc * (y[p].x + ym[p].x) - qb * fy);
     }
   }
-  // chi_ab(|k|) (solvent_spline.cu:36-47, applied per point by oz)
-  double X[V * V];
+  // chi_ab(|k|) (solvent_spline.cu:36-47, applied per point by oz), in T
+  T X[V * V];
   if (a.xs) {
     // cubic cell: |k| = (pi/L) sqrt(s), s = sum of three odd squares
     const int ox = 2 * ix - a.nx + 1, oy = 2 * iy - a.ny + 1, oz = 2 * iz - a.nz + 1;
     const unsigned sq = (unsigned)(ox * ox + oy * oy + oz * oz);
-    const double2 *xr = reinterpret_cast<const double2 *>(a.xs + (size_t)((sq - 3u) >> 3) * V * V);
+    const size_t row = (size_t)((sq - 3u) >> 3) * V * V;
+    if constexpr (sizeof(T) == 4 && V * V % 4 == 0) {
+      const float4 *xr = reinterpret_cast<const float4 *>(a.xs32 + row);   // 16-byte rows
 #pragma unroll
-    for (int ab = 0; ab < V * V / 2; ++ab) {
-      const double2 q = xr[ab];
-      X[2 * ab] = q.x;
-      X[2 * ab + 1] = q.y;
+      for (int ab = 0; ab < V * V / 4; ++ab) {
+        const float4 q = xr[ab];
+        X[4 * ab] = q.x;
+        X[4 * ab + 1] = q.y;
+        X[4 * ab + 2] = q.z;
+        X[4 * ab + 3] = q.w;
+      }
+    } else if constexpr (sizeof(T) == 4) {
+#pragma unroll
+      for (int ab = 0; ab < V * V; ++ab) X[ab] = a.xs32[row + ab];
+    } else {
+      const double2 *xr = reinterpret_cast<const double2 *>(a.xs + row);
+#pragma unroll
+      for (int ab = 0; ab < V * V / 2; ++ab) {
+        const double2 q = xr[ab];
+        X[2 * ab] = (T)q.x;
+        X[2 * ab + 1] = (T)q.y;
+      }
+      if (V * V % 2) X[V * V - 1] = (T)a.xs[row + V * V - 1];
     }
-    if (V * V % 2) X[V * V - 1] = a.xs[(size_t)((sq - 3u) >> 3) * V * V + V * V - 1];
   } else {
     // general cell: natural spline on knots k_i = dk (i+1) with the
     // bisection semantics of splint.cc:9-16 on uniform knots
@@ -470,7 +489,7 @@ __device__ __forceinline__ void kspace_pair_fk(const IterArgs<T> &a, double2 fk,
 #pragma unroll
     for (int ab = 0; ab < V * V; ++ab) {
       const double2 lo = cf[2 * ab], hi2 = cf[2 * ab + 1];
-      X[ab] = ((hi2.y * tt + hi2.x) * tt + lo.y) * tt + lo.x;
+      X[ab] = (T)(((hi2.y * tt + hi2.x) * tt + lo.y) * tt + lo.x);
     }
   }
   C H[V];
@@ -479,7 +498,7 @@ __device__ __forceinline__ void kspace_pair_fk(const IterArgs<T> &a, double2 fk,
     T hr = 0, hi = 0;
 #pragma unroll
     for (int vb = 0; vb < V; ++vb) {
-      const T x = (T)X[va * V + vb];
+      const T x = X[va * V + vb];
       hr += F[vb].x * x;                       // oz, calculate_cuda.cu:44-58
       hi += F[vb].y * x;
     }
@@ -1910,7 +1929,11 @@ void launch_pass_r(Context &c, const IterArgs<T> &a) {
 
 template <typename T, int V, int CLOS, bool REF>
 void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
-  if constexpr (sizeof(T) == 4 && V <= 2) {
+  // the fused-axis passes run the plain FP32 bulk; the refinement form
+  // (which also streams R0) stays on the 3D transforms, where its pipelined
+  // passes are faster.  Every phase starts without a pending update (its
+  // first pass A reads no transform), so the two forms never share a buffer.
+  if constexpr (sizeof(T) == 4 && V <= 2 && !REF) {
     if (c.xfused) {
       if (c.nx == 256) launch_iteration_x<V, CLOS, REF, 16>(c, a);
       else launch_iteration_x<V, CLOS, REF, 8>(c, a);
@@ -1953,6 +1976,7 @@ IterArgs<T> make_args(Context &c, bool fp64) {
   a.n = c.n; a.nx = c.nx; a.ny = c.ny; a.nz = c.nz;
   a.fdx = FastDiv((unsigned)c.nx); a.fdy = FastDiv((unsigned)c.ny);
   a.xs = c.d_xs;
+  a.xs32 = c.d_xs32;
   a.invvol = 1.0 / c.vol; a.dv = c.dv;
   a.fkh = c.d_fkh; a.chi = c.chi.d_coef; a.ntab = c.chi.ntab; a.dk = c.chi.dk;
   a.bx = c.prm.box[0]; a.by = c.prm.box[1]; a.bz = c.prm.box[2];
@@ -2749,6 +2773,7 @@ int upload_chi(Context &c) {
   // Cubic cells: evaluate the spline once per distinct |k|^2 (the sorted
   // unique-|k| table of initialize_g.cu:31-43, indexed directly).
   if (c.d_xs) { cudaFree(c.d_xs); c.d_xs = nullptr; c.nxs = 0; }
+  if (c.d_xs32) { cudaFree(c.d_xs32); c.d_xs32 = nullptr; }
   if (c.nx == c.ny && c.nx == c.nz && c.prm.box[0] == c.prm.box[1] &&
       c.prm.box[0] == c.prm.box[2]) {
     const long long nm = c.nx - 1;
@@ -2767,8 +2792,11 @@ int upload_chi(Context &c) {
         xs[(size_t)idx * V * V + ab] = ((o[3] * t + o[2]) * t + o[1]) * t + o[0];
       }
     }
+    std::vector<float> xs32(xs.begin(), xs.end());     // the FP32 passes' copy
     if (!cuda_ok(c, cudaMalloc(&c.d_xs, sizeof(double) * xs.size()), "chi table alloc") ||
-        !cuda_ok(c, cudaMemcpy(c.d_xs, xs.data(), sizeof(double) * xs.size(), cudaMemcpyHostToDevice), "chi table copy"))
+        !cuda_ok(c, cudaMemcpy(c.d_xs, xs.data(), sizeof(double) * xs.size(), cudaMemcpyHostToDevice), "chi table copy") ||
+        !cuda_ok(c, cudaMalloc(&c.d_xs32, sizeof(float) * xs32.size()), "chi table alloc") ||
+        !cuda_ok(c, cudaMemcpy(c.d_xs32, xs32.data(), sizeof(float) * xs32.size(), cudaMemcpyHostToDevice), "chi table copy"))
       return RISM3D_CUDA_ERROR;
     c.nxs = nidx;
   }
