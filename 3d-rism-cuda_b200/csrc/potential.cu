@@ -35,6 +35,34 @@ struct SiteLJ {
   double eps[kMaxSites];
 };
 
+// e^-x in FP64 for 0 <= x <= 40 (the e^-r factor of the split Coulomb
+// terms), branch-free: Cody-Waite range reduction x = k ln2 + f with k the
+// integer nearest x / ln2, so |f| <= ln2 / 2 (ln2 split into a 39-bit head,
+// exact in k ln2 for |k| < 2^13, and the rest), then e^-f from its Taylor
+// series to degree 13 (truncation below 5e-18 relative for |f| <= ln2 / 2),
+// and the factor 2^-k written into the exponent field.
+__device__ __forceinline__ double exp_neg(double x) {
+  constexpr double kLn2Hi = 0.6931471805592082, kLn2Lo = 7.371002565167799e-13;
+  constexpr double kInvLn2 = 1.4426950408889634;
+  const double k = rint(x * kInvLn2);
+  const double g = -fma(-k, kLn2Lo, fma(-k, kLn2Hi, x));      // -f
+  double p = 1.0 / 6227020800.0;                                // 1/13!
+  p = fma(p, g, 1.0 / 479001600.0);
+  p = fma(p, g, 1.0 / 39916800.0);
+  p = fma(p, g, 1.0 / 3628800.0);
+  p = fma(p, g, 1.0 / 362880.0);
+  p = fma(p, g, 1.0 / 40320.0);
+  p = fma(p, g, 1.0 / 5040.0);
+  p = fma(p, g, 1.0 / 720.0);
+  p = fma(p, g, 1.0 / 120.0);
+  p = fma(p, g, 1.0 / 24.0);
+  p = fma(p, g, 1.0 / 6.0);
+  p = fma(p, g, 0.5);
+  p = fma(p, g, 1.0);
+  p = fma(p, g, 1.0);
+  return p * __longlong_as_double((long long)(1023 - (int)k) << 52);
+}
+
 // Real-space grids.  A block covers a brick of 8 x 8 x 8 grid points and
 // each warp a compact 8 x 4 x 2 sub-brick (4 x 2 x 1 A at 0.5 A spacing);
 // each thread owns two neighbouring points along x (the atom tile read once
@@ -144,9 +172,9 @@ k_potential_r(int nx, int ny, int nz, int bricks_x, int bricks_y, double drx, do
         if (ra >= 1.0e-5) {                 // cal_Coulomb.cu:114-120
           const double qr = at.w * ri;
           if (ra < (MIX ? 20.0 : 40.0)) {
-            const double em1 = expm1(-ra);  // e^-r - 1
-            afr[k] -= qr * em1;             // q (1 - e^-r) / r
-            aes[k] += qr * (em1 + 1.0);     // q e^-r / r
+            const double er = exp_neg(ra);  // e^-r
+            afr[k] += qr * (1.0 - er);      // q (1 - e^-r) / r
+            aes[k] += qr * er;              // q e^-r / r
           } else if (MIX && ra < 40.0) {
             const double es = qr * (double)expf(-(float)ra);
             afr[k] += qr - es;
