@@ -104,6 +104,10 @@ void free_device(Context &c) {
   c.xfused = false;
   if (c.d_xroots) cudaFree(c.d_xroots);
   c.d_xroots = nullptr;
+  if (c.f_Ydm) cudaFree(c.f_Ydm);
+  if (c.f_RPdm) cudaFree(c.f_RPdm);
+  c.f_Ydm = c.f_RPdm = nullptr;
+  c.dm_depth = 0;
   if (c.d_fkt) cudaFree(c.d_fkt);
   c.d_fkt = nullptr;
   delete c.ky_map;
@@ -203,6 +207,18 @@ static int alloc_state(Context &c) {
   if (mixed) {
     const int rc = setup_fused_axes(c);
     if (rc != RISM3D_OK) return rc;
+  }
+  // depth-M Anderson for the plain FP32 bulk (opt-in, single solutes)
+  c.dm_depth = 0;
+  if (const char *e = getenv("RISM3D_MDIIS")) {
+    const int M = atoi(e);
+    if (mixed && c.nb == 1 && M >= 2 && M <= 6) {
+      const size_t b = sizeof(float) * (size_t)M * V * n;
+      if (!A((void **)&c.f_Ydm, b, "alloc MDIIS history") ||
+          !A((void **)&c.f_RPdm, b, "alloc MDIIS history"))
+        return RISM3D_CUDA_ERROR;
+      c.dm_depth = M;
+    }
   }
   {
     const int rc = setup_pipe_r(c);

@@ -54,6 +54,10 @@ struct DevState {
   double s1, s2;   // AN2 coefficients for the next update
   double rms;
   double sums[6];  // sum R^2, c0, c1, a00, a01, a11 of the last pass R
+  int dm_fill;     // depth-M Anderson (opt-in): history slots filled,
+  int dm_last;     // the slot written last (-1: none yet),
+  int dm_use;      // and the slots the next update mixes
+  double sdm[8];   // its coefficients per slot (bias included)
 };
 
 // 1/sqrt(x) for x > 0: the FP64 hardware approximation (rsqrt.approx.f64,
@@ -200,6 +204,10 @@ struct Context {
   // FP32 passes with the x and y axes of the transforms folded in (single
   // solutes, natv <= 2, nx = ny = 64 or 256): cuFFT then transforms along z
   // only (plan32z), with the x-line roots of unity in d_xroots
+  // depth-M Anderson for the plain FP32 bulk (opt-in RISM3D_MDIIS=M):
+  // history [M][V][N] of Y = t + m R and of R
+  int dm_depth = 0;
+  float *f_Ydm = nullptr, *f_RPdm = nullptr;
   bool pipe_r = false;       // pass R as the cp.async pipeline (natv <= 2)
   bool bulk_r = false;       // pass R as the bulk-copy (cp.async.bulk) stream
   bool xfused = false;

@@ -1682,6 +1682,252 @@ __device__ void finalize_block(DevState *st, const double *part, int nblocks,
   if (st->iter >= st->maxstep) st->done = 3;   // iterate.cu:51 loop bound
 }
 
+// -------------------------------------------- depth-M Anderson (opt-in)
+// RISM3D_MDIIS=M (2..kDmMax): the plain FP32 bulk of a mixed single-solute
+// solve mixes the last M history entries instead of AN2's two.  Slot i holds
+// Y_i = t_i + m R_i and R_i, written round-robin.  Pass R forms R^2,
+// c_i = <R, d_i> and a_ij = <d_i, d_j> (d_i = R - R_i, weights 1/rho_v) over
+// the filled slots; the finalize solves a s = c in FP64 and adds the AN2
+// bias mp to the newest slot; pass A applies t = y + sum_i s_i (Y_i - y),
+// y = t + m R.  With M = 2 this is AN2's update (anderson.cu:35-63), and the
+// elimination below runs in the order of the reference's 2 x 2 solve
+// (leg, anderson.cu:87-112).  Sums: [0] R^2, [1 + i] c_i, [1 + kDmMax + tri]
+// a_ij (packed upper triangle).
+constexpr int kDmMax = 6;
+constexpr int kDmSums = 1 + kDmMax + kDmMax * (kDmMax + 1) / 2;
+__host__ __device__ constexpr int dm_tri(int i, int j) {   // i <= j
+  return i * kDmMax - i * (i - 1) / 2 + (j - i);
+}
+
+template <int V, int CLOS>
+__global__ void __launch_bounds__(kThreads) k_pass_a_dm(IterArgs<float> a) {
+  constexpr int P = (V + 1) / 2;
+  const DevState *st = a.st;
+  const int done = st->done, mode = st->mode, slot = st->upd_slot, use = st->dm_use;
+  if (done && (st->after_done != 0 || done != 3 || mode == 0)) return;
+  const float m = (float)st->m;
+  float s[kDmMax];
+#pragma unroll
+  for (int i = 0; i < kDmMax; ++i) s[i] = i < use ? (float)st->sdm[i] : 0.0f;
+  const long long n = a.n;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    int ix, iy, iz, dir;
+    float2 dkf;
+    point_phase(j, a.fdx, a.fdy, a.tw, ix, iy, iz, dir, dkf);
+    float h[2 * P];
+    if (mode != 0) {
+      const float sc = (float)a.invvol * (float)dir;          // timekb, fft3d.cu:52-60
+      const float2 w = make_float2(dkf.x * sc, -dkf.y * sc);
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const float2 z = cmul(a.buf[(size_t)p * n + j], w);
+        h[2 * p] = z.x;
+        h[2 * p + 1] = z.y;
+      }
+    }
+    float c[2 * P];
+#pragma unroll
+    for (int v = 0; v < 2 * P; ++v) c[v] = 0.0f;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const size_t iv = (size_t)v * n + j;
+      const float tv = a.t[iv], Uv = a.U[iv];
+      float tn = tv;
+      if (mode != 0) {
+        const float R = residual<CLOS, false>(h[v], tv, Uv, 0.0f);
+        const float y = tv + m * R;
+        if (mode == 1) {
+          tn = tv + R;                                          // newdt0 (Picard)
+        } else {
+          tn = y;
+#pragma unroll
+          for (int i = 0; i < kDmMax; ++i)
+            if (i < use) tn += s[i] * (a.Y[(size_t)i * V * n + iv] - y);
+        }
+        a.Y[(size_t)slot * V * n + iv] = y;
+        a.RP[(size_t)slot * V * n + iv] = R;
+        a.t[iv] = tn;
+      }
+      c[v] = cfun<CLOS, false>(tn, Uv);
+    }
+    if (done) continue;                          // the pending update only
+    const float2 wf = make_float2(dkf.x * dir, dkf.y * dir);   // timekf, fft3d.cu:41-49
+#pragma unroll
+    for (int p = 0; p < P; ++p) a.buf[(size_t)p * n + j] = cmul(make_float2(c[2 * p], c[2 * p + 1]), wf);
+  }
+}
+
+// The last block of k_pass_r_dm: fixed-order reduction of the block sums,
+// the stopping tests of finalize_block, then the Picard step or the depth-M
+// solve, and the slot the next pass A writes.
+__device__ void finalize_dm(DevState *st, const double *part, int nblocks, double nv_points,
+                            double *hist, int hist_cap, int M) {
+  __shared__ double tot[kDmSums];
+  __shared__ double wsum[32];
+  for (int k = 0; k < kDmSums; ++k) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+      s += __ldcg(part + (size_t)k * nblocks + b);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += wsum[w];
+      tot[k] = t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  st->sums[0] = tot[0];
+  const double rms = sqrt(tot[0] / nv_points);
+  st->rms = rms;
+  if (st->measure) return;
+  st->iter += 1;
+  if (hist && st->iter <= hist_cap) hist[st->iter - 1] = rms;  // iterate.cu:63 output
+  if (!isfinite(rms)) { st->done = 2; st->mode = 0; return; }  // iterate.cu:54-57
+  if (rms <= st->conv) { st->done = 1; st->mode = 0; return; } // :58-59
+  if (st->watch) {
+    if (rms < 0.9 * st->best) { st->best = rms; st->since = 0; }
+    else if (++st->since > 30) { st->done = 4; st->mode = 0; return; }
+  }
+  const int fill = st->dm_fill;
+  if (st->count > 0 || fill < 1) {                             // anderson.cu:43-49
+    if (st->count > 0) st->count -= 1;
+    st->mode = 1;
+    st->dm_use = 0;
+  } else {
+    // a s = c over the filled slots: each pivot row normalised, then
+    // eliminated from the rows below, then back substitution
+    double A[kDmMax][kDmMax], b[kDmMax];
+    for (int i = 0; i < fill; ++i) {
+      b[i] = tot[1 + i];
+      for (int j = 0; j < fill; ++j)
+        A[i][j] = tot[1 + kDmMax + (i <= j ? dm_tri(i, j) : dm_tri(j, i))];
+    }
+    for (int i = 0; i < fill; ++i) {
+      const double p = A[i][i];
+      for (int j = i + 1; j < fill; ++j) A[i][j] /= p;
+      b[i] /= p;
+      for (int k = i + 1; k < fill; ++k) {
+        const double f = A[k][i];
+        for (int j = i + 1; j < fill; ++j) A[k][j] -= f * A[i][j];
+        b[k] -= f * b[i];
+      }
+    }
+    for (int i = fill - 1; i >= 0; --i)
+      for (int j = i + 1; j < fill; ++j) b[i] -= A[i][j] * b[j];
+    for (int i = 0; i < kDmMax; ++i)
+      st->sdm[i] = i < fill ? b[i] + (i == st->dm_last ? st->mp : 0.0) : 0.0;
+    st->dm_use = fill;
+    st->mode = 2;
+  }
+  const int next = (st->dm_last + 1) % M;                      // round-robin slots
+  st->upd_slot = next;
+  st->dm_last = next;
+  st->dm_fill = fill < M ? fill + 1 : M;
+  if (st->iter >= st->maxstep) st->done = 3;   // iterate.cu:51 loop bound
+}
+
+template <int V, int CLOS>
+__global__ void __launch_bounds__(kThreads) k_pass_r_dm(IterArgs<float> a, int M) {
+  constexpr int P = (V + 1) / 2;
+  __shared__ double red[kThreads / 32][kDmSums];
+  __shared__ bool last;
+  DevState *st = a.st;
+  if (st->done) {                                // loop stopped: count idle cycles
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->after_done += 1;
+    return;
+  }
+  const bool gram = st->count <= 0;
+  const int fill = st->dm_fill;
+  const long long n = a.n;
+  double w8[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) w8[v] = a.sp->irho[v];
+  double acc[kDmSums];
+#pragma unroll
+  for (int k = 0; k < kDmSums; ++k) acc[k] = 0.0;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    int ix, iy, iz, dir;
+    float2 dkf;
+    point_phase(j, a.fdx, a.fdy, a.tw, ix, iy, iz, dir, dkf);
+    const float sc = (float)a.invvol * (float)dir;
+    const float2 w = make_float2(dkf.x * sc, -dkf.y * sc);
+    float h[2 * P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const float2 z = cmul(a.buf[(size_t)p * n + j], w);
+      h[2 * p] = z.x;
+      h[2 * p + 1] = z.y;
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const size_t iv = (size_t)v * n + j;
+      const double R = (double)residual<CLOS, false>(h[v], a.t[iv], a.U[iv], 0.0f);
+      acc[0] += R * R;                            // cal_rms.cu:18
+      if (gram) {
+        double d[kDmMax];
+#pragma unroll
+        for (int i = 0; i < kDmMax; ++i)
+          d[i] = i < fill ? R - (double)a.RP[(size_t)i * V * n + iv] : 0.0;
+#pragma unroll
+        for (int i = 0; i < kDmMax; ++i) {
+          if (i >= fill) break;
+          acc[1 + i] += w8[v] * R * d[i];
+#pragma unroll
+          for (int k = i; k < kDmMax; ++k)
+            if (k < fill) acc[1 + kDmMax + dm_tri(i, k)] += w8[v] * d[i] * d[k];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kDmSums; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[k] = v;
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < kDmSums; ++k) red[wid][k] = acc[k];
+  __syncthreads();
+  for (int k = threadIdx.x; k < kDmSums; k += blockDim.x) {
+    double s = 0.0;
+    for (int w2 = 0; w2 < kThreads / 32; ++w2) s += red[w2][k];
+    a.part[(size_t)k * a.nblocks + blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(a.count, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_dm(st, a.part, a.nblocks, (double)n * V, a.hist, a.hist_cap, M);
+  if (threadIdx.x == 0) *a.count = 0u;
+}
+
+// After a depth-M bulk: its two newest history entries become AN2's two
+// slots (the newest in slot 1, the other in slot 0, the next write to slot
+// 0), so that the refinement continues the history as after an AN2 bulk.
+__global__ void k_dm_handover(long long vn, int M, const float *Ydm, const float *RPdm,
+                              DevState *st, float *Y, float *RP) {
+  const int last = st->dm_last, fill = st->dm_fill;
+  if (last < 0 || fill < 1) return;
+  const int prev = fill >= 2 ? (last + M - 1) % M : last;
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < vn;
+       f += (long long)gridDim.x * blockDim.x) {
+    Y[vn + f] = Ydm[(size_t)last * vn + f];
+    RP[vn + f] = RPdm[(size_t)last * vn + f];
+    Y[f] = Ydm[(size_t)prev * vn + f];
+    RP[f] = RPdm[(size_t)prev * vn + f];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->binary = 0;
+}
+
 // U_SR = u_v + q_v cf esr for a charge-up stage (FP64 and FP32 copies);
 // arrays [B][V][N], esr [B][N].
 __global__ void k_stage_u(long long n, int nv, long long total, const double *u,
@@ -1927,8 +2173,24 @@ void launch_pass_r(Context &c, const IterArgs<T> &a) {
   k_pass_r<T, V, CLOS, REF><<<dim3(a.nblocks, c.nb), kThreads, 0, c.stream>>>(a);
 }
 
+// One FP32 bulk iteration with the depth-M Anderson passes (3D cuFFT path).
+template <int V, int CLOS>
+void launch_iteration_dm(Context &c, const IterArgs<float> &a, cufftHandle plan) {
+  k_pass_a_dm<V, CLOS><<<wave_blocks(k_pass_a_dm<V, CLOS>, a.n, 1), kThreads, 0, c.stream>>>(a);
+  cufftExecC2C(plan, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_FORWARD);
+  k_kspace<float, V><<<wave_blocks(k_kspace<float, V>, a.n / 2, 1), kThreads, 0, c.stream>>>(a);
+  cufftExecC2C(plan, (cufftComplex *)a.buf, (cufftComplex *)a.buf, CUFFT_INVERSE);
+  k_pass_r_dm<V, CLOS><<<a.nblocks, kThreads, 0, c.stream>>>(a, c.dm_depth);
+}
+
 template <typename T, int V, int CLOS, bool REF>
 void launch_iteration(Context &c, const IterArgs<T> &a, cufftHandle plan) {
+  if constexpr (sizeof(T) == 4 && !REF) {
+    if (c.dm_depth && (const void *)a.Y == (const void *)c.f_Ydm) {
+      launch_iteration_dm<V, CLOS>(c, a, plan);
+      return;
+    }
+  }
   // the fused-axis passes run the plain FP32 bulk; the refinement form
   // (which also streams R0) stays on the 3D transforms, where its pipelined
   // passes are faster.  Every phase starts without a pending update (its
@@ -2097,6 +2359,7 @@ __global__ void k_phase_begin(DevState *st, int nb, int kind, double conv, int m
     s.maxstep = max(1, maxstep - s.stage_iter);
     s.watch = watch; s.since = 0; s.best = 1e300; s.loops = 0;
     if (kind == kRefine32 && fallback) { s.done = 4; s.after_done = 1; }
+    if (kind == kPlain32) { s.dm_fill = 0; s.dm_last = -1; s.dm_use = 0; }
     if (kind == kFinal64 && fresh) { s.count = an2_count; s.binary = 0; }
   }
 }
@@ -2357,9 +2620,16 @@ int solve_v(Context &c, int chargeup) {
       c.launches += 3;
       double sw = c.prm.mixed_switch > 0 ? c.prm.mixed_switch : 100.0 * c.prm.convergence;
       if (sw < c.prm.convergence) sw = c.prm.convergence;
-      st = run_phase<float, V, CLOS, false>(c, c.plan32, c.f_t, c.f_U, c.f_Y, c.f_RP, c.f_buf,
+      st = run_phase<float, V, CLOS, false>(c, c.plan32, c.f_t, c.f_U,
+                                           c.dm_depth ? c.f_Ydm : c.f_Y,
+                                           c.dm_depth ? c.f_RPdm : c.f_RP, c.f_buf,
                                            false, kPlain32, sw, true);
       if (st != RISM3D_OK) { status = st; break; }
+      if (c.dm_depth) {
+        k_dm_handover<<<gb, kThreads, 0, c.stream>>>(vn, c.dm_depth, c.f_Ydm, c.f_RPdm, c.d_state,
+                                                      c.f_Y, c.f_RP);
+        c.launches += 1;
+      }
       k_promote_base<<<gb, kThreads, 0, c.stream>>>(vn, c.f_t, c.d_state, c.d_t);
       c.launches += 1;
       st = refine_base<V, CLOS>(c);

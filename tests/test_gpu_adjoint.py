@@ -140,8 +140,12 @@ def test_config4_gradients_on_32_atoms_match_central_differences():
     error linear in the step (measured ~5x larger at 5e-3 A than at 1e-3 A);
     the extrapolation 2 D(h) - D(2h) removes its mean, and the steps are
     h = 2.5e-4 A and 5e-4 A (with 1e-3 A and 2e-3 A, 2 of the 96 components
-    were 2.4e-4 and 4.8e-4 off).  LJ sigma and epsilon are
-    checked on 4 of the atoms.  The differences re-solve in FP64 to a 1e-11
+    were 2.4e-4 and 4.8e-4 off).  LJ sigma (step 1e-4 A) and epsilon (step
+    5e-4 of each epsilon) are checked on 4 of the atoms.  The epsilon step
+    is not 1e-4: mu is resolved to ~1e-6 J/mol, and for the atom with the
+    smallest epsilon gradient (-0.0118) a 1e-4 step moves mu by only a few
+    times that, so its difference quotient was 1 % off, against 1e-5 at
+    5e-4 (2e-4: 1.3e-3; 1e-3: 3e-4, the step's truncation).  The differences re-solve in FP64 to a 1e-11
     residual, each started from the unperturbed solution (a mixed-precision
     context evaluates the LJ grid in FP32, whose rounding moves mu by more
     than the 1e-3 A position steps resolve).
@@ -185,7 +189,7 @@ def test_config4_gradients_on_32_atoms_match_central_differences():
         sp, sm = case.sig.copy(), case.sig.copy()
         sp[u] += 1e-4; sm[u] -= 1e-4
         fds.append((mu(sig=sp) - mu(sig=sm)) / 2e-4)
-        he = 1e-4 * case.eps[u]
+        he = 5e-4 * case.eps[u]
         ep, em = case.eps.copy(), case.eps.copy()
         ep[u] += he; em[u] -= he
         fde.append((mu(eps=ep) - mu(eps=em)) / (2 * he))

@@ -151,3 +151,33 @@ def test_pass_r_forms_agree(precision):
         else:
             assert abs(r["sfe_sc"] - out[0]["sfe_sc"]) < 0.1 * MU_TOL
             assert abs(r["iterations"] - out[0]["iterations"]) <= max(10, 0.1 * out[0]["iterations"])
+
+
+@pytest.mark.parametrize("name", ["cfg0_chain12", "cfg2_protein846_kh"])
+def test_depth_m_anderson_bulk(name):
+    """The opt-in depth-M Anderson accelerator of the FP32 bulk
+    (RISM3D_MDIIS=M).  With M = 2 it is AN2's own update, so the mixed solve
+    takes the AN2 form's steps (within the rounding of the FP64 Gram sums,
+    which the two passes add in different orders) to the same mu_ex; with
+    M = 5 it converges to the same fixed point (mu_ex within the FP32 bulk's
+    reach of the AN2 result, the FP64 cycles gate both)."""
+    import os
+    import rism3d_b200 as R
+    case, _, _ = load_case(name)
+    s = product_solver(case, precision=R.MIXED)
+    r_an2 = s.solve()
+    s.close()
+    out = {}
+    for M in (2, 5):
+        os.environ["RISM3D_MDIIS"] = str(M)
+        try:
+            s = product_solver(case, precision=R.MIXED)
+        finally:
+            del os.environ["RISM3D_MDIIS"]
+        out[M] = s.solve()
+        s.close()
+    assert abs(out[2]["iterations"] - r_an2["iterations"]) <= max(3, 0.05 * r_an2["iterations"]), \
+        (out[2]["iterations"], r_an2["iterations"])
+    for M in (2, 5):
+        assert abs(out[M]["sfe_sc"] - r_an2["sfe_sc"]) < 0.1 * MU_TOL, (M, out[M]["sfe_sc"], r_an2["sfe_sc"])
+        assert abs(out[M]["pmv"] - r_an2["pmv"]) < 1e-4
