@@ -396,7 +396,7 @@ __device__ void pass_a_final(const IterArgs<T> &a, int mode, int done, int slot,
 }
 
 template <typename T, int V, int CLOS, bool REF>
-__global__ void __launch_bounds__(kThreads) k_pass_a(IterArgs<T> a0) {
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_pass_a(IterArgs<T> a0) {
   const IterArgs<T> a = solute_view<T, V>(a0);
   const DevState *st = a.st;
   const int done = st->done;
