@@ -395,8 +395,18 @@ __device__ void pass_a_final(const IterArgs<T> &a, int mode, int done, int slot,
   }
 }
 
+// Resident blocks per SM that pass A's register bound asks for: with one
+// packed site pair the FP32 forms fit 64 registers (4 blocks) and the FP64
+// KH plain form 80 (3 blocks) without spills; every other form keeps the
+// compiler's choice (a bound there spills).
+template <typename T, int V, int CLOS, bool REF> struct PassAOccupancy {
+  static constexpr int blocks =
+      V > 2 ? 1 : sizeof(T) == 4 ? 4 : (V == 1 || (CLOS == 0 && !REF)) ? 3 : 1;
+};
+
 template <typename T, int V, int CLOS, bool REF>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_pass_a(IterArgs<T> a0) {
+__global__ void __launch_bounds__(kThreads, (PassAOccupancy<T, V, CLOS, REF>::blocks))
+    k_pass_a(IterArgs<T> a0) {
   const IterArgs<T> a = solute_view<T, V>(a0);
   const DevState *st = a.st;
   const int done = st->done;
