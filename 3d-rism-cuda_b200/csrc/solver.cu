@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(kThreads, (PassAOccupancy<T, V, CLOS, REF>::bl
     if (st->after_done == 0) pass_a_final<T, V, CLOS, REF>(a, mode, done, slot, s1, s2, m);
     return;                                     // past the snapshot: idle
   }
-  constexpr int PTS = sizeof(T) == 4 ? 2 : 1;
+  constexpr int PTS = (sizeof(T) == 4 && V <= 2) ? 2 : 1;
   if (mode == 2) pass_a_body<T, V, CLOS, 2, PTS, REF>(a, slot, s1, s2, m);
   else if (mode == 1) pass_a_body<T, V, CLOS, 1, PTS, REF>(a, slot, s1, s2, m);
   else pass_a_body<T, V, CLOS, 0, PTS, REF>(a, slot, s1, s2, m);
