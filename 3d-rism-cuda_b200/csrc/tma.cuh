@@ -10,7 +10,7 @@
 // wait_group).  Shared-memory writes of ordinary threads become visible to
 // the TMA unit only after fence.proxy.async.
 //
-// No load here uses cluster multicast: every CTA fetches its own data.
+// Every CTA fetches its own data: each load names only this CTA's shared memory.
 #pragma once
 
 #include <cuda.h>
