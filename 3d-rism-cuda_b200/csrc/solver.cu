@@ -396,12 +396,13 @@ __device__ void pass_a_final(const IterArgs<T> &a, int mode, int done, int slot,
 }
 
 // Resident blocks per SM that pass A's register bound asks for: with one
-// packed site pair the FP32 forms fit 64 registers (4 blocks) and the FP64
-// KH plain form 80 (3 blocks) without spills; every other form keeps the
-// compiler's choice (a bound there spills).
+// packed site pair the FP32 plain form fits 64 registers (4 blocks) and the
+// FP64 KH plain form 80 (3 blocks) without spills.  Every other form keeps
+// the compiler's choice: a bound spills there, or (the FP32 refinement form,
+// used when its pipelined pass is off) runs slower at 64 registers.
 template <typename T, int V, int CLOS, bool REF> struct PassAOccupancy {
   static constexpr int blocks =
-      V > 2 ? 1 : sizeof(T) == 4 ? 4 : (V == 1 || (CLOS == 0 && !REF)) ? 3 : 1;
+      V > 2 ? 1 : sizeof(T) == 4 ? (REF ? 1 : 4) : (V == 1 || (CLOS == 0 && !REF)) ? 3 : 1;
 };
 
 template <typename T, int V, int CLOS, bool REF>
