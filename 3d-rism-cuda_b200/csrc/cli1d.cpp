@@ -1,6 +1,8 @@
-// rism1d-b200: solvent susceptibility tables (.xvk) from the 1D XRISM solve.
+// rism1d-b200: solvent susceptibility tables (.xvk) from the 1D XRISM (or,
+// with -D, DRISM) solve.
 //
-//   rism1d-b200 [-T kelvin] [-n ntab] [-r dr] [-c KH|HNC] [-e conv] [-v] sites.txt out.xvk
+//   rism1d-b200 [-T kelvin] [-n ntab] [-r dr] [-c KH|HNC] [-e conv] [-D eps [-a smear]] [-v]
+//               sites.txt out.xvk
 //
 // sites.txt: one line per site, "NAME SPC SYM sigma[A] eps[J/mol] q[e] x y z
 // density[M]" (the column layout of an .xvk header; lines starting with #
@@ -25,21 +27,23 @@ int main(int argc, char **argv) {
   p.closure = RISM3D_KH;
   p.convergence = 1e-12;
   int opt;
-  while ((opt = getopt(argc, argv, "T:n:r:c:e:v")) != -1) {
+  while ((opt = getopt(argc, argv, "T:n:r:c:e:D:a:v")) != -1) {
     switch (opt) {
       case 'T': p.temperature = atof(optarg); break;
       case 'n': p.ntab = atoi(optarg); break;
       case 'r': p.dr = atof(optarg); break;
       case 'c': p.closure = strcmp(optarg, "HNC") == 0 ? RISM3D_HNC : RISM3D_KH; break;
       case 'e': p.convergence = atof(optarg); break;
+      case 'D': p.dielectric = atof(optarg); break;
+      case 'a': p.smear = atof(optarg); break;
       case 'v': p.verbose = 1; break;
       default:
-        fprintf(stderr, "usage: %s [-T K] [-n ntab] [-r dr] [-c KH|HNC] [-e conv] [-v] sites out.xvk\n", argv[0]);
+        fprintf(stderr, "usage: %s [-T K] [-n ntab] [-r dr] [-c KH|HNC] [-e conv] [-D eps [-a smear]] [-v] sites out.xvk\n", argv[0]);
         return 1;
     }
   }
   if (argc - optind != 2) {
-    fprintf(stderr, "usage: %s [-T K] [-n ntab] [-r dr] [-c KH|HNC] [-e conv] [-v] sites out.xvk\n", argv[0]);
+    fprintf(stderr, "usage: %s [-T K] [-n ntab] [-r dr] [-c KH|HNC] [-e conv] [-D eps [-a smear]] [-v] sites out.xvk\n", argv[0]);
     return 1;
   }
   std::ifstream in(argv[optind]);

@@ -21,6 +21,18 @@
 // computed with a radix-2 FFT of length 2N (N a power of two).  The table
 // row j = N (k = pi/dr) has sin = 0 at every r_i: h = 0, X = w.
 //
+// DRISM (p->dielectric > 0; Perkyns and Pettitt, J. Chem. Phys. 97, 7656
+// (1992)): the intramolecular matrix becomes W' = W + P chi, where chi
+// couples the sites of molecules with a dipole moment mu,
+//   chi_ij(k) = z_i(k) hc(k) z_j(k),  z_i = j0(k x_i) j0(k y_i) j1(k z_i),
+//   hc(k) = (eps / Y - 3) / (4 pi rho_d) exp(-a^2 k^2 / 4),
+//   Y = 4 pi beta sum_s rho_s mu_s^2 / 9,  rho_d = sum_s rho_s,
+// with (x, y, z) each site's coordinates from its molecule's |q|-weighted
+// centre and the dipole along z.  The equation above is solved for h - chi,
+// and the closure and the tables see h.  The DIIS mixing defaults to 0.1
+// there: at 0.3 it could settle on a second, unphysical solution (negative
+// ion-ion structure at k -> 0).
+//
 // Iteration: DIIS (Pulay) on t_s with the residual R = t_s' - t_s, depth
 // 10, mixing 0.3, falling back to damped Picard steps when the DIIS system
 // is ill-conditioned.  Water-like solvents do not converge from t = 0 at
@@ -132,6 +144,7 @@ struct System {
   std::vector<int> pi, pj;               // pair list i <= j
   std::vector<double> ulj, ues, uL_k, w; // [pair][r] x2, [pair][k] x2
   std::vector<double> us, uLl;           // the potential at the current lambda
+  std::vector<double> chi;               // DRISM bridge [pair][k] (empty: XRISM)
 };
 
 int pair_index(const System &s, int i, int j) {
@@ -204,6 +217,57 @@ int rism1d_solve(const rism1d_params *p, int nsite, const rism1d_site *sites, do
       s.w[(size_t)pp * M + m] = wv;
     }
   }
+  if (p->dielectric > 0) {
+    // dipolar molecules: centre, dipole along z, and the bridge's strength
+    const int nspc = *std::max_element(s.spc.begin(), s.spc.end());
+    std::vector<double> cx(ns), cy(ns), cz(ns);
+    std::vector<char> dip(ns, 0);
+    double rhod = 0.0, rmu2 = 0.0;
+    for (int sp = 1; sp <= nspc; ++sp) {
+      double wx = 0, wy = 0, wz = 0, wt = 0, mx = 0, my = 0, mz = 0, rho_s = 0;
+      for (int i = 0; i < ns; ++i) {
+        if (s.spc[i] != sp) continue;
+        const double wq = std::fabs(s.q[i]);
+        wx += wq * s.x[i]; wy += wq * s.y[i]; wz += wq * s.z[i]; wt += wq;
+        mx += s.q[i] * s.x[i]; my += s.q[i] * s.y[i]; mz += s.q[i] * s.z[i];
+        rho_s = s.rho[i];
+      }
+      const double mu2 = mx * mx + my * my + mz * mz;
+      if (!(mu2 > 1e-12)) continue;
+      if (mx * mx + my * my > 1e-12 * mu2) {
+        g_err1d = "DRISM: the dipole of species " + std::to_string(sp) + " is not along z";
+        return RISM3D_BAD_INPUT;
+      }
+      const double sg = mz > 0 ? 1.0 : -1.0;
+      for (int i = 0; i < ns; ++i) {
+        if (s.spc[i] != sp) continue;
+        cx[i] = s.x[i] - wx / wt; cy[i] = s.y[i] - wy / wt; cz[i] = sg * (s.z[i] - wz / wt);
+        dip[i] = 1;
+      }
+      rhod += rho_s;
+      rmu2 += rho_s * mu2;
+    }
+    if (rhod > 0) {
+      const double yd = 4.0 * kPi * ubeta * rmu2 / 9.0;
+      const double hc0 = (p->dielectric / yd - 3.0) / (4.0 * kPi * rhod);
+      const double a = p->smear > 0 ? p->smear : 2.0;
+      auto j0 = [](double x) { return std::fabs(x) < 1e-8 ? 1.0 : std::sin(x) / x; };
+      auto j1 = [](double x) {
+        return std::fabs(x) < 1e-4 ? x / 3.0 : std::sin(x) / (x * x) - std::cos(x) / x;
+      };
+      s.chi.assign((size_t)s.npair * M, 0.0);
+      for (int pp = 0; pp < s.npair; ++pp) {
+        const int i = s.pi[pp], j = s.pj[pp];
+        if (!dip[i] || !dip[j]) continue;
+        for (int m = 0; m < M; ++m) {
+          const double kk = k[m];
+          const double zi = j0(kk * cx[i]) * j0(kk * cy[i]) * j1(kk * cz[i]);
+          const double zj = j0(kk * cx[j]) * j0(kk * cy[j]) * j1(kk * cz[j]);
+          s.chi[(size_t)pp * M + m] = zi * zj * hc0 * std::exp(-a * a * kk * kk / 4.0);
+        }
+      }
+    }
+  }
   Dst dst(N);
   const size_t L = (size_t)s.npair * M;
   std::vector<double> ts(L, 0.0), cs(L), Ck(L), Tk(L), tn(L), Hk(L), tmp(M), tmp2(M);
@@ -231,8 +295,10 @@ int rism1d_solve(const rism1d_params *p, int nsite, const rism1d_site *sites, do
       for (int pp = 0; pp < s.npair; ++pp) {
         const int i = s.pi[pp], j = s.pj[pp];
         const double wv = s.w[(size_t)pp * M + m];
+        const double xb = s.chi.empty() ? 0.0 : s.chi[(size_t)pp * M + m];
         const double cv = Ck[(size_t)pp * M + m] - s.uLl[(size_t)pp * M + m];
-        Wm[(size_t)i * ns + j] = Wm[(size_t)j * ns + i] = wv;
+        Wm[(size_t)i * ns + j] = wv + s.rho[i] * xb;     // W' = W + P chi
+        Wm[(size_t)j * ns + i] = wv + s.rho[j] * xb;
         Cm[(size_t)i * ns + j] = Cm[(size_t)j * ns + i] = cv;
       }
       for (int i = 0; i < ns; ++i)
@@ -251,7 +317,8 @@ int rism1d_solve(const rism1d_params *p, int nsite, const rism1d_site *sites, do
       if (!solve_dense(ns, A, B, ns)) return false;
       for (int pp = 0; pp < s.npair; ++pp) {
         const int i = s.pi[pp], j = s.pj[pp];
-        const double h = 0.5 * (B[(size_t)i * ns + j] + B[(size_t)j * ns + i]);
+        const double h = 0.5 * (B[(size_t)i * ns + j] + B[(size_t)j * ns + i]) +
+                         (s.chi.empty() ? 0.0 : s.chi[(size_t)pp * M + m]);
         if (keep_h) Hk[(size_t)pp * M + m] = h;
         Tk[(size_t)pp * M + m] = h - Ck[(size_t)pp * M + m];
       }
@@ -267,7 +334,7 @@ int rism1d_solve(const rism1d_params *p, int nsite, const rism1d_site *sites, do
   };
   // DIIS at charge scale lambda from the current t_s
   const int depth = 10;
-  const double mix = p->mixing > 0 ? p->mixing : 0.3;
+  const double mix = p->mixing > 0 ? p->mixing : (s.chi.empty() ? 0.3 : 0.1);
   const double conv = p->convergence > 0 ? p->convergence : 1e-12;
   const int maxit = p->maxstep > 0 ? p->maxstep : 10000;
   int it_total = 0;
@@ -348,6 +415,42 @@ int rism1d_solve(const rism1d_params *p, int nsite, const rism1d_site *sites, do
   // final cycle for h(k); X_ab(k) = sum over sites j of type b of
   // (w_ij + rho_j h_ij) with i the first site of type a
   cycle(ts, tn, true);
+  // A physical solution has a positive-definite structure-factor matrix of
+  // the species at the smallest k, S_mn = d_mn + sqrt(rho_m rho_n) h_mn
+  // (first sites).  The equations for a salt solution also have solutions
+  // with a negative concentration structure factor (plain XRISM always
+  // lands there; DRISM can, depending on the iteration path): refused.
+  {
+    std::vector<int> first;
+    for (int i = 0; i < ns; ++i) {
+      bool seen = false;
+      for (int f : first) seen = seen || s.spc[f] == s.spc[i];
+      if (!seen) first.push_back(i);
+    }
+    const int ms = (int)first.size();
+    std::vector<double> S((size_t)ms * ms);
+    for (int a = 0; a < ms; ++a)
+      for (int c = 0; c < ms; ++c) {
+        const int pp = pair_index(s, first[a], first[c]);
+        S[(size_t)a * ms + c] = (a == c ? 1.0 : 0.0) +
+                                std::sqrt(s.rho[first[a]] * s.rho[first[c]]) * Hk[(size_t)pp * M];
+      }
+    for (int a = 0; a < ms; ++a) {                 // Cholesky: every pivot positive
+      for (int c = 0; c < a; ++c) S[(size_t)a * ms + a] -= S[(size_t)a * ms + c] * S[(size_t)a * ms + c];
+      const double d = S[(size_t)a * ms + a];
+      if (!(d > 0.0)) {
+        g_err1d = "the 1D solution is unphysical: the species structure factor at k -> 0 "
+                  "is not positive definite (for a salt solution use DRISM, dielectric > 0)";
+        return RISM3D_NOT_CONVERGED;
+      }
+      S[(size_t)a * ms + a] = std::sqrt(d);
+      for (int b = a + 1; b < ms; ++b) {
+        double v = S[(size_t)b * ms + a];
+        for (int c = 0; c < a; ++c) v -= S[(size_t)b * ms + c] * S[(size_t)a * ms + c];
+        S[(size_t)b * ms + a] = v / S[(size_t)a * ms + a];
+      }
+    }
+  }
   const int nt = s.ntype;
   if (xvv) {
     for (int a = 0; a < nt; ++a)

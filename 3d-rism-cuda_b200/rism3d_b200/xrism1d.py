@@ -13,7 +13,8 @@ from . import KH, HNC, RismError, lib  # noqa: F401
 class Params(C.Structure):
     _fields_ = [("temperature", C.c_double), ("ntab", C.c_int), ("dr", C.c_double),
                 ("closure", C.c_int), ("convergence", C.c_double), ("maxstep", C.c_int),
-                ("mixing", C.c_double), ("verbose", C.c_int)]
+                ("mixing", C.c_double), ("verbose", C.c_int),
+                ("dielectric", C.c_double), ("smear", C.c_double)]
 
 
 class Site(C.Structure):
@@ -61,10 +62,14 @@ def read_sites(path):
 
 
 def solve(rows, temperature, ntab=4096, dr=0.05, closure=KH, convergence=1e-12,
-          maxstep=10000, mixing=0.3, verbose=0):
-    """Returns (xvv [ntype, ntype, ntab], xt [1/Pa], iterations)."""
+          maxstep=10000, mixing=0.0, verbose=0, dielectric=0.0, smear=0.0):
+    """Returns (xvv [ntype, ntype, ntab], xt [1/Pa], iterations).
+    dielectric > 0 selects DRISM with that dielectric constant (smear: the
+    bridge's damping length in A, 0 = 2.0); mixing 0 takes the solver's
+    default (0.3 for XRISM, 0.1 for DRISM)."""
     L = _bind()
-    p = Params(temperature, ntab, dr, closure, convergence, maxstep, mixing, verbose)
+    p = Params(temperature, ntab, dr, closure, convergence, maxstep, mixing, verbose,
+               dielectric, smear)
     sites = make_sites(rows)
     nt = max(abs(int(r[2])) for r in rows)
     xvv = np.zeros((nt, nt, ntab))

@@ -286,13 +286,16 @@ int rism3d_iterate(rism3d_ctx *ctx, int chargeup);
  * .cuv, .euv, .qv according to the control file's outlist letters. */
 int rism3d_output(rism3d_ctx *ctx);
 
-/* ---- 1D XRISM solvent tables ------------------------------------------
+/* ---- 1D XRISM / DRISM solvent tables ----------------------------------
  * No counterpart in the reference: it reads X_ab(k) from .xvk files
  * (solvent_read.cc:31-60) made by a separate program that it does not
  * ship.  rism1d_solve computes them for a molecular solvent (any mixture of
  * rigid molecules and ions) with the 1D extended RISM equations and the KH
  * (or HNC) closure on the grid r_i = i dr, k_j = j pi / (ntab dr), and
- * rism1d_write_xvk writes them in the .xvk layout the 3D solver reads. */
+ * rism1d_write_xvk writes them in the .xvk layout the 3D solver reads.
+ * With dielectric > 0 the equations are the dielectrically consistent
+ * DRISM ones (Perkyns and Pettitt): every molecule with a dipole moment
+ * must have it along +z or -z in its site coordinates. */
 typedef struct {
   double temperature;   /* K */
   int ntab;             /* radial / k points (power of two) */
@@ -300,8 +303,10 @@ typedef struct {
   int closure;          /* RISM3D_KH or RISM3D_HNC */
   double convergence;   /* rms of the t update (0 = 1e-12) */
   int maxstep;          /* 0 = 10000 */
-  double mixing;        /* DIIS mixing (0 = 0.3) */
+  double mixing;        /* DIIS mixing (0 = 0.3; with DRISM 0.1) */
   int verbose;
+  double dielectric;    /* > 0: DRISM with this dielectric constant; 0: XRISM */
+  double smear;         /* DRISM bridge damping length a, A (0 = 2.0) */
 } rism1d_params;
 
 typedef struct {
